@@ -1,0 +1,483 @@
+"""ctypes view of the CPU oracle (``oracle/lzx_oracle.c``).
+
+TEST INFRASTRUCTURE ONLY: the correctness oracle for the CUDA path and the
+timed CPU baseline.  Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU
+legs of ``bench.py`` import this module; the product package ``lzx_b200``
+never does.  Every wrapped C function restates a function of the reference
+(idrees2516/lzx, Rust) and cites its file:line in ``lzx_oracle.c``.
+
+Parity pin: the Goldilocks and Keccak restatements are checked against the
+reference's own known-answer tests (``tests/golden/reference_kats.json``); the
+NTT and commitment restatements are checked against the reference's identity
+tests and against direct evaluation at psi^(2j+1).  No reference-produced
+NTT/commit digests exist to compare with (the reference's KAT manifest is
+generated at run time and not committed).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import threading
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_BUILD = os.path.join(_HERE, "_build")
+_lock = threading.Lock()
+_lib = None
+_native = None
+
+GL_P = 0xFFFFFFFF00000001
+
+# CRT set: the four largest 30-bit primes q == 1 (mod 512), with the smallest
+# generator of each multiplicative group and the 2-adicity of q - 1.
+CRT_PRIMES = (
+    (1073738753, 10, 3),
+    (1073732609, 10, 3),
+    (1073731073, 9, 3),
+    (1073726977, 9, 5),
+)
+# Modulus32 constants of the reference, lattice-ring/src/modulus.rs:46-55
+Q_32 = (3221225473, 30, 5)
+Q_12289 = (12289, 12, 11)
+Q_2013265921 = (2013265921, 27, 31)
+
+
+class Mod32(C.Structure):
+    _fields_ = [("q", C.c_uint32), ("two_adicity", C.c_uint32), ("generator", C.c_uint32),
+                ("barrett_recip", C.c_uint64)]
+
+
+class Ntt32(C.Structure):
+    _fields_ = [("modulus", Mod32), ("log_n", C.c_uint32), ("n_inv", C.c_uint32),
+                ("pow_psi", C.c_void_p), ("pow_psi_inv", C.c_void_p), ("pow_omega", C.c_void_p),
+                ("pow_omega_inv", C.c_void_p), ("level_tw", C.c_void_p),
+                ("level_tw_inv", C.c_void_p)]
+
+
+class NttGl(C.Structure):
+    _fields_ = [("log_n", C.c_uint32), ("n_inv", C.c_uint64), ("pow_psi", C.c_void_p),
+                ("pow_psi_inv", C.c_void_p), ("level_tw", C.c_void_p), ("level_tw_inv", C.c_void_p)]
+
+
+def _build(target: str) -> None:
+    subprocess.run(["make", "-s", "-C", _HERE, target], check=True)
+
+
+def _declare(lib):
+    P = C.c_void_p
+    sz, u32, u64, i32 = C.c_size_t, C.c_uint32, C.c_uint64, C.c_int
+    sig = {
+        "orc_mod32_new": (Mod32, [u32, u32, u32]),
+        "orc_mod32_reduce_u64": (u32, [P, u64]),
+        "orc_mod32_reduce_i64": (u32, [P, C.c_int64]),
+        "orc_mod32_mul": (u32, [P, u32, u32]),
+        "orc_mod32_add": (u32, [P, u32, u32]),
+        "orc_mod32_sub": (u32, [P, u32, u32]),
+        "orc_mod32_neg": (u32, [P, u32]),
+        "orc_mod32_pow": (u32, [P, u32, u64]),
+        "orc_mod32_inv": (u32, [P, u32]),
+        "orc_mod32_root_of_unity": (u32, [P, u32]),
+        "orc_gl_from_u64": (u64, [u64]),
+        "orc_gl_from_u128": (u64, [u64, u64]),
+        "orc_gl_add": (u64, [u64, u64]),
+        "orc_gl_sub": (u64, [u64, u64]),
+        "orc_gl_neg": (u64, [u64]),
+        "orc_gl_mul": (u64, [u64, u64]),
+        "orc_gl_pow": (u64, [u64, u64]),
+        "orc_gl_inv": (u64, [u64]),
+        "orc_ntt32_new": (i32, [Mod32, u32, P]),
+        "orc_ntt32_free": (None, [P]),
+        "orc_ntt32_forward": (i32, [P, P, sz]),
+        "orc_ntt32_forward_fast": (i32, [P, P, sz]),
+        "orc_ntt32_inverse": (i32, [P, P, sz]),
+        "orc_ntt32_inverse_fast": (i32, [P, P, sz]),
+        "orc_ntt32_forward_partial": (i32, [P, P, sz, u32]),
+        "orc_ntt32_complete_partial": (i32, [P, P, sz, u32]),
+        "orc_ntt32_forward_batch": (i32, [P, P, sz, i32]),
+        "orc_ntt32_inverse_batch": (i32, [P, P, sz, i32]),
+        "orc_nttgl_new": (i32, [u32, P]),
+        "orc_nttgl_free": (None, [P]),
+        "orc_nttgl_forward_fast": (i32, [P, P, sz]),
+        "orc_nttgl_inverse_fast": (i32, [P, P, sz]),
+        "orc_nttgl_forward_batch": (i32, [P, P, sz, i32]),
+        "orc_nttgl_inverse_batch": (i32, [P, P, sz, i32]),
+        "orc_ajtai32_commit": (i32, [P, P, sz, sz, P, P]),
+        "orc_ajtai32_commit_naive": (i32, [P, P, sz, sz, P, P]),
+        "orc_ring32_mul": (i32, [P, P, P, P]),
+        "orc_ajtaigl_commit_batch": (i32, [P, P, sz, sz, P, sz, P, i32, i32]),
+        "orc_ajtaigl_commit_batch_i8": (i32, [P, P, sz, sz, P, sz, P, i32, i32]),
+        "orc_avx512_available": (i32, []),
+        "orc_neo_mul": (None, [sz, P, P, P]),
+        "orc_neo_commit_naive": (i32, [sz, sz, sz, P, P, sz, P]),
+        "orc_neo_commit_pay_per_bit": (i32, [sz, sz, sz, P, P, sz, P, P]),
+        "orc_decomp_b": (None, [P, sz, u32, P]),
+        "orc_gadget_decompose": (i32, [u64, sz, u64, P]),
+        "orc_keccak_f1600": (None, [P]),
+        "orc_sha3_256": (None, [P, sz, P]),
+        "orc_shake256": (None, [P, sz, P, sz]),
+        "orc_xof": (None, [P, sz, P, sz, P, sz]),
+        "orc_hash_domain": (None, [P, sz, P, sz, P]),
+        "orc_uniform_from_seed": (None, [P, u32, P, sz, P, sz, u64, P]),
+        "orc_ring_random": (None, [P, u32, P, sz, P]),
+        "orc_ajtai32_from_seed": (i32, [P, sz, sz, P, P, P]),
+        "orc_sample_small_secret": (None, [P, u32, sz, u32, P, sz, P]),
+        "orc_synth_u64": (u64, [u64, u64, u64]),
+        "orc_synth_mod32": (None, [u64, u64, u32, P, sz, sz]),
+        "orc_synth_gl": (None, [u64, u64, P, sz, sz]),
+        "orc_synth_i8": (None, [u64, u64, P, sz, sz]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+def lib(native: bool = False):
+    """The oracle shared library (built on first use)."""
+    global _lib, _native
+    with _lock:
+        if native:
+            if _native is None:
+                path = os.path.join(_BUILD, "liblzx_oracle_native.so")
+                if not os.path.exists(path):
+                    _build("native")
+                _native = _declare(C.CDLL(path))
+            return _native
+        if _lib is None:
+            path = os.path.join(_BUILD, "liblzx_oracle.so")
+            if not os.path.exists(path):
+                _build("all")
+            _lib = _declare(C.CDLL(path))
+        return _lib
+
+
+def ptr(a: np.ndarray):
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _bytes_ptr(b: bytes):
+    buf = C.create_string_buffer(b, len(b) or 1)
+    return buf
+
+
+# ----------------------------------------------------------------- Modulus32
+
+class Modulus32:
+    """Modulus32 (lattice-ring/src/modulus.rs:22-161) over the C restatement."""
+
+    def __init__(self, q: int, two_adicity: int, generator: int):
+        self._m = lib().orc_mod32_new(q, two_adicity, generator)
+        self.q, self.two_adicity, self.generator = q, two_adicity, generator
+
+    @property
+    def barrett_recip(self) -> int:
+        return self._m.barrett_recip
+
+    def _p(self):
+        return C.byref(self._m)
+
+    def reduce_u64(self, x: int) -> int:
+        return lib().orc_mod32_reduce_u64(self._p(), x)
+
+    def reduce_i64(self, x: int) -> int:
+        return lib().orc_mod32_reduce_i64(self._p(), x)
+
+    def mul(self, a, b):
+        return lib().orc_mod32_mul(self._p(), a, b)
+
+    def add(self, a, b):
+        return lib().orc_mod32_add(self._p(), a, b)
+
+    def sub(self, a, b):
+        return lib().orc_mod32_sub(self._p(), a, b)
+
+    def neg(self, a):
+        return lib().orc_mod32_neg(self._p(), a)
+
+    def pow(self, a, e):
+        return lib().orc_mod32_pow(self._p(), a, e)
+
+    def inv(self, a):
+        return None if a == 0 else lib().orc_mod32_inv(self._p(), a)
+
+    def root_of_unity(self, k):
+        return None if k > self.two_adicity else lib().orc_mod32_root_of_unity(self._p(), k)
+
+
+# ----------------------------------------------------------------- NTT tables
+
+class NttError(Exception):
+    def __init__(self, code):
+        super().__init__({1: "LengthMismatch", 2: "AdicityTooSmall"}.get(code, str(code)))
+        self.code = code
+
+
+def _check(rc):
+    if rc != 0:
+        raise NttError(rc)
+
+
+class NttTables32:
+    """NttTables (lattice-ring/src/ntt.rs:16-317) over a u32 modulus."""
+
+    def __init__(self, modulus: Modulus32, log_n: int):
+        self._t = Ntt32()
+        _check(lib().orc_ntt32_new(modulus._m, log_n, C.byref(self._t)))
+        self.modulus, self.log_n, self.n = modulus, log_n, 1 << log_n
+
+    def __del__(self):
+        if getattr(self, "_t", None) is not None and _lib is not None:
+            _lib.orc_ntt32_free(C.byref(self._t))
+            self._t = None
+
+    def _run(self, fn, a: np.ndarray, *extra):
+        a = np.ascontiguousarray(a, dtype=np.uint32).copy()
+        _check(getattr(lib(), fn)(C.byref(self._t), ptr(a), a.size, *extra))
+        return a
+
+    def forward(self, a):
+        return self._run("orc_ntt32_forward", a)
+
+    def forward_fast(self, a):
+        return self._run("orc_ntt32_forward_fast", a)
+
+    def inverse(self, a):
+        return self._run("orc_ntt32_inverse", a)
+
+    def inverse_fast(self, a):
+        return self._run("orc_ntt32_inverse_fast", a)
+
+    def forward_partial(self, a, levels):
+        return self._run("orc_ntt32_forward_partial", a, levels)
+
+    def complete_partial(self, a, already):
+        return self._run("orc_ntt32_complete_partial", a, already)
+
+    def forward_batch(self, a: np.ndarray, nthreads: int = 0, inplace: bool = False):
+        a = a if inplace else np.array(a, dtype=np.uint32, copy=True)
+        assert a.dtype == np.uint32 and a.size % self.n == 0
+        _check(lib().orc_ntt32_forward_batch(C.byref(self._t), ptr(a), a.size // self.n, nthreads))
+        return a
+
+    def inverse_batch(self, a: np.ndarray, nthreads: int = 0, inplace: bool = False):
+        a = a if inplace else np.array(a, dtype=np.uint32, copy=True)
+        assert a.dtype == np.uint32 and a.size % self.n == 0
+        _check(lib().orc_ntt32_inverse_batch(C.byref(self._t), ptr(a), a.size // self.n, nthreads))
+        return a
+
+    def ring_mul(self, a, b):
+        a = np.ascontiguousarray(a, dtype=np.uint32)
+        b = np.ascontiguousarray(b, dtype=np.uint32)
+        out = np.empty(self.n, dtype=np.uint32)
+        lib().orc_ring32_mul(C.byref(self._t), ptr(a), ptr(b), ptr(out))
+        return out
+
+
+class NttTablesGl:
+    """The ntt.rs algorithm instantiated over Goldilocks (field.rs, generator 7)."""
+
+    def __init__(self, log_n: int):
+        self._t = NttGl()
+        _check(lib().orc_nttgl_new(log_n, C.byref(self._t)))
+        self.log_n, self.n = log_n, 1 << log_n
+
+    def __del__(self):
+        if getattr(self, "_t", None) is not None and _lib is not None:
+            _lib.orc_nttgl_free(C.byref(self._t))
+            self._t = None
+
+    def forward_fast(self, a):
+        a = np.ascontiguousarray(a, dtype=np.uint64).copy()
+        _check(lib().orc_nttgl_forward_fast(C.byref(self._t), ptr(a), a.size))
+        return a
+
+    def inverse_fast(self, a):
+        a = np.ascontiguousarray(a, dtype=np.uint64).copy()
+        _check(lib().orc_nttgl_inverse_fast(C.byref(self._t), ptr(a), a.size))
+        return a
+
+    def forward_batch(self, a, nthreads: int = 0, inplace: bool = False):
+        a = a if inplace else np.array(a, dtype=np.uint64, copy=True)
+        _check(lib().orc_nttgl_forward_batch(C.byref(self._t), ptr(a), a.size // self.n, nthreads))
+        return a
+
+    def inverse_batch(self, a, nthreads: int = 0, inplace: bool = False):
+        a = a if inplace else np.array(a, dtype=np.uint64, copy=True)
+        _check(lib().orc_nttgl_inverse_batch(C.byref(self._t), ptr(a), a.size // self.n, nthreads))
+        return a
+
+
+# ----------------------------------------------------------------- commits
+
+def ajtai32_commit(tables: NttTables32, matrix_ntt: np.ndarray, k: int, m: int, s: np.ndarray):
+    """AjtaiPublicKey::commit (lattice-commitment/src/ajtai.rs:118-153)."""
+    matrix_ntt = np.ascontiguousarray(matrix_ntt, dtype=np.uint32)
+    s = np.ascontiguousarray(s, dtype=np.uint32)
+    out = np.empty(k * tables.n, dtype=np.uint32)
+    lib().orc_ajtai32_commit(C.byref(tables._t), ptr(matrix_ntt), k, m, ptr(s), ptr(out))
+    return out.reshape(k, tables.n)
+
+
+def ajtai32_commit_naive(tables: NttTables32, matrix: np.ndarray, k: int, m: int, s: np.ndarray):
+    """AjtaiPublicKey::commit_naive_reference (ajtai.rs:158-180)."""
+    matrix = np.ascontiguousarray(matrix, dtype=np.uint32)
+    s = np.ascontiguousarray(s, dtype=np.uint32)
+    out = np.empty(k * tables.n, dtype=np.uint32)
+    lib().orc_ajtai32_commit_naive(C.byref(tables._t), ptr(matrix), k, m, ptr(s), ptr(out))
+    return out.reshape(k, tables.n)
+
+
+def ajtaigl_commit_batch(tables: NttTablesGl, matrix_ntt, kappa, m, w, nthreads=0, simd=True,
+                         native=False):
+    """Cached-NTT commit (ajtai.rs:118-153) over Goldilocks for a batch of witnesses.
+
+    ``w`` is either uint64 residues [B, m, d] or int8 digits [B, m, d]."""
+    L = lib(native)
+    matrix_ntt = np.ascontiguousarray(matrix_ntt, dtype=np.uint64)
+    d = tables.n
+    w = np.ascontiguousarray(w)
+    batch = w.size // (m * d)
+    out = np.empty((batch, kappa, d), dtype=np.uint64)
+    fn = L.orc_ajtaigl_commit_batch_i8 if w.dtype == np.int8 else L.orc_ajtaigl_commit_batch
+    if w.dtype != np.int8:
+        w = w.astype(np.uint64, copy=False)
+    fn(C.byref(tables._t), ptr(matrix_ntt), kappa, m, ptr(w), batch, ptr(out), nthreads,
+       1 if simd else 0)
+    return out
+
+
+def neo_mul(a, b):
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    b = np.ascontiguousarray(b, dtype=np.uint64)
+    out = np.empty_like(a)
+    lib().orc_neo_mul(a.size, ptr(a), ptr(b), ptr(out))
+    return out
+
+
+def neo_commit_naive(d, kappa, m, matrix, cols):
+    matrix = np.ascontiguousarray(matrix, dtype=np.uint64)
+    cols = np.ascontiguousarray(cols, dtype=np.uint64)
+    ncols = cols.size // d
+    out = np.empty((kappa, d), dtype=np.uint64)
+    rc = lib().orc_neo_commit_naive(d, kappa, m, ptr(matrix), ptr(cols), ncols, ptr(out))
+    if rc:
+        raise ValueError("Shape")
+    return out
+
+
+def neo_commit_pay_per_bit(d, kappa, m, matrix, cols):
+    matrix = np.ascontiguousarray(matrix, dtype=np.uint64)
+    cols = np.ascontiguousarray(cols, dtype=np.uint64)
+    ncols = cols.size // d
+    out = np.empty((kappa, d), dtype=np.uint64)
+    adds = C.c_uint64(0)
+    rc = lib().orc_neo_commit_pay_per_bit(d, kappa, m, ptr(matrix), ptr(cols), ncols, ptr(out),
+                                          C.byref(adds))
+    if rc:
+        raise ValueError("Shape")
+    return out, adds.value
+
+
+def decomp_b(z, b_bits):
+    z = np.ascontiguousarray(z, dtype=np.uint64)
+    rows = -(-64 // b_bits)
+    out = np.empty((rows, z.size), dtype=np.uint64)
+    lib().orc_decomp_b(ptr(z), z.size, b_bits, ptr(out))
+    return out
+
+
+def gadget_decompose(base, num_digits, x):
+    out = np.empty(num_digits, dtype=np.int64)
+    rc = lib().orc_gadget_decompose(base, num_digits, x, ptr(out))
+    if rc:
+        raise ValueError("ValueTooLarge")
+    return out
+
+
+# ----------------------------------------------------------------- hashing
+
+def sha3_256(data: bytes) -> bytes:
+    out = C.create_string_buffer(32)
+    buf = _bytes_ptr(data)
+    lib().orc_sha3_256(buf, len(data), out)
+    return out.raw
+
+
+def shake256(data: bytes, n: int) -> bytes:
+    out = C.create_string_buffer(max(n, 1))
+    buf = _bytes_ptr(data)
+    lib().orc_shake256(buf, len(data), out, n)
+    return out.raw[:n]
+
+
+def xof(domain: bytes, msg: bytes, n: int) -> bytes:
+    out = C.create_string_buffer(max(n, 1))
+    lib().orc_xof(_bytes_ptr(domain), len(domain), _bytes_ptr(msg), len(msg), out, n)
+    return out.raw[:n]
+
+
+def hash_domain(domain: bytes, msg: bytes) -> bytes:
+    out = C.create_string_buffer(32)
+    lib().orc_hash_domain(_bytes_ptr(domain), len(domain), _bytes_ptr(msg), len(msg), out)
+    return out.raw
+
+
+def uniform_from_seed(modulus: Modulus32, log_n: int, domain: bytes, seed: bytes, index: int):
+    out = np.empty(1 << log_n, dtype=np.uint32)
+    lib().orc_uniform_from_seed(modulus._p(), log_n, _bytes_ptr(domain), len(domain),
+                                _bytes_ptr(seed), len(seed), index, ptr(out))
+    return out
+
+
+def ring_random(modulus: Modulus32, log_n: int, seed: bytes):
+    out = np.empty(1 << log_n, dtype=np.uint32)
+    lib().orc_ring_random(modulus._p(), log_n, _bytes_ptr(seed), len(seed), ptr(out))
+    return out
+
+
+def ajtai32_from_seed(tables: NttTables32, k: int, m: int, seed: bytes):
+    n = tables.n
+    mat = np.empty(k * m * n, dtype=np.uint32)
+    mat_ntt = np.empty(k * m * n, dtype=np.uint32)
+    lib().orc_ajtai32_from_seed(C.byref(tables._t), k, m, _bytes_ptr(seed), ptr(mat),
+                                ptr(mat_ntt))
+    return mat, mat_ntt
+
+
+def sample_small_secret(modulus: Modulus32, log_n: int, m: int, bound: int, seed: bytes):
+    out = np.empty(m * (1 << log_n), dtype=np.uint32)
+    lib().orc_sample_small_secret(modulus._p(), log_n, m, bound, _bytes_ptr(seed), len(seed),
+                                  ptr(out))
+    return out
+
+
+# ----------------------------------------------------------------- synthetic inputs
+
+def synth_u64(seed, stream, index):
+    return lib().orc_synth_u64(seed, stream, index)
+
+
+def synth_mod32(seed, stream, q, count, offset=0):
+    out = np.empty(count, dtype=np.uint32)
+    lib().orc_synth_mod32(seed, stream, q, ptr(out), count, offset)
+    return out
+
+
+def synth_gl(seed, stream, count, offset=0):
+    out = np.empty(count, dtype=np.uint64)
+    lib().orc_synth_gl(seed, stream, ptr(out), count, offset)
+    return out
+
+
+def synth_i8(seed, stream, count, offset=0):
+    out = np.empty(count, dtype=np.int8)
+    lib().orc_synth_i8(seed, stream, ptr(out), count, offset)
+    return out
+
+
+def avx512_available() -> bool:
+    return bool(lib().orc_avx512_available())
