@@ -1,0 +1,361 @@
+#!/usr/bin/env python
+"""Benchmark of the LZX commitment hot path on B200.
+
+Workload (one step): the batched negacyclic NTT round trip of 2^16
+polynomials of degree d = 256 under the 4-prime 30-bit CRT set (the four
+largest 30-bit primes q == 1 mod 512): a forward transform of all 2^26
+residues followed by the inverse transform, each reading and writing HBM.
+Unit: coefficient-transforms per second (each of the two transforms counts
+each coefficient once, 2^27 per step).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+* value: device-resident inputs (256 MiB in, larger than the 126 MB L2, so no
+  flush is needed), CUDA events on the launching stream, max over ranks.
+* e2e: the same steps through the host-buffer C-ABI entry points
+  (lc_ntt_forward_host / lc_ntt_inverse_host) from pinned host memory,
+  host<->device copies inside the timed region.
+* roofline: the forward NTT kernel, algorithmic bytes 8 B per coefficient per
+  launch (4 B read + 4 B written) over its CUDA-event duration, against the
+  measured HBM copy bandwidth.
+* cpu_baseline: the oracle restatement of the reference's forward_fast /
+  inverse_fast on this host's cores (a bounded sample).
+* --impl reference: the reference's CPU path (its scalar algorithm restated in
+  C, the Rust reference cannot be built here) on all host threads, same
+  metric and unit.
+Multi-GPU: every rank runs the full per-GPU workload on its own device (weak
+scaling); no collective touches the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Ajtai commit ring-elems/s & NTT coeffs/s; batched+IMMA vs plain GPU, bit-exact"
+UNIT = "coeffs/s"
+LOG_N = 8
+COUNT = 1 << 16
+CRT = ((1073738753, 10, 3), (1073732609, 10, 3), (1073731073, 9, 3), (1073726977, 9, 5))
+WORKLOAD = "NTT round trip: 2^16 polys x d=256 x 4 CRT primes (30-bit, q=1 mod 512), u32"
+COEFFS = COUNT * (1 << LOG_N) * len(CRT)       # residues per transform
+TRANSFORMS_PER_STEP = 2                         # forward + inverse
+ALG_BYTES_PER_LAUNCH = COEFFS * 8               # 4 B read + 4 B write per residue
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ CPU legs
+
+def cpu_ntt_rate(polys: int, nthreads: int, reps: int = 1, native: bool = True):
+    """Oracle forward_fast + inverse_fast over `polys` x 4 primes; coeffs/s."""
+    import numpy as np
+
+    import oracle
+    from lzx_b200 import synth
+    oracle.prefer_native(native)
+    tabs, data = [], []
+    for i, (q, a, g) in enumerate(CRT):
+        tabs.append(oracle.NttTables32(oracle.Modulus32(q, a, g), LOG_N))
+        data.append(synth.synth_mod32(7, i, q, polys << LOG_N))
+    best = None
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        for t, x in zip(tabs, data):
+            t.forward_batch(x, nthreads=nthreads, inplace=True)
+            t.inverse_batch(x, nthreads=nthreads, inplace=True)
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    return TRANSFORMS_PER_STEP * polys * (1 << LOG_N) * len(CRT) / best, best
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    nt = host_threads()
+    polys = 1 << 14  # bounded sample: a quarter of the per-GPU batch per step
+    for _ in range(max(args.warmup, 1)):
+        cpu_ntt_rate(polys, nt)
+    times = []
+    for _ in range(args.steps):
+        _, dt = cpu_ntt_rate(polys, nt)
+        times.append(dt)
+    total = sum(times)
+    value = TRANSFORMS_PER_STEP * polys * (1 << LOG_N) * len(CRT) * args.steps / total
+    sample = (f"{polys} polys x d=256 x 4 primes (1/4 of the per-GPU batch) forward+inverse per "
+              f"step, {nt} threads")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded counter-based residues)",
+        "config": {"workload": WORKLOAD, "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nt, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        import tempfile
+        fd, self.path = tempfile.mkstemp(prefix="clk", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", self.gpu_id, f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9 and parts[1].isdigit():
+                    rows.append(parts)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.remove(self.path)
+            except Exception:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [int(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": int(rows[0][2]),
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max(float(r[3]) for r in rows if r[3].replace('.', '', 1).isdigit())
+                if any(r[3].replace('.', '', 1).isdigit() for r in rows) else None}
+
+
+# ------------------------------------------------------------------ our arm
+
+def run_ours(args):
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from lzx_b200 import CRT_SET_30BIT, NttTables, _lib, synth
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    L = _lib.lib()
+    plan = NttTables(CRT_SET_30BIT, LOG_N)
+    host = synth.crt_batch(1234 + rank, CRT_SET_30BIT, COUNT, 1 << LOG_N)
+    x = torch.from_numpy(host.view(np.int32)).cuda()
+    y = torch.empty_like(x)
+    z = torch.empty_like(x)
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+    h = plan.handle
+    xp, yp, zp = C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), C.c_void_p(z.data_ptr())
+
+    def step():
+        st = L.lc_ntt_forward(h, xp, yp, COUNT, sp)
+        st |= L.lc_ntt_inverse(h, yp, zp, COUNT, sp)
+        return st
+
+    for _ in range(max(args.warmup, 1)):
+        assert step() == 0
+    torch.cuda.synchronize()
+    assert torch.equal(z, x), "round trip mismatch"
+
+    K = args.steps
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(K)]
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    props = torch.cuda.get_device_properties(local)
+    gpu_id = f"GPU-{props.uuid}" if getattr(props, "uuid", None) else str(local)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(gpu_id) as clk:
+        start.record(stream)
+        for k in range(K):
+            ev[k][0].record(stream)
+            L.lc_ntt_forward(h, xp, yp, COUNT, sp)
+            ev[k][1].record(stream)
+            L.lc_ntt_inverse(h, yp, zp, COUNT, sp)
+            ev[k][2].record(stream)
+        end.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    assert L.lc_ntt_plan_check(h, sp) == 0
+    assert torch.equal(z, x)
+    ms_local = start.elapsed_time(end)
+    fwd_ms = [ev[k][0].elapsed_time(ev[k][1]) for k in range(K)]
+    inv_ms = [ev[k][1].elapsed_time(ev[k][2]) for k in range(K)]
+    ms = max_over_ranks(ms_local)
+    value = world * TRANSFORMS_PER_STEP * COEFFS * K / (ms / 1e3)
+    clocks = clk.summary()
+
+    # ---- end to end through the host-buffer entry points (pinned memory)
+    KE = args.e2e_steps if args.e2e_steps is not None else max(3, min(K, 10))
+    hin = torch.from_numpy(host.view(np.int32).copy()).pin_memory()
+    hmid = torch.empty_like(hin).pin_memory()
+    hout = torch.empty_like(hin).pin_memory()
+    hi, hm, ho = (C.c_void_p(t.data_ptr()) for t in (hin, hmid, hout))
+    for _ in range(2):
+        assert L.lc_ntt_forward_host(h, hi, hm, COUNT) == 0
+        assert L.lc_ntt_inverse_host(h, hm, ho, COUNT) == 0
+    assert torch.equal(hout, hin)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(KE):
+        L.lc_ntt_forward_host(h, hi, hm, COUNT)
+        L.lc_ntt_inverse_host(h, hm, ho, COUNT)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    assert torch.equal(hout, hin)
+    e2e_value = world * TRANSFORMS_PER_STEP * COEFFS * KE / e2e_s
+
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+
+    peak, peak_kind = peaks()
+    fwd_avg = statistics.mean(fwd_ms)
+    inv_avg = statistics.mean(inv_ms)
+    achieved = ALG_BYTES_PER_LAUNCH / (fwd_avg / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "ntt_crt4_d256_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get("forward_bytes_per_launch")
+    roofline = {
+        "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "frac": achieved / peak, "traffic": traffic,
+        "kernel": "ntt_tile_kernel<ShoupLazy, log_n=8, log_v=4> forward",
+        "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, copy)",
+        "algorithmic_bytes_per_launch": ALG_BYTES_PER_LAUNCH,
+        "kernel_ms": {"forward": fwd_avg, "inverse": inv_avg},
+        "inverse_achieved_gbs": ALG_BYTES_PER_LAUNCH / (inv_avg / 1e3) / 1e9,
+    }
+
+    cpu = None
+    if not args.no_cpu_baseline:
+        nt = host_threads()
+        polys = 1 << 14
+        rate_all, dt_all = cpu_ntt_rate(polys, nt, reps=2)
+        rate_one, dt_one = cpu_ntt_rate(1 << 11, 1, reps=1)
+        cpu = {"value": rate_all, "unit": UNIT, "cores": nt, "kind": "port",
+               "sample": f"{polys} polys x d=256 x 4 primes forward+inverse, oracle restatement "
+                         f"of ntt.rs forward_fast/inverse_fast, {nt} threads",
+               "single_thread": {"value": rate_one, "cores": 1,
+                                 "sample": f"{1 << 11} polys x d=256 x 4 primes"}}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded counter-based residues, uniform mod q)",
+        "config": {"workload": WORKLOAD, "polys_per_gpu": COUNT, "d": 1 << LOG_N,
+                   "moduli": [c[0] for c in CRT], "transforms_per_step": 2,
+                   "l2": "inputs 256 MiB per transform > 126 MB L2 (no flush)",
+                   "parallelism": f"replicated per GPU x{world}"},
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": UNIT,
+                "h2d_bytes_per_step": 2 * COEFFS * 4, "d2h_bytes_per_step": 2 * COEFFS * 4,
+                "steps": KE, "api": "lc_ntt_forward_host + lc_ntt_inverse_host, pinned host memory"},
+        "gpu_launches": 2 * K,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

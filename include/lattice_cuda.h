@@ -1,0 +1,111 @@
+/*
+ * lattice_cuda.h -- C ABI of the B200 (sm_100a) commitment hot path of LZX.
+ *
+ * Drop-in GPU backend for the negacyclic NTT over Z_q[X]/(X^n+1) and the Ajtai
+ * commitment c = A.w of idrees2516/lzx (Rust crates lattice-ring and
+ * lattice-commitment).  Every result is an exact residue, bit-identical to the
+ * reference's scalar code.  Plain C types only: pointers, sizes, status codes.
+ *
+ * Conventions
+ *   - Ring degree n = 2^log_n.  A batch of polynomials is coefficient-
+ *     contiguous and element-major ([count][n]); a plan with several u32
+ *     moduli (a CRT set) takes [modulus][count][n].
+ *   - u32 plans hold residues as uint32_t in [0,q); Goldilocks plans as
+ *     uint64_t in [0,p), p = 2^64 - 2^32 + 1.  Inputs must be canonical.
+ *   - "Device" entry points take device pointers (16-byte aligned) and an
+ *     optional cudaStream_t (NULL = legacy default stream); they only enqueue
+ *     work.  "Host" entry points take host pointers, are synchronous and move
+ *     the data themselves.
+ *   - Status codes map 1:1 onto the reference's error enums where one exists
+ *     (NttError, lattice-ring/src/ntt.rs:38-42; RingError, ring.rs:17-21;
+ *     AjtaiError, lattice-commitment/src/ajtai.rs:43-49).  No entry point
+ *     aborts or prints.
+ *   - There is no CPU fallback: without a usable sm_100 device every compute
+ *     entry point returns LC_ERR_NO_DEVICE.
+ */
+#ifndef LATTICE_CUDA_H
+#define LATTICE_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LC_API __attribute__((visibility("default")))
+
+typedef enum lc_status {
+  LC_OK = 0,
+  LC_ERR_LENGTH_MISMATCH = 1,     /* NttError::LengthMismatch (ntt.rs:40), RingError::LengthMismatch (ring.rs:20) */
+  LC_ERR_ADICITY_TOO_SMALL = 2,   /* NttError::AdicityTooSmall (ntt.rs:41) */
+  LC_ERR_DIMENSION_MISMATCH = 3,  /* AjtaiError::DimensionMismatch (ajtai.rs:45) */
+  LC_ERR_NORM_EXCEEDED = 4,       /* AjtaiError::NormExceeded (ajtai.rs:46) */
+  LC_ERR_COMMITMENT_MISMATCH = 5, /* AjtaiError::CommitmentMismatch (ajtai.rs:47) */
+  LC_ERR_NON_CANONICAL = 6,       /* RingElement::from_bytes rejection (ring.rs:394-400) */
+  LC_ERR_INVALID_ARGUMENT = 7,    /* null/misaligned pointer, bad modulus, bad sizes */
+  LC_ERR_UNSUPPORTED = 8,         /* valid in the reference but not built here (e.g. log_n) */
+  LC_ERR_CUDA = 9,                /* a CUDA runtime call failed */
+  LC_ERR_OUT_OF_MEMORY = 10,
+  LC_ERR_TIMEOUT = 11,            /* a bounded device-side wait expired */
+  LC_ERR_NO_DEVICE = 12           /* no sm_100 device available */
+} lc_status;
+
+typedef void *lc_stream; /* cudaStream_t */
+
+typedef struct lc_ntt_plan lc_ntt_plan;
+
+/* Library version ("major.minor.patch") and a static string for a status. */
+LC_API const char *lc_version(void);
+LC_API const char *lc_status_string(int status);
+/* 1 when a CUDA device of compute capability 10.x is usable, else 0. */
+LC_API int lc_device_available(void);
+
+/* ------------------------------------------------------------------------
+ * NTT plans.  Replace NttTables::new(Modulus32, log_n)
+ * (lattice-ring/src/ntt.rs:46-106): psi = g^((q-1) >> (log_n+1)) exactly as
+ * Modulus32::root_of_unity_order_2n (modulus.rs:149-161).  The plan keeps
+ * its twiddle tables resident on the current device.
+ *   - lc_ntt_plan_create_u32: num_moduli (1..8) u32 primes sharing log_n;
+ *     q odd, 2 < q < 2^32; returns LC_ERR_ADICITY_TOO_SMALL when
+ *     log_n + 1 > two_adicity (ntt.rs:47-50) and LC_ERR_INVALID_ARGUMENT when
+ *     psi does not have order exactly 2n.  Supported log_n: 1..11.
+ *   - lc_ntt_plan_create_goldilocks: the same transform over Goldilocks
+ *     (lattice-core/src/field.rs), generator 7 (field.rs:195-200), log_n 1..10.
+ * ---------------------------------------------------------------------- */
+LC_API int lc_ntt_plan_create_u32(uint32_t log_n, const uint32_t *q, const uint32_t *two_adicity,
+                                  const uint32_t *generator, uint32_t num_moduli,
+                                  lc_ntt_plan **out);
+LC_API int lc_ntt_plan_create_goldilocks(uint32_t log_n, lc_ntt_plan **out);
+LC_API void lc_ntt_plan_destroy(lc_ntt_plan *plan);
+/* n, number of moduli, element size in bytes (4 or 8). */
+LC_API int lc_ntt_plan_info(const lc_ntt_plan *plan, uint32_t *log_n, uint32_t *num_moduli,
+                            uint32_t *elem_bytes);
+
+/* Batched forward transform, device pointers.  Replaces
+ * NttTables::forward_fast / RingElement::to_ntt (ntt.rs:118-146,
+ * ring.rs:344-351) applied to `count` polynomials per modulus; output in the
+ * reference's natural order out[j] = a(psi^(2j+1)).  in == out is allowed. */
+LC_API int lc_ntt_forward(const lc_ntt_plan *plan, const void *in, void *out, size_t count,
+                          lc_stream stream);
+/* Batched inverse, device pointers.  Replaces NttTables::inverse_fast /
+ * RingElement::from_ntt (ntt.rs:187-216, ring.rs:354-367). */
+LC_API int lc_ntt_inverse(const lc_ntt_plan *plan, const void *in, void *out, size_t count,
+                          lc_stream stream);
+
+/* Host-buffer variants: synchronous; copy in, transform, copy out (pipelined
+ * in chunks over two streams).  in == out is allowed.  Pinned host memory
+ * gives the full PCIe rate; pageable memory works at a lower rate. */
+LC_API int lc_ntt_forward_host(lc_ntt_plan *plan, const void *in, void *out, size_t count);
+LC_API int lc_ntt_inverse_host(lc_ntt_plan *plan, const void *in, void *out, size_t count);
+
+/* Wait for `stream`, then report (and clear) any device-side error recorded
+ * by this plan's kernels since the last check (LC_ERR_TIMEOUT), or a pending
+ * CUDA error (LC_ERR_CUDA). */
+LC_API int lc_ntt_plan_check(lc_ntt_plan *plan, lc_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LATTICE_CUDA_H */

@@ -1,0 +1,187 @@
+// arith.cuh -- exact modular arithmetic for the NTT butterflies (device side).
+//
+// Three policies share one interface so that one kernel template serves every
+// modulus family of the reference's NTT (lattice-ring/src/ntt.rs) :
+//
+//   ShoupLazy  : u32 primes q < 2^30 (the CRT set).  Harvey butterflies with
+//                operands kept lazily in [0,4q) (forward) / [0,2q) (inverse);
+//                twiddle products by Shoup's method with a precomputed
+//                floor(w*2^32/q).  4q < 2^32, so nothing overflows.
+//   MontCanon  : any odd u32 prime (Modulus32::Q_32 = 3*2^30+1 has no lazy
+//                headroom).  Signed Montgomery reduction with R = 2^32 and
+//                twiddles stored as w*R mod q; every value stays in [0,q).
+//   Goldilocks : p = 2^64 - 2^32 + 1 with 2^64 == 2^32 - 1 folding
+//                (lattice-core/src/field.rs:38-55); values in [0,p).
+//
+// All three return canonical residues, so the transforms are bit-identical to
+// the reference's Barrett / u128 arithmetic (ntt.rs:118-216).
+#pragma once
+
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace lc {
+
+// ------------------------------------------------------------- u32, lazy
+
+struct ShoupLazy {
+  using T = uint32_t;
+  using Tw = uint2;  // {w, floor(w * 2^32 / q)}
+  uint32_t q, q2;
+
+  LC_D explicit ShoupLazy(uint32_t q_) : q(q_), q2(2 * q_) {}
+
+  // a*w mod q in [0, 2q) for any a < 2^32 (q < 2^31).
+  LC_D uint32_t mulw(uint32_t a, Tw w) const {
+    uint32_t qh = __umulhi(a, w.y);
+    return a * w.x - qh * q;
+  }
+  // Cooley-Tukey (forward) butterfly: X,Y in [0,4q) -> [0,4q).
+  LC_D void fwd(uint32_t& x, uint32_t& y, Tw w) const {
+    uint32_t X = min(x, x - q2);  // [0,2q)
+    uint32_t t = mulw(y, w);      // [0,2q)
+    x = X + t;
+    y = X - t + q2;
+  }
+  // Gentleman-Sande (inverse) butterfly: X,Y in [0,2q) -> [0,2q).
+  LC_D void inv(uint32_t& x, uint32_t& y, Tw w) const {
+    uint32_t s = x + y;
+    uint32_t d = x - y + q2;
+    x = min(s, s - q2);
+    y = mulw(d, w);
+  }
+  // Last inverse level fused with the n^{-1} scaling: X,Y in [0,2q).
+  LC_D void inv_last(uint32_t& x, uint32_t& y, Tw ninv, Tw wninv) const {
+    uint32_t s = x + y;        // [0,4q)
+    uint32_t d = x - y + q2;   // (0,4q)
+    x = mulw(s, ninv);
+    y = mulw(d, wninv);
+  }
+  LC_D void scale(uint32_t& x, Tw c) const { x = mulw(x, c); }
+  LC_D uint32_t fwd_final(uint32_t x) const {
+    x = min(x, x - q2);
+    return min(x, x - q);
+  }
+  LC_D uint32_t inv_final(uint32_t x) const { return min(x, x - q); }
+};
+
+// ------------------------------------------------------------- u32, canonical Montgomery
+
+struct MontCanon {
+  using T = uint32_t;
+  using Tw = uint2;  // {w * 2^32 mod q, unused}
+  uint32_t q, qinv;  // qinv = q^{-1} mod 2^32
+
+  LC_D MontCanon(uint32_t q_, uint32_t qinv_) : q(q_), qinv(qinv_) {}
+
+  // a * wR * 2^-32 mod q, canonical, for a, wR < q.
+  LC_D uint32_t mont(uint32_t a, uint32_t wR) const {
+    uint64_t t = (uint64_t)a * wR;
+    uint32_t m = (uint32_t)t * qinv;
+    uint32_t th = (uint32_t)(t >> 32);
+    uint32_t mh = __umulhi(m, q);
+    uint32_t r = th - mh;
+    return th < mh ? r + q : r;
+  }
+  LC_D uint32_t add(uint32_t a, uint32_t b) const {
+    uint32_t s = a + b;
+    return (s < a || s >= q) ? s - q : s;
+  }
+  LC_D uint32_t sub(uint32_t a, uint32_t b) const {
+    uint32_t d = a - b;
+    return a < b ? d + q : d;
+  }
+  LC_D void fwd(uint32_t& x, uint32_t& y, Tw w) const {
+    uint32_t t = mont(y, w.x);
+    uint32_t X = x;
+    x = add(X, t);
+    y = sub(X, t);
+  }
+  LC_D void inv(uint32_t& x, uint32_t& y, Tw w) const {
+    uint32_t X = x, Y = y;
+    x = add(X, Y);
+    y = mont(sub(X, Y), w.x);
+  }
+  LC_D void inv_last(uint32_t& x, uint32_t& y, Tw ninv, Tw wninv) const {
+    uint32_t X = x, Y = y;
+    x = mont(add(X, Y), ninv.x);
+    y = mont(sub(X, Y), wninv.x);
+  }
+  LC_D void scale(uint32_t& x, Tw c) const { x = mont(x, c.x); }
+  LC_D uint32_t fwd_final(uint32_t x) const { return x; }
+  LC_D uint32_t inv_final(uint32_t x) const { return x; }
+};
+
+// ------------------------------------------------------------- Goldilocks
+
+constexpr uint64_t kGlP = 0xFFFFFFFF00000001ull;
+constexpr uint64_t kGlEps = 0xFFFFFFFFull;  // 2^64 mod p
+
+// 128-bit product a*b as (hi, lo).
+LC_D void mul64x64(uint64_t a, uint64_t b, uint64_t& hi, uint64_t& lo) {
+  lo = a * b;
+  hi = __umul64hi(a, b);
+}
+
+// Reduce hi*2^64 + lo into [0, 2^64) (congruent mod p, not yet canonical):
+// hi = hh*2^32 + hl, 2^64 == 2^32-1, 2^96 == -1.
+LC_D uint64_t gl_reduce128_lazy(uint64_t hi, uint64_t lo) {
+  uint32_t hh = (uint32_t)(hi >> 32);
+  uint32_t hl = (uint32_t)hi;
+  uint64_t t0 = lo - hh;
+  if (lo < hh) t0 -= kGlEps;                  // borrowed 2^64 == 2^32-1
+  uint64_t t1 = ((uint64_t)hl << 32) - hl;    // hl * (2^32-1)
+  uint64_t r = t0 + t1;
+  if (r < t1) r += kGlEps;                    // carried 2^64 == 2^32-1
+  return r;
+}
+
+LC_D uint64_t gl_canon(uint64_t x) { return x >= kGlP ? x - kGlP : x; }
+
+LC_D uint64_t gl_mul(uint64_t a, uint64_t b) {
+  uint64_t hi, lo;
+  mul64x64(a, b, hi, lo);
+  return gl_canon(gl_reduce128_lazy(hi, lo));
+}
+
+// Canonical inputs -> canonical output.
+LC_D uint64_t gl_add(uint64_t a, uint64_t b) {
+  uint64_t s = a + b;
+  if (s < a) s += kGlEps;  // cannot carry again for a, b < p
+  return gl_canon(s);
+}
+
+LC_D uint64_t gl_sub(uint64_t a, uint64_t b) {
+  uint64_t d = a - b;
+  if (a < b) d -= kGlEps;  // == d + p (mod 2^64)
+  return d;                // a, b < p  =>  result < p
+}
+
+struct Goldilocks {
+  using T = uint64_t;
+  using Tw = uint64_t;
+
+  LC_D Goldilocks() {}
+  LC_D void fwd(uint64_t& x, uint64_t& y, Tw w) const {
+    uint64_t t = gl_mul(y, w);
+    uint64_t X = x;
+    x = gl_add(X, t);
+    y = gl_sub(X, t);
+  }
+  LC_D void inv(uint64_t& x, uint64_t& y, Tw w) const {
+    uint64_t X = x, Y = y;
+    x = gl_add(X, Y);
+    y = gl_mul(gl_sub(X, Y), w);
+  }
+  LC_D void inv_last(uint64_t& x, uint64_t& y, Tw ninv, Tw wninv) const {
+    uint64_t X = x, Y = y;
+    x = gl_mul(gl_add(X, Y), ninv);
+    y = gl_mul(gl_sub(X, Y), wninv);
+  }
+  LC_D void scale(uint64_t& x, Tw c) const { x = gl_mul(x, c); }
+  LC_D uint64_t fwd_final(uint64_t x) const { return x; }
+  LC_D uint64_t inv_final(uint64_t x) const { return x; }
+};
+
+}  // namespace lc

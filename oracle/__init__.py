@@ -135,9 +135,21 @@ def _declare(lib):
     return lib
 
 
+_prefer_native = False
+
+
+def prefer_native(flag: bool = True) -> None:
+    """Route every oracle call through a copy built with -march=native (for timing)."""
+    global _prefer_native
+    if flag:
+        lib(native=True)
+    _prefer_native = flag
+
+
 def lib(native: bool = False):
     """The oracle shared library (built on first use)."""
     global _lib, _native
+    native = native or _prefer_native
     with _lock:
         if native:
             if _native is None:

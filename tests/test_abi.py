@@ -1,0 +1,74 @@
+"""CPU-side checks of the C ABI: the library builds, loads and exports every
+entry point declared in include/*.h; host-side validation behaves like the
+reference's error enums without touching a GPU."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import pytest
+
+import lzx_b200
+from lzx_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_library_exports_every_declared_symbol():
+    declared = _lib.declared_functions()
+    assert "lc_ntt_forward" in declared and "lc_ntt_plan_create_u32" in declared
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True,
+                         text=True, check=True).stdout
+    exported = set(re.findall(r"\bT (lc_\w+)", out))
+    missing = [f for f in declared if f not in exported]
+    assert not missing, missing
+    L = _lib.lib()
+    for f in declared:
+        assert hasattr(L, f)
+
+
+def test_build_targets_sm100a_only():
+    from lzx_b200 import build
+    assert "arch=compute_100a,code=sm_100a" in build.NVCC_FLAGS
+    assert build.up_to_date(), "in-tree library is older than its sources"
+
+
+def test_status_strings_and_version():
+    L = _lib.lib()
+    assert L.lc_version() == lzx_b200.__version__.encode()
+    assert L.lc_status_string(0) == b"ok"
+    assert L.lc_status_string(_lib.LC_ERR_ADICITY_TOO_SMALL) == b"adicity too small"
+    assert L.lc_status_string(12345) == b"unknown status"
+
+
+def test_host_validation_precedes_device():
+    """NttTables::new rejects log_n + 1 > adicity (ntt.rs:47-50) before any device work."""
+    with pytest.raises(lzx_b200.NttError) as e:
+        lzx_b200.NttTables(lzx_b200.Modulus32.Q_12289, 12)
+    assert e.value.kind == "AdicityTooSmall"
+    with pytest.raises(lzx_b200.NttError):
+        lzx_b200.NttTables(lzx_b200.CRT_SET_30BIT, 10)  # adicity 9 and 10 primes
+    L = _lib.lib()
+    h = C.c_void_p()
+    arr = lambda *xs: (C.c_uint32 * len(xs))(*xs)
+    assert L.lc_ntt_plan_create_u32(8, arr(4), arr(30), arr(3), 1, C.byref(h)) == \
+        _lib.LC_ERR_INVALID_ARGUMENT  # even modulus
+    assert L.lc_ntt_plan_create_u32(8, arr(12289), arr(12), arr(11), 0, C.byref(h)) == \
+        _lib.LC_ERR_INVALID_ARGUMENT  # no moduli
+    assert L.lc_ntt_plan_create_goldilocks(32, C.byref(h)) == _lib.LC_ERR_ADICITY_TOO_SMALL
+    assert L.lc_ntt_forward(None, None, None, 1, None) == _lib.LC_ERR_INVALID_ARGUMENT
+
+
+def test_no_cpu_fallback_without_gpu():
+    L = _lib.lib()
+    if L.lc_device_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(lzx_b200.LatticeCudaError) as e:
+        lzx_b200.NttTables(lzx_b200.Modulus32.Q_32, 8)
+    assert e.value.status == _lib.LC_ERR_NO_DEVICE
+
+
+def test_header_cites_reference_interfaces():
+    src = open(os.path.join(ROOT, "include", "lattice_cuda.h")).read()
+    for cite in ("ntt.rs:46-106", "ntt.rs:118-146", "ntt.rs:187-216", "ntt.rs:38-42"):
+        assert cite in src

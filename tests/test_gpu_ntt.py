@@ -1,0 +1,198 @@
+"""GPU parity of the batched NTT/INTT against the CPU oracle (bit-exact).
+
+Re-runs the reference's NTT tests (lattice-ring/src/ntt.rs:364-479,
+ring.rs:485-568) on the CUDA path, checks the golden vectors, every modulus
+family and ring degree the kernels build, the edge values, and the full-size
+CRT batch (2^16 polynomials x 4 primes x d=256) through size-independent
+properties plus a sampled oracle comparison.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle
+from lzx_b200 import (CRT_SET_30BIT, GoldilocksNttTables, Modulus32, NttError, NttTables, RingConfig,
+                      RingElement, _lib)
+from lzx_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _need_gpu():
+    if not torch.cuda.is_available() or not _lib.lib().lc_device_available():
+        pytest.fail("GPU tests need an sm_100 device and the CUDA library")
+
+
+def ora_tables(m: Modulus32, log_n):
+    return oracle.NttTables32(oracle.Modulus32(m.q, m.two_adicity, m.generator), log_n)
+
+
+def to_dev(a: np.ndarray):
+    if a.dtype == np.uint32:
+        return torch.from_numpy(a.view(np.int32)).cuda()
+    return torch.from_numpy(a.view(np.int64)).cuda()
+
+
+def from_dev(t, dtype):
+    return t.cpu().numpy().view(dtype)
+
+
+MODULI = [Modulus32.Q_32, Modulus32.Q_12289, Modulus32.Q_2013265921, CRT_SET_30BIT[0],
+          CRT_SET_30BIT[3]]
+
+
+@pytest.mark.parametrize("m", MODULI, ids=lambda m: str(m.q))
+@pytest.mark.parametrize("log_n", list(range(1, 12)))
+def test_u32_forward_inverse_match_oracle(m, log_n):
+    if log_n + 1 > m.two_adicity:
+        with pytest.raises(NttError):
+            NttTables(m, log_n)
+        return
+    n, count = 1 << log_n, 37
+    a = synth.synth_mod32(100 + log_n, 1, m.q, count * n).reshape(count, n)
+    t = NttTables(m, log_n)
+    ot = ora_tables(m, log_n)
+    want = ot.forward_batch(a)
+    dev = to_dev(a.copy())
+    t.forward_fast(dev)
+    torch.cuda.synchronize()
+    got = from_dev(dev, np.uint32)
+    assert np.array_equal(got, want)
+    t.inverse_fast(dev)
+    torch.cuda.synchronize()
+    assert np.array_equal(from_dev(dev, np.uint32), a)
+    # inverse of arbitrary (non-image) input equals the oracle's inverse_fast
+    b = synth.synth_mod32(200 + log_n, 2, m.q, count * n).reshape(count, n)
+    assert np.array_equal(t.inverse_fast(b.copy()), ot.inverse_batch(b))
+
+
+@pytest.mark.parametrize("log_n", list(range(1, 11)))
+def test_goldilocks_forward_inverse_match_oracle(log_n):
+    n, count = 1 << log_n, 33
+    a = synth.synth_gl(300 + log_n, 1, count * n).reshape(count, n)
+    t = GoldilocksNttTables(log_n)
+    ot = oracle.NttTablesGl(log_n)
+    want = ot.forward_batch(a)
+    got = t.forward_fast(a.copy())
+    assert np.array_equal(got, want)
+    assert np.array_equal(t.inverse_fast(got.copy()), a)
+    b = synth.synth_gl(400 + log_n, 2, count * n).reshape(count, n)
+    assert np.array_equal(t.inverse_fast(b.copy()), ot.inverse_batch(b))
+
+
+def test_golden_vectors(golden):
+    for v in golden["ntt_q32_kat_manifest"] + golden["ntt_q32_extra"]:
+        t = NttTables(Modulus32.Q_32, v["log_n"])
+        a = np.array(v["input"], dtype=np.uint32)
+        assert t.forward_fast(a.copy()).tolist() == v["forward"]
+    for v in golden["ntt_crt"]:
+        t = NttTables(Modulus32(v["q"], v["two_adicity"], v["generator"]), v["log_n"])
+        a = np.array(v["input"], dtype=np.uint32)
+        assert t.forward_fast(a.copy()).tolist() == v["forward"]
+    for v in golden["ntt_goldilocks"]:
+        t = GoldilocksNttTables(v["log_n"])
+        a = np.array([int(x) for x in v["input"]], dtype=np.uint64)
+        assert [str(x) for x in t.forward_fast(a.copy()).tolist()] == v["forward"]
+
+
+def test_crt_set_layout_matches_per_prime_plans():
+    """A 4-prime plan on [prime][count][n] equals four single-prime transforms."""
+    count, n = 513, 256
+    a = synth.crt_batch(5, CRT_SET_30BIT, count, n)
+    t = NttTables(CRT_SET_30BIT, 8)
+    got = t.forward_fast(a.copy())
+    for i, m in enumerate(CRT_SET_30BIT):
+        assert np.array_equal(got[i], ora_tables(m, 8).forward_batch(a[i]))
+    assert np.array_equal(t.inverse_fast(got.copy()), a)
+
+
+@pytest.mark.parametrize("m", [Modulus32.Q_32, CRT_SET_30BIT[1]], ids=lambda m: str(m.q))
+def test_edge_values(m):
+    """Zeros, q-1 everywhere (lazy-reduction extremes), impulses, count 0 and 1."""
+    log_n, n = 8, 256
+    t = NttTables(m, log_n)
+    ot = ora_tables(m, log_n)
+    cases = np.stack([np.zeros(n, np.uint32), np.full(n, m.q - 1, np.uint32),
+                      np.eye(n, dtype=np.uint32)[0], np.eye(n, dtype=np.uint32)[n - 1],
+                      np.full(n, 1, np.uint32)])
+    assert np.array_equal(t.forward_fast(cases.copy()), ot.forward_batch(cases))
+    assert np.array_equal(t.inverse_fast(cases.copy()), ot.inverse_batch(cases))
+    one = cases[1:2].copy()
+    assert np.array_equal(t.forward_fast(one), ot.forward_batch(cases[1:2]))
+    empty = np.zeros((0, n), np.uint32)
+    assert t.forward_fast(empty).shape == (0, n)
+
+
+def test_length_mismatch_and_alignment():
+    t = NttTables(Modulus32.Q_32, 8)
+    with pytest.raises(NttError) as e:
+        t.forward_fast(np.zeros(128, np.uint32))  # ntt.rs:469-479
+    assert e.value.kind == "LengthMismatch"
+    buf = torch.zeros(256 * 4 + 1, dtype=torch.int32, device="cuda")
+    L = _lib.lib()
+    st = L.lc_ntt_forward(t.handle, C.c_void_p(buf.data_ptr() + 4), C.c_void_p(buf.data_ptr() + 4),
+                          4, None)
+    assert st == _lib.LC_ERR_INVALID_ARGUMENT
+
+
+def test_out_of_place_device_and_host_agree():
+    count, n = 1000, 256
+    a = synth.crt_batch(9, CRT_SET_30BIT, count, n)
+    t = NttTables(CRT_SET_30BIT, 8)
+    src = to_dev(a.copy())
+    dst = torch.empty_like(src)
+    t.forward_fast(src, out=dst)
+    torch.cuda.synchronize()
+    host = t.forward_fast(a.copy())
+    assert np.array_equal(from_dev(dst, np.uint32).reshape(host.shape), host)
+    assert np.array_equal(from_dev(src, np.uint32).reshape(a.shape), a)  # input untouched
+    assert _lib.lib().lc_ntt_plan_check(t.handle, None) == 0
+
+
+def test_full_size_crt_round_trip_and_samples():
+    """2^16 polynomials x d=256 x 4 primes: the bench workload."""
+    count, n = 1 << 16, 256
+    a = synth.crt_batch(2024, CRT_SET_30BIT, count, n)
+    t = NttTables(CRT_SET_30BIT, 8)
+    dev = to_dev(a.copy())
+    t.forward_fast(dev)
+    torch.cuda.synchronize()
+    fwd = from_dev(dev, np.uint32).reshape(a.shape)
+    rng = np.random.default_rng(1)
+    idx = np.sort(rng.choice(count, 1024, replace=False))
+    idx = np.unique(np.concatenate([idx, [0, count - 1]]))
+    for i, m in enumerate(CRT_SET_30BIT):
+        assert np.array_equal(fwd[i, idx], ora_tables(m, 8).forward_batch(a[i, idx]))
+    # linearity: NTT(a + b) == NTT(a) + NTT(b) on the whole batch
+    b = synth.crt_batch(77, CRT_SET_30BIT, count, n)
+    qs = np.array([m.q for m in CRT_SET_30BIT], dtype=np.uint64)[:, None, None]
+    s = ((a.astype(np.uint64) + b) % qs).astype(np.uint32)
+    fb = t.forward_fast(b.copy())
+    fs = t.forward_fast(s.copy())
+    assert np.array_equal(fs, ((fwd.astype(np.uint64) + fb) % qs).astype(np.uint32))
+    t.inverse_fast(dev)
+    torch.cuda.synchronize()
+    assert np.array_equal(from_dev(dev, np.uint32).reshape(a.shape), a)
+    assert _lib.lib().lc_ntt_plan_check(t.handle, None) == 0
+
+
+def test_ring_element_api():
+    """ring.rs:485-568 on the GPU-backed ring."""
+    c = RingConfig(Modulus32.Q_32, 6)
+    a = c.random(b"m-a")
+    assert a.mul(c.one()) == a
+    assert a.mul(c.zero()).is_zero()
+    x_nm1 = RingElement.from_coeffs(c, np.eye(c.n(), dtype=np.uint32)[c.n() - 1])
+    assert c.x_gen().mul(x_nm1) == c.constant(c.modulus.q - 1)
+    b = c.random(b"m-b")
+    om = oracle.Modulus32(*oracle.Q_32)
+    assert np.array_equal(a.mul(b).coeffs(), ora_tables(Modulus32.Q_32, 6).ring_mul(a.coeffs(), b.coeffs()))
+    assert np.array_equal(c.random(b"m-a").coeffs(), oracle.ring_random(om, 6, b"m-a"))
+    ev = a.to_ntt()
+    assert RingElement.from_ntt(c, ev) == a
+    u = c.uniform_from_seed(b"ajtai-A", bytes([42]) * 32, 7)
+    assert np.array_equal(u.coeffs(), oracle.uniform_from_seed(om, 6, b"ajtai-A", bytes([42]) * 32, 7))
