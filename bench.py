@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--variant", type=int, default=None,
+                    help="NTT kernel variant (default: autotune on the workload)")
     return ap.parse_args()
 
 
@@ -236,6 +238,17 @@ def run_ours(args):
     h = plan.handle
     xp, yp, zp = C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), C.c_void_p(z.data_ptr())
 
+    from lzx_b200 import tune
+    if args.variant is None:
+        variant = tune.tune_ntt(plan, COUNT)
+        tuned = tune.last_results(plan, COUNT)
+        tuning = {"variant": variant, "shape": tune.VARIANT_SHAPES[variant],
+                  "forward_ms": tuned[1], "inverse_ms": tuned[2]}
+    else:
+        variant = args.variant
+        _lib.check(L.lc_ntt_plan_set_variant(h, variant), "set_variant")
+        tuning = {"variant": variant, "shape": tune.VARIANT_SHAPES[variant]}
+
     def step():
         st = L.lc_ntt_forward(h, xp, yp, COUNT, sp)
         st |= L.lc_ntt_inverse(h, yp, zp, COUNT, sp)
@@ -311,6 +324,7 @@ def run_ours(args):
         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
         "frac": achieved / peak, "traffic": traffic,
         "kernel": "ntt_tile_kernel<ShoupLazy, log_n=8, log_v=4> forward",
+        "tuning": tuning,
         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, copy)",
         "algorithmic_bytes_per_launch": ALG_BYTES_PER_LAUNCH,
         "kernel_ms": {"forward": fwd_avg, "inverse": inv_avg},

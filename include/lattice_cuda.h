@@ -82,6 +82,12 @@ LC_API void lc_ntt_plan_destroy(lc_ntt_plan *plan);
 LC_API int lc_ntt_plan_info(const lc_ntt_plan *plan, uint32_t *log_n, uint32_t *num_moduli,
                             uint32_t *elem_bytes);
 
+/* Tuning hook (no counterpart in the reference, which has no kernels): picks
+ * one of the instantiated tile shapes / pipeline depths of this plan's
+ * transform kernels, 0 = the default.  Results are identical for every
+ * variant; only the speed changes.  LC_ERR_INVALID_ARGUMENT outside 0..4. */
+LC_API int lc_ntt_plan_set_variant(lc_ntt_plan *plan, int variant);
+
 /* Batched forward transform, device pointers.  Replaces
  * NttTables::forward_fast / RingElement::to_ntt (ntt.rs:118-146,
  * ring.rs:344-351) applied to `count` polynomials per modulus; output in the

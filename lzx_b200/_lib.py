@@ -65,6 +65,7 @@ def _declare(L):
         "lc_ntt_forward_host": (i32, [P, P, P, sz]),
         "lc_ntt_inverse_host": (i32, [P, P, P, sz]),
         "lc_ntt_plan_check": (i32, [P, P]),
+        "lc_ntt_plan_set_variant": (i32, [P, i32]),
     }
     optional = {
     }

@@ -68,6 +68,7 @@ struct lc_ntt_plan {
   uint32_t tw_inv_entries = 0;
   uint32_t tw_bytes = 0;
   uint32_t* d_err = nullptr;
+  int variant = 0;
   lc::HostPipeline staging;
 };
 

@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <mutex>
 #include <new>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/lattice_cuda.h"
@@ -128,29 +129,61 @@ int map_cuda(cudaError_t e) {
 
 // ---------------------------------------------------------------- launch
 
-template <class A, int LOG_N, int LOG_V, bool INV>
-static int launch_tile(const NttParams& p, cudaStream_t s) {
-  constexpr int NT = 256;
-  using G = Geo<LOG_N, LOG_V>;
-  using SL = Slots<A, LOG_N, LOG_V>;
-  constexpr size_t per_it = (size_t)(NT / G::T) * SL::S * sizeof(typename A::T);
-  constexpr int IT = per_it >= 36 * 1024 ? 1 : (int)((36 * 1024) / per_it);
-  using C = NttKernelCfg<A, LOG_N, LOG_V, NT, IT, INV>;
-  auto kern = ntt_tile_kernel<A, LOG_N, LOG_V, NT, IT, INV>;
+template <class A, int LOG_N, int LOG_V, int NT, int IT, int STAGES, bool INV>
+static int launch_tile_cfg(const NttParams& p, cudaStream_t s) {
+  using C = NttKernelCfg<A, LOG_N, LOG_V, NT, IT, STAGES, INV>;
+  auto kern = ntt_tile_kernel<A, LOG_N, LOG_V, NT, IT, STAGES, INV>;
   static bool attr_done = false;
   if (!attr_done) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
     if (e != cudaSuccess) return map_cuda(e);
     attr_done = true;
   }
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, C::SMEM);
+  if (e != cudaSuccess) return map_cuda(e);
+  per_sm = std::max(per_sm, 1);
   const unsigned long long ntiles = (p.count + C::P - 1) / C::P;
   const int sms = device_sm_count();
-  const unsigned long long per_sm = std::max<size_t>(1, (size_t)(200 * 1024) / C::SMEM);
   unsigned long long gx = std::min<unsigned long long>(ntiles, (unsigned long long)sms * per_sm);
   gx = std::max<unsigned long long>(gx, 1);
   dim3 grid((unsigned)gx, p.num_moduli);
   kern<<<grid, NT, C::SMEM, s>>>(p);
   return map_cuda(cudaGetLastError());
+}
+
+// Tile size: about 36 KB of polynomials per stage by default.
+template <class A, int LOG_N, int LOG_V, int NT>
+constexpr int default_it() {
+  using G = Geo<LOG_N, LOG_V>;
+  using SL = Slots<A, LOG_N, LOG_V>;
+  constexpr size_t per_it = (size_t)(NT / G::T) * SL::S * sizeof(typename A::T);
+  return per_it >= 18 * 1024 ? 1 : (int)((18 * 1024) / per_it);
+}
+
+// Ring degrees whose tile kernels are instantiated in several shapes for the
+// tuner: the CRT batch (u32, d = 256) and the commit witnesses (Goldilocks, d = 64).
+template <class A, int LOG_N>
+constexpr bool tunable() {
+  return (LOG_N == 8 && std::is_same<A, ShoupLazy>::value) ||
+         (LOG_N == 6 && std::is_same<A, Goldilocks>::value);
+}
+
+template <class A, int LOG_N, int LOG_V, bool INV>
+static int launch_tile(const NttParams& p, int variant, cudaStream_t s) {
+  if constexpr (!tunable<A, LOG_N>()) {
+    (void)variant;
+    return launch_tile_cfg<A, LOG_N, LOG_V, 256, default_it<A, LOG_N, LOG_V, 256>(), 2, INV>(p, s);
+  } else {
+  // variant 0 is the tuned default; 1..4 are alternatives kept for the tuner
+  switch (variant) {
+    case 1: return launch_tile_cfg<A, LOG_N, LOG_V, 256, 2 * default_it<A, LOG_N, LOG_V, 256>(), 1, INV>(p, s);
+    case 2: return launch_tile_cfg<A, LOG_N, LOG_V, 256, 2 * default_it<A, LOG_N, LOG_V, 256>(), 2, INV>(p, s);
+    case 3: return launch_tile_cfg<A, LOG_N, LOG_V, 128, default_it<A, LOG_N, LOG_V, 128>(), 2, INV>(p, s);
+    case 4: return launch_tile_cfg<A, LOG_N, LOG_V, 512, default_it<A, LOG_N, LOG_V, 512>(), 2, INV>(p, s);
+    default: return launch_tile_cfg<A, LOG_N, LOG_V, 256, default_it<A, LOG_N, LOG_V, 256>(), 2, INV>(p, s);
+  }
+  }
 }
 
 template <class A, int LOG_N, bool INV>
@@ -164,7 +197,7 @@ static int launch_small(const NttParams& p, cudaStream_t s) {
 }
 
 template <class A, bool INV>
-static int dispatch(int log_n, const NttParams& p, cudaStream_t s) {
+static int dispatch(int log_n, const NttParams& p, int variant, cudaStream_t s) {
   constexpr bool wide = sizeof(typename A::T) == 8;
   switch (log_n) {
     case 1: return launch_small<A, 1, INV>(p, s);
@@ -172,16 +205,16 @@ static int dispatch(int log_n, const NttParams& p, cudaStream_t s) {
     case 3: return launch_small<A, 3, INV>(p, s);
     case 4: return launch_small<A, 4, INV>(p, s);
     case 5:
-      if constexpr (wide) return launch_tile<A, 5, 3, INV>(p, s);
+      if constexpr (wide) return launch_tile<A, 5, 3, INV>(p, variant, s);
       else return launch_small<A, 5, INV>(p, s);
-    case 6: return launch_tile<A, 6, 3, INV>(p, s);
-    case 7: return launch_tile<A, 7, 4, INV>(p, s);
-    case 8: return launch_tile<A, 8, 4, INV>(p, s);
-    case 9: return launch_tile<A, 9, 5, INV>(p, s);
-    case 10: return launch_tile<A, 10, 5, INV>(p, s);
+    case 6: return launch_tile<A, 6, 3, INV>(p, variant, s);
+    case 7: return launch_tile<A, 7, 4, INV>(p, variant, s);
+    case 8: return launch_tile<A, 8, 4, INV>(p, variant, s);
+    case 9: return launch_tile<A, 9, 5, INV>(p, variant, s);
+    case 10: return launch_tile<A, 10, 5, INV>(p, variant, s);
     case 11:
       if constexpr (wide) return LC_ERR_UNSUPPORTED;
-      else return launch_tile<A, 11, 6, INV>(p, s);
+      else return launch_tile<A, 11, 6, INV>(p, variant, s);
     default: return LC_ERR_UNSUPPORTED;
   }
 }
@@ -202,13 +235,14 @@ int run_ntt(const lc_ntt_plan* plan, const void* in, void* out, size_t count, bo
   }
   p.err = plan->d_err;
   const int ln = (int)plan->log_n;
+  const int v = plan->variant;
   switch (plan->kind) {
     case PlanKind::U32Lazy:
-      return inverse ? dispatch<ShoupLazy, true>(ln, p, s) : dispatch<ShoupLazy, false>(ln, p, s);
+      return inverse ? dispatch<ShoupLazy, true>(ln, p, v, s) : dispatch<ShoupLazy, false>(ln, p, v, s);
     case PlanKind::U32Mont:
-      return inverse ? dispatch<MontCanon, true>(ln, p, s) : dispatch<MontCanon, false>(ln, p, s);
+      return inverse ? dispatch<MontCanon, true>(ln, p, v, s) : dispatch<MontCanon, false>(ln, p, v, s);
     case PlanKind::Goldilocks:
-      return inverse ? dispatch<Goldilocks, true>(ln, p, s) : dispatch<Goldilocks, false>(ln, p, s);
+      return inverse ? dispatch<Goldilocks, true>(ln, p, v, s) : dispatch<Goldilocks, false>(ln, p, v, s);
   }
   return LC_ERR_INVALID_ARGUMENT;
 }
@@ -368,6 +402,12 @@ LC_API void lc_ntt_plan_destroy(lc_ntt_plan* plan) {
   if (plan->d_err) cudaFree(plan->d_err);
   plan->staging.release();
   delete plan;
+}
+
+LC_API int lc_ntt_plan_set_variant(lc_ntt_plan* plan, int variant) {
+  if (!plan || variant < 0 || variant > 4) return LC_ERR_INVALID_ARGUMENT;
+  plan->variant = variant;
+  return LC_OK;
 }
 
 LC_API int lc_ntt_plan_info(const lc_ntt_plan* plan, uint32_t* log_n, uint32_t* num_moduli,

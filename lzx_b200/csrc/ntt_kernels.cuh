@@ -103,7 +103,7 @@ struct Slots {
   static constexpr int S = G::N + PAD;
 };
 
-template <class A, int LOG_N, int LOG_V, int NT, int IT, bool INVERSE>
+template <class A, int LOG_N, int LOG_V, int NT, int IT, int STAGES, bool INVERSE>
 struct NttKernelCfg {
   using G = Geo<LOG_N, LOG_V>;
   using SL = Slots<A, LOG_N, LOG_V>;
@@ -113,24 +113,130 @@ struct NttKernelCfg {
   static constexpr int P = GROUPS * IT;  // polynomials per tile
   static constexpr int TW_ENTRIES = INVERSE ? G::inv_entries() : G::fwd_entries();
   static constexpr size_t TW_BYTES = ((size_t)TW_ENTRIES * sizeof(Tw) + 15) / 16 * 16;
-  static constexpr size_t DATA_BYTES = (size_t)P * SL::S * sizeof(T);
-  static constexpr size_t SMEM = TW_BYTES + DATA_BYTES + 16;
+  static constexpr size_t STAGE_BYTES = (size_t)P * SL::S * sizeof(T);
+  static constexpr size_t SMEM = TW_BYTES + STAGES * STAGE_BYTES + 8 * STAGES;
   static_assert(NT % G::T == 0, "block size");
+  static_assert(STAGES == 1 || STAGES == 2, "stages");
   static_assert((SL::S * sizeof(T)) % 16 == 0, "slot alignment for bulk copies");
+  static_assert(STAGE_BYTES % 16 == 0, "stage alignment");
 };
 
-template <class A, int LOG_N, int LOG_V, int NT, int IT, bool INVERSE>
+// One polynomial held by a group of T threads: the complete forward
+// (natural coefficients -> natural evaluations) or inverse transform of the
+// shared-memory slot, in place.
+template <class A, int LOG_N, int LOG_V, bool INVERSE>
+LC_D void transform_slot(typename A::T* slot, const typename A::Tw* tw, const A& ar, uint32_t t) {
+  using G = Geo<LOG_N, LOG_V>;
+  using T = typename A::T;
+  using Tw = typename A::Tw;
+  constexpr int V = G::V, LO0 = G::LO0, TT = G::T;
+  T v[V];
+  if (!INVERSE) {
+    // ---- phase 0: natural-order coefficients, register bits [LO0, LOG_N)
+#pragma unroll
+    for (int r = 0; r < V; ++r) v[r] = slot[(r << LO0) | t];
+#pragma unroll
+    for (int b = LOG_N - 1; b >= LO0; --b) {
+      const int rb = 1 << (b - LO0);
+#pragma unroll
+      for (int r = 0; r < V; ++r) {
+        if (r & rb) continue;
+        const Tw w = tw[(1 << (LOG_N - 1 - b)) + (r >> (b + 1 - LO0))];
+        ar.fwd(v[r], v[r | rb], w);
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < V; ++r) {
+      const uint32_t idx = (r << LO0) | t;
+      slot[idx ^ ((idx >> LOG_V) & G::XM)] = v[r];
+    }
+    __syncwarp();
+    // ---- phase 1: register bits [0, LOG_V), levels b < LO0
+#pragma unroll
+    for (int r = 0; r < V; ++r) {
+      const uint32_t idx = (t << LOG_V) | r;
+      v[r] = slot[idx ^ ((idx >> LOG_V) & G::XM)];
+    }
+#pragma unroll
+    for (int b = LO0 - 1; b >= 0; --b) {
+      const int rb = 1 << b;
+#pragma unroll
+      for (int r = 0; r < V; ++r) {
+        if (r & rb) continue;
+        const Tw w = tw[G::fwd_phase1_off(b) + (r >> (b + 1)) * TT + t];
+        ar.fwd(v[r], v[r | rb], w);
+      }
+    }
+    __syncwarp();
+    // ---- output in natural order: LN index (t<<LOG_V)|r sits at brv of it
+#pragma unroll
+    for (int r = 0; r < V; ++r)
+      slot[(brv_bits(r, LOG_V) << LO0) | brv_bits(t, LO0)] = ar.fwd_final(v[r]);
+  } else {
+    // ---- phase 0: evaluations (natural order) read at bit-reversed slots,
+    //      register bits [0, LOG_V), levels b < LOG_V (per-lane twiddles)
+#pragma unroll
+    for (int r = 0; r < V; ++r) v[r] = slot[(brv_bits(r, LOG_V) << LO0) | brv_bits(t, LO0)];
+#pragma unroll
+    for (int b = 0; b < LOG_V; ++b) {
+      const int rb = 1 << b;
+#pragma unroll
+      for (int r = 0; r < V; ++r) {
+        if (r & rb) continue;
+        const Tw w = tw[G::inv_phase0_off(b) + (r >> (b + 1)) * TT + t];
+        ar.inv(v[r], v[r | rb], w);
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < V; ++r) {
+      const uint32_t idx = (t << LOG_V) | r;
+      slot[idx ^ ((idx >> LOG_V) & G::XM)] = v[r];
+    }
+    __syncwarp();
+    // ---- phase 1: register bits [LO0, LOG_N), levels b >= LOG_V (uniform twiddles)
+#pragma unroll
+    for (int r = 0; r < V; ++r) {
+      const uint32_t idx = (r << LO0) | t;
+      v[r] = slot[idx ^ ((idx >> LOG_V) & G::XM)];
+    }
+    constexpr int P1 = G::inv_phase1_off();
+#pragma unroll
+    for (int b = LOG_V; b < LOG_N; ++b) {
+      const int rb = 1 << (b - LO0);
+#pragma unroll
+      for (int r = 0; r < V; ++r) {
+        if (r & rb) continue;
+        if (b == LOG_N - 1) {
+          ar.inv_last(v[r], v[r | rb], tw[P1 + 0], tw[P1 + 1]);
+        } else {
+          const Tw w = tw[P1 + (1 << (LOG_N - 1 - b)) + (r >> (b + 1 - LO0))];
+          ar.inv(v[r], v[r | rb], w);
+        }
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < V; ++r) slot[(r << LO0) | t] = ar.inv_final(v[r]);
+  }
+}
+
+// Persistent tile loop.  STAGES == 2 double-buffers the tiles: the bulk load
+// of the next tile is in flight while the current one is transformed.
+template <class A, int LOG_N, int LOG_V, int NT, int IT, int STAGES, bool INVERSE>
 __global__ void __launch_bounds__(NT) ntt_tile_kernel(const __grid_constant__ NttParams p) {
-  using C = NttKernelCfg<A, LOG_N, LOG_V, NT, IT, INVERSE>;
+  using C = NttKernelCfg<A, LOG_N, LOG_V, NT, IT, STAGES, INVERSE>;
   using G = typename C::G;
   using T = typename C::T;
   using Tw = typename C::Tw;
-  constexpr int N = G::N, V = G::V, LO0 = G::LO0, TT = G::T, S = C::SL::S, P = C::P;
+  constexpr int N = G::N, TT = G::T, S = C::SL::S, P = C::P;
 
   extern __shared__ __align__(128) unsigned char smem_raw[];
   Tw* tw = reinterpret_cast<Tw*>(smem_raw);
   T* data = reinterpret_cast<T*>(smem_raw + C::TW_BYTES);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + C::TW_BYTES + C::DATA_BYTES);
+  uint64_t* bar =
+      reinterpret_cast<uint64_t*>(smem_raw + C::TW_BYTES + STAGES * C::STAGE_BYTES);
 
   const uint32_t mi = blockIdx.y;
   const A ar = make_arith<A>(p, mi);
@@ -144,7 +250,7 @@ __global__ void __launch_bounds__(NT) ntt_tile_kernel(const __grid_constant__ Nt
     for (int i = tid; i < C::TW_ENTRIES; i += NT) tw[i] = src[i];
   }
   if (tid == 0) {
-    mbar_init(bar, 1);
+    for (int s = 0; s < STAGES; ++s) mbar_init(&bar[s], 1);
     fence_mbar_init();
   }
   __syncthreads();
@@ -152,127 +258,67 @@ __global__ void __launch_bounds__(NT) ntt_tile_kernel(const __grid_constant__ Nt
   const T* in = reinterpret_cast<const T*>(p.in) + (size_t)mi * p.count * N;
   T* out = reinterpret_cast<T*>(p.out) + (size_t)mi * p.count * N;
   const unsigned long long ntiles = (p.count + P - 1) / P;
-  uint32_t phase = 0;
 
-  for (unsigned long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+  auto tile_valid = [&](unsigned long long tile) -> int {
     const unsigned long long first = tile * P;
-    const int nvalid = (int)((p.count - first) < (unsigned long long)P ? (p.count - first) : P);
+    return (int)((p.count - first) < (unsigned long long)P ? (p.count - first) : P);
+  };
+  auto issue_load = [&](unsigned long long tile, int s) {
+    const unsigned long long first = tile * P;
+    const int nv = tile_valid(tile);
+    T* dst = data + (size_t)s * (C::STAGE_BYTES / sizeof(T));
+    mbar_arrive_expect_tx(&bar[s], (uint32_t)(nv * N * sizeof(T)));
+    for (int q = 0; q < nv; ++q) bulk_g2s(dst + q * S, in + (first + q) * N, N * sizeof(T), &bar[s]);
+  };
+
+  unsigned long long tile = blockIdx.x;
+  if (STAGES == 2 && tid == 0 && tile < ntiles) issue_load(tile, 0);
+  uint32_t parity = 0;   // bit s: parity of the next completion of stage s
+  int other_inflight = -1;  // (thread 0) stage whose prefetch was issued this iteration
+  bool failed = false;
+  for (int i = 0; tile < ntiles; ++i, tile += gridDim.x) {
+    const int s = (STAGES == 1) ? 0 : (i & 1);
     if (tid == 0) {
-      bulk_wait_read<0>();  // previous tile's stores have finished reading the slots
-      mbar_arrive_expect_tx(bar, (uint32_t)(nvalid * N * sizeof(T)));
-      for (int q = 0; q < nvalid; ++q)
-        bulk_g2s(data + q * S, in + (first + q) * N, N * sizeof(T), bar);
+      other_inflight = -1;
+      if (STAGES == 1) {
+        bulk_wait_read<0>();  // the previous tile's stores have read the slots
+        issue_load(tile, 0);
+      } else if (tile + gridDim.x < ntiles) {
+        bulk_wait_read<0>();  // stores of the previous iteration (stage s^1) are done reading
+        issue_load(tile + gridDim.x, s ^ 1);
+        other_inflight = s ^ 1;
+      }
     }
-    const bool ok = mbar_wait(bar, phase);
-    phase ^= 1;
+    const bool ok = mbar_wait(&bar[s], (parity >> s) & 1u);
+    parity ^= 1u << s;
     if (__syncthreads_or(!ok)) {
-      if (tid == 0) record_error(p.err, LC_DEVERR_TIMEOUT);
+      failed = true;
       break;
     }
 
+    T* stage = data + (size_t)s * (C::STAGE_BYTES / sizeof(T));
 #pragma unroll 1
-    for (int it = 0; it < IT; ++it) {
-      T* slot = data + (it * C::GROUPS + grp) * S;
-      T v[V];
-      if (!INVERSE) {
-        // ---- phase 0: natural-order coefficients, register bits [LO0, LOG_N)
-#pragma unroll
-        for (int r = 0; r < V; ++r) v[r] = slot[(r << LO0) | t];
-#pragma unroll
-        for (int b = LOG_N - 1; b >= LO0; --b) {
-          const int rb = 1 << (b - LO0);
-#pragma unroll
-          for (int r = 0; r < V; ++r) {
-            if (r & rb) continue;
-            const Tw w = tw[(1 << (LOG_N - 1 - b)) + (r >> (b + 1 - LO0))];
-            ar.fwd(v[r], v[r | rb], w);
-          }
-        }
-        __syncwarp();
-#pragma unroll
-        for (int r = 0; r < V; ++r) {
-          const uint32_t idx = (r << LO0) | t;
-          slot[idx ^ ((idx >> LOG_V) & G::XM)] = v[r];
-        }
-        __syncwarp();
-        // ---- phase 1: register bits [0, LOG_V), levels b < LO0
-#pragma unroll
-        for (int r = 0; r < V; ++r) {
-          const uint32_t idx = (t << LOG_V) | r;
-          v[r] = slot[idx ^ ((idx >> LOG_V) & G::XM)];
-        }
-#pragma unroll
-        for (int b = LO0 - 1; b >= 0; --b) {
-          const int rb = 1 << b;
-#pragma unroll
-          for (int r = 0; r < V; ++r) {
-            if (r & rb) continue;
-            const Tw w = tw[G::fwd_phase1_off(b) + (r >> (b + 1)) * TT + t];
-            ar.fwd(v[r], v[r | rb], w);
-          }
-        }
-        __syncwarp();
-        // ---- output in natural order: LN index (t<<LOG_V)|r sits at brv of it
-#pragma unroll
-        for (int r = 0; r < V; ++r)
-          slot[(brv_bits(r, LOG_V) << LO0) | brv_bits(t, LO0)] = ar.fwd_final(v[r]);
-      } else {
-        // ---- phase 0: evaluations (natural order) read at bit-reversed slots,
-        //      register bits [0, LOG_V), levels b < LOG_V (per-lane twiddles)
-#pragma unroll
-        for (int r = 0; r < V; ++r) v[r] = slot[(brv_bits(r, LOG_V) << LO0) | brv_bits(t, LO0)];
-#pragma unroll
-        for (int b = 0; b < LOG_V; ++b) {
-          const int rb = 1 << b;
-#pragma unroll
-          for (int r = 0; r < V; ++r) {
-            if (r & rb) continue;
-            const Tw w = tw[G::inv_phase0_off(b) + (r >> (b + 1)) * TT + t];
-            ar.inv(v[r], v[r | rb], w);
-          }
-        }
-        __syncwarp();
-#pragma unroll
-        for (int r = 0; r < V; ++r) {
-          const uint32_t idx = (t << LOG_V) | r;
-          slot[idx ^ ((idx >> LOG_V) & G::XM)] = v[r];
-        }
-        __syncwarp();
-        // ---- phase 1: register bits [LO0, LOG_N), levels b >= LOG_V (uniform twiddles)
-#pragma unroll
-        for (int r = 0; r < V; ++r) {
-          const uint32_t idx = (r << LO0) | t;
-          v[r] = slot[idx ^ ((idx >> LOG_V) & G::XM)];
-        }
-        constexpr int P1 = G::inv_phase1_off();
-#pragma unroll
-        for (int b = LOG_V; b < LOG_N; ++b) {
-          const int rb = 1 << (b - LO0);
-#pragma unroll
-          for (int r = 0; r < V; ++r) {
-            if (r & rb) continue;
-            if (b == LOG_N - 1) {
-              ar.inv_last(v[r], v[r | rb], tw[P1 + 0], tw[P1 + 1]);
-            } else {
-              const Tw w = tw[P1 + (1 << (LOG_N - 1 - b)) + (r >> (b + 1 - LO0))];
-              ar.inv(v[r], v[r | rb], w);
-            }
-          }
-        }
-        __syncwarp();
-#pragma unroll
-        for (int r = 0; r < V; ++r) slot[(r << LO0) | t] = ar.inv_final(v[r]);
-      }
-    }
+    for (int it = 0; it < IT; ++it)
+      transform_slot<A, LOG_N, LOG_V, INVERSE>(stage + (it * C::GROUPS + grp) * S, tw, ar, t);
 
     fence_proxy_async_smem();
     __syncthreads();
     if (tid == 0) {
-      for (int q = 0; q < nvalid; ++q) bulk_s2g(out + (first + q) * N, data + q * S, N * sizeof(T));
+      const unsigned long long first = tile * P;
+      const int nv = tile_valid(tile);
+      for (int q = 0; q < nv; ++q) bulk_s2g(out + (first + q) * N, stage + q * S, N * sizeof(T));
       bulk_commit();
     }
   }
-  if (tid == 0) bulk_wait<0>();
+  if (tid == 0) {
+    if (failed) {
+      record_error(p.err, LC_DEVERR_TIMEOUT);
+      // a prefetch issued into the other stage must land before the CTA exits
+      // (bounded wait; the timed-out stage itself is not waited for again)
+      if (other_inflight >= 0) mbar_wait(&bar[other_inflight], (parity >> other_inflight) & 1u);
+    }
+    bulk_wait<0>();
+  }
 }
 
 // ---------------------------------------------------------------------------

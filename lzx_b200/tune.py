@@ -1,0 +1,67 @@
+"""Autotuner for the NTT tile kernels.
+
+Each plan can run one of several instantiated kernel shapes (threads per CTA,
+polynomials per tile, single- or double-buffered TMA staging); all give
+identical residues.  :func:`tune_ntt` times every variant on the caller's
+batch with CUDA events (device-resident buffers larger than L2, warm-up first)
+and pins the fastest on the plan.  Results are cached per (plan shape, count).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+from . import _lib
+
+NUM_VARIANTS = 5
+VARIANT_SHAPES = {
+    0: "256 threads, ~18 KB tiles, 2-stage TMA pipeline",
+    1: "256 threads, ~36 KB tiles, 1 stage",
+    2: "256 threads, ~36 KB tiles, 2 stages",
+    3: "128 threads, ~18 KB tiles, 2 stages",
+    4: "512 threads, ~18 KB tiles, 2 stages",
+}
+_cache: dict = {}
+
+
+def time_variants(plan, count: int, reps: int = 10, warmup: int = 3, inverse: bool = False):
+    """Return {variant: mean ms per launch} for ``count`` polynomials per modulus."""
+    import torch
+    L = _lib.lib()
+    elems = plan.n * plan.num_moduli * count
+    dtype = torch.int64 if plan.elem_dtype.__name__ == "uint64" else torch.int32
+    x = torch.zeros(elems, dtype=dtype, device="cuda")
+    y = torch.empty_like(x)
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    fn = L.lc_ntt_inverse if inverse else L.lc_ntt_forward
+    out = {}
+    for v in range(NUM_VARIANTS):
+        _lib.check(L.lc_ntt_plan_set_variant(plan.handle, v), "set_variant")
+        for _ in range(warmup):
+            _lib.check(fn(plan.handle, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), count,
+                          st), "tune")
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn(plan.handle, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), count, st)
+        b.record()
+        torch.cuda.synchronize()
+        out[v] = a.elapsed_time(b) / reps
+    _lib.check(L.lc_ntt_plan_check(plan.handle, st), "tune check")
+    return out
+
+
+def tune_ntt(plan, count: int, reps: int = 10) -> int:
+    """Time every variant on this batch size and keep the fastest on ``plan``."""
+    key = (plan.n, plan.num_moduli, plan.elem_dtype.__name__, count)
+    if key not in _cache:
+        fwd = time_variants(plan, count, reps)
+        inv = time_variants(plan, count, reps, inverse=True)
+        _cache[key] = (min(fwd, key=lambda v: fwd[v] + inv[v]), fwd, inv)
+    best = _cache[key][0]
+    _lib.check(_lib.lib().lc_ntt_plan_set_variant(plan.handle, best), "set_variant")
+    return best
+
+
+def last_results(plan, count: int):
+    key = (plan.n, plan.num_moduli, plan.elem_dtype.__name__, count)
+    return _cache.get(key)
