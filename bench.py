@@ -323,7 +323,7 @@ def run_ours(args):
     roofline = {
         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
         "frac": achieved / peak, "traffic": traffic,
-        "kernel": "ntt_tile_kernel<ShoupLazy, log_n=8, log_v=4> forward",
+        "kernel": "NTT forward, ShoupLazy, log_n=8, log_v=4 (tuned variant)",
         "tuning": tuning,
         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, copy)",
         "algorithmic_bytes_per_launch": ALG_BYTES_PER_LAUNCH,

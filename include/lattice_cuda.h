@@ -91,7 +91,8 @@ LC_API int lc_ntt_plan_set_variant(lc_ntt_plan *plan, int variant);
 /* Batched forward transform, device pointers.  Replaces
  * NttTables::forward_fast / RingElement::to_ntt (ntt.rs:118-146,
  * ring.rs:344-351) applied to `count` polynomials per modulus; output in the
- * reference's natural order out[j] = a(psi^(2j+1)).  in == out is allowed. */
+ * reference's natural order out[j] = a(psi^(2j+1)).  in == out is allowed;
+ * count <= 2^29 (LC_ERR_INVALID_ARGUMENT above). */
 LC_API int lc_ntt_forward(const lc_ntt_plan *plan, const void *in, void *out, size_t count,
                           lc_stream stream);
 /* Batched inverse, device pointers.  Replaces NttTables::inverse_fast /

@@ -44,11 +44,25 @@ struct ShoupLazy {
     x = X + t;
     y = X - t + q2;
   }
+  // First forward level: canonical inputs need no correction of X.
+  LC_D void fwd_first(uint32_t& x, uint32_t& y, Tw w) const {
+    uint32_t X = x;
+    uint32_t t = mulw(y, w);
+    x = X + t;
+    y = X - t + q2;
+  }
   // Gentleman-Sande (inverse) butterfly: X,Y in [0,2q) -> [0,2q).
   LC_D void inv(uint32_t& x, uint32_t& y, Tw w) const {
     uint32_t s = x + y;
     uint32_t d = x - y + q2;
     x = min(s, s - q2);
+    y = mulw(d, w);
+  }
+  // First inverse level: canonical inputs, so X + Y < 2q already.
+  LC_D void inv_first(uint32_t& x, uint32_t& y, Tw w) const {
+    uint32_t s = x + y;
+    uint32_t d = x - y + q2;
+    x = s;
     y = mulw(d, w);
   }
   // Last inverse level fused with the n^{-1} scaling: X,Y in [0,2q).
@@ -103,6 +117,8 @@ struct MontCanon {
     x = add(X, Y);
     y = mont(sub(X, Y), w.x);
   }
+  LC_D void fwd_first(uint32_t& x, uint32_t& y, Tw w) const { fwd(x, y, w); }
+  LC_D void inv_first(uint32_t& x, uint32_t& y, Tw w) const { inv(x, y, w); }
   LC_D void inv_last(uint32_t& x, uint32_t& y, Tw ninv, Tw wninv) const {
     uint32_t X = x, Y = y;
     x = mont(add(X, Y), ninv.x);
@@ -174,6 +190,8 @@ struct Goldilocks {
     x = gl_add(X, Y);
     y = gl_mul(gl_sub(X, Y), w);
   }
+  LC_D void fwd_first(uint64_t& x, uint64_t& y, Tw w) const { fwd(x, y, w); }
+  LC_D void inv_first(uint64_t& x, uint64_t& y, Tw w) const { inv(x, y, w); }
   LC_D void inv_last(uint64_t& x, uint64_t& y, Tw ninv, Tw wninv) const {
     uint64_t X = x, Y = y;
     x = gl_mul(gl_add(X, Y), ninv);

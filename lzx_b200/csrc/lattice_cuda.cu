@@ -20,6 +20,10 @@ using namespace lc;
 
 namespace lc {
 
+// Largest batch (polynomials per modulus) of one call; keeps the kernels' tile
+// counters in 32 bits.
+constexpr size_t kMaxBatch = (size_t)1 << 29;
+
 // --------------------------------------------------------------- host modular arithmetic
 
 typedef unsigned __int128 u128;
@@ -133,22 +137,46 @@ template <class A, int LOG_N, int LOG_V, int NT, int IT, int STAGES, bool INV>
 static int launch_tile_cfg(const NttParams& p, cudaStream_t s) {
   using C = NttKernelCfg<A, LOG_N, LOG_V, NT, IT, STAGES, INV>;
   auto kern = ntt_tile_kernel<A, LOG_N, LOG_V, NT, IT, STAGES, INV>;
+  constexpr size_t smem = C::SMEM;
   static bool attr_done = false;
   if (!attr_done) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
-    if (e != cudaSuccess) return map_cuda(e);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e == cudaErrorInvalidValue ? LC_ERR_UNSUPPORTED : map_cuda(e);
     attr_done = true;
   }
   int per_sm = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, C::SMEM);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem);
   if (e != cudaSuccess) return map_cuda(e);
   per_sm = std::max(per_sm, 1);
   const unsigned long long ntiles = (p.count + C::P - 1) / C::P;
   const int sms = device_sm_count();
   unsigned long long gx = std::min<unsigned long long>(ntiles, (unsigned long long)sms * per_sm);
   gx = std::max<unsigned long long>(gx, 1);
-  dim3 grid((unsigned)gx, p.num_moduli);
-  kern<<<grid, NT, C::SMEM, s>>>(p);
+  kern<<<dim3((unsigned)gx, p.num_moduli), NT, smem, s>>>(p);
+  return map_cuda(cudaGetLastError());
+}
+
+template <class A, int LOG_N, int LOG_V, int WARPS, int IT, int STAGES, bool INV>
+static int launch_warp_cfg(const NttParams& p, cudaStream_t s) {
+  using C = NttWarpCfg<A, LOG_N, LOG_V, WARPS, IT, STAGES, INV>;
+  auto kern = ntt_warp_kernel<A, LOG_N, LOG_V, WARPS, IT, STAGES, INV>;
+  constexpr size_t smem = C::SMEM;
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e == cudaErrorInvalidValue ? LC_ERR_UNSUPPORTED : map_cuda(e);
+    attr_done = true;
+  }
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, C::NT, smem);
+  if (e != cudaSuccess) return map_cuda(e);
+  per_sm = std::max(per_sm, 1);
+  const unsigned long long wtiles = (p.count + C::P - 1) / C::P;
+  const unsigned long long need = (wtiles + WARPS - 1) / WARPS;
+  const int sms = device_sm_count();
+  unsigned long long gx = std::min<unsigned long long>(need, (unsigned long long)sms * per_sm);
+  gx = std::max<unsigned long long>(gx, 1);
+  kern<<<dim3((unsigned)gx, p.num_moduli), C::NT, smem, s>>>(p);
   return map_cuda(cudaGetLastError());
 }
 
@@ -158,7 +186,7 @@ constexpr int default_it() {
   using G = Geo<LOG_N, LOG_V>;
   using SL = Slots<A, LOG_N, LOG_V>;
   constexpr size_t per_it = (size_t)(NT / G::T) * SL::S * sizeof(typename A::T);
-  return per_it >= 18 * 1024 ? 1 : (int)((18 * 1024) / per_it);
+  return per_it >= 4 * 1024 ? 1 : (int)((4 * 1024) / per_it);
 }
 
 // Ring degrees whose tile kernels are instantiated in several shapes for the
@@ -173,15 +201,15 @@ template <class A, int LOG_N, int LOG_V, bool INV>
 static int launch_tile(const NttParams& p, int variant, cudaStream_t s) {
   if constexpr (!tunable<A, LOG_N>()) {
     (void)variant;
-    return launch_tile_cfg<A, LOG_N, LOG_V, 256, default_it<A, LOG_N, LOG_V, 256>(), 2, INV>(p, s);
+    return launch_tile_cfg<A, LOG_N, LOG_V, 128, default_it<A, LOG_N, LOG_V, 128>(), 2, INV>(p, s);
   } else {
   // variant 0 is the tuned default; 1..4 are alternatives kept for the tuner
   switch (variant) {
-    case 1: return launch_tile_cfg<A, LOG_N, LOG_V, 256, 2 * default_it<A, LOG_N, LOG_V, 256>(), 1, INV>(p, s);
-    case 2: return launch_tile_cfg<A, LOG_N, LOG_V, 256, 2 * default_it<A, LOG_N, LOG_V, 256>(), 2, INV>(p, s);
-    case 3: return launch_tile_cfg<A, LOG_N, LOG_V, 128, default_it<A, LOG_N, LOG_V, 128>(), 2, INV>(p, s);
-    case 4: return launch_tile_cfg<A, LOG_N, LOG_V, 512, default_it<A, LOG_N, LOG_V, 512>(), 2, INV>(p, s);
-    default: return launch_tile_cfg<A, LOG_N, LOG_V, 256, default_it<A, LOG_N, LOG_V, 256>(), 2, INV>(p, s);
+    case 1: return launch_tile_cfg<A, LOG_N, LOG_V, 128, default_it<A, LOG_N, LOG_V, 128>(), 3, INV>(p, s);
+    case 2: return launch_tile_cfg<A, LOG_N, LOG_V, 256, default_it<A, LOG_N, LOG_V, 256>(), 2, INV>(p, s);
+    case 3: return launch_warp_cfg<A, LOG_N, LOG_V, 4, 1, 2, INV>(p, s);
+    case 4: return launch_warp_cfg<A, LOG_N, LOG_V, 4, 1, 3, INV>(p, s);
+    default: return launch_tile_cfg<A, LOG_N, LOG_V, 128, default_it<A, LOG_N, LOG_V, 128>(), 2, INV>(p, s);
   }
   }
 }
@@ -222,6 +250,7 @@ static int dispatch(int log_n, const NttParams& p, int variant, cudaStream_t s) 
 int run_ntt(const lc_ntt_plan* plan, const void* in, void* out, size_t count, bool inverse,
             cudaStream_t s) {
   if (count == 0) return LC_OK;
+  if (count > kMaxBatch) return LC_ERR_INVALID_ARGUMENT;
   NttParams p{};
   p.in = in;
   p.out = out;

@@ -17,8 +17,7 @@
 //   * T = 2^(LOG_N-LOG_V) threads own one polynomial, V = 2^LOG_V values
 //     each, in registers.  Phase 0 runs the butterfly levels whose bit lies
 //     in the thread's register index (no data exchange); the group then
-//     transposes through an XOR-swizzled copy of the slot (bank-conflict
-//     free) and phase 1 runs the remaining levels.  T <= 32, so a group
+//     transposes through a padded copy of the slot (bank-conflict free) and phase 1 runs the remaining levels.  T <= 32, so a group
 //     lives inside one warp and synchronises with __syncwarp.
 //   * Results go back to the same slot in output order and thread 0 issues
 //     1-D bulk stores.
@@ -52,7 +51,6 @@ struct Geo {
   static constexpr int V = 1 << LOG_V;
   static constexpr int LO0 = LOG_N - LOG_V;  // lane bits per polynomial
   static constexpr int T = 1 << LO0;         // threads per polynomial
-  static constexpr int XM = (1 << (LOG_V < LO0 ? LOG_V : LO0)) - 1;
   static_assert(LO0 >= 1 && LO0 <= 5 && LOG_N <= 2 * LOG_V, "two-phase geometry");
   // Twiddle table layout (entries), see the host-side generator.
   __host__ __device__ static constexpr int fwd_phase1_off(int b) {
@@ -98,9 +96,12 @@ template <class A, int LOG_N, int LOG_V>
 struct Slots {
   using G = Geo<LOG_N, LOG_V>;
   using T = typename A::T;
-  // pad so that the polynomials sharing a warp land on disjoint banks
-  static constexpr int PAD = (sizeof(T) == 4) ? (G::T < 32 ? G::T : 0) : (G::T < 16 ? G::T : 0);
-  static constexpr int S = G::N + PAD;
+  // One pad word per 2^LOG_V words: the transposing copy lives at
+  // idx + (idx >> LOG_V), which keeps both access patterns bank-conflict free
+  // and every address a per-thread base plus a compile-time offset.  N + T
+  // words also spread the polynomials that share a warp over disjoint banks.
+  static constexpr int S = G::N + G::T;
+  LC_HD static constexpr int padded(int idx) { return idx + (idx >> LOG_V); }
 };
 
 template <class A, int LOG_N, int LOG_V, int NT, int IT, int STAGES, bool INVERSE>
@@ -116,7 +117,7 @@ struct NttKernelCfg {
   static constexpr size_t STAGE_BYTES = (size_t)P * SL::S * sizeof(T);
   static constexpr size_t SMEM = TW_BYTES + STAGES * STAGE_BYTES + 8 * STAGES;
   static_assert(NT % G::T == 0, "block size");
-  static_assert(STAGES == 1 || STAGES == 2, "stages");
+  static_assert(STAGES >= 1 && STAGES <= 4, "stages");
   static_assert((SL::S * sizeof(T)) % 16 == 0, "slot alignment for bulk copies");
   static_assert(STAGE_BYTES % 16 == 0, "stage alignment");
 };
@@ -127,6 +128,7 @@ struct NttKernelCfg {
 template <class A, int LOG_N, int LOG_V, bool INVERSE>
 LC_D void transform_slot(typename A::T* slot, const typename A::Tw* tw, const A& ar, uint32_t t) {
   using G = Geo<LOG_N, LOG_V>;
+  using SL = Slots<A, LOG_N, LOG_V>;
   using T = typename A::T;
   using Tw = typename A::Tw;
   constexpr int V = G::V, LO0 = G::LO0, TT = G::T;
@@ -142,22 +144,19 @@ LC_D void transform_slot(typename A::T* slot, const typename A::Tw* tw, const A&
       for (int r = 0; r < V; ++r) {
         if (r & rb) continue;
         const Tw w = tw[(1 << (LOG_N - 1 - b)) + (r >> (b + 1 - LO0))];
-        ar.fwd(v[r], v[r | rb], w);
+        if (b == LOG_N - 1)
+          ar.fwd_first(v[r], v[r | rb], w);
+        else
+          ar.fwd(v[r], v[r | rb], w);
       }
     }
     __syncwarp();
 #pragma unroll
-    for (int r = 0; r < V; ++r) {
-      const uint32_t idx = (r << LO0) | t;
-      slot[idx ^ ((idx >> LOG_V) & G::XM)] = v[r];
-    }
+    for (int r = 0; r < V; ++r) slot[SL::padded((r << LO0) | t)] = v[r];
     __syncwarp();
     // ---- phase 1: register bits [0, LOG_V), levels b < LO0
 #pragma unroll
-    for (int r = 0; r < V; ++r) {
-      const uint32_t idx = (t << LOG_V) | r;
-      v[r] = slot[idx ^ ((idx >> LOG_V) & G::XM)];
-    }
+    for (int r = 0; r < V; ++r) v[r] = slot[SL::padded((t << LOG_V) | r)];
 #pragma unroll
     for (int b = LO0 - 1; b >= 0; --b) {
       const int rb = 1 << b;
@@ -185,22 +184,19 @@ LC_D void transform_slot(typename A::T* slot, const typename A::Tw* tw, const A&
       for (int r = 0; r < V; ++r) {
         if (r & rb) continue;
         const Tw w = tw[G::inv_phase0_off(b) + (r >> (b + 1)) * TT + t];
-        ar.inv(v[r], v[r | rb], w);
+        if (b == 0)
+          ar.inv_first(v[r], v[r | rb], w);
+        else
+          ar.inv(v[r], v[r | rb], w);
       }
     }
     __syncwarp();
 #pragma unroll
-    for (int r = 0; r < V; ++r) {
-      const uint32_t idx = (t << LOG_V) | r;
-      slot[idx ^ ((idx >> LOG_V) & G::XM)] = v[r];
-    }
+    for (int r = 0; r < V; ++r) slot[SL::padded((t << LOG_V) | r)] = v[r];
     __syncwarp();
     // ---- phase 1: register bits [LO0, LOG_N), levels b >= LOG_V (uniform twiddles)
 #pragma unroll
-    for (int r = 0; r < V; ++r) {
-      const uint32_t idx = (r << LO0) | t;
-      v[r] = slot[idx ^ ((idx >> LOG_V) & G::XM)];
-    }
+    for (int r = 0; r < V; ++r) v[r] = slot[SL::padded((r << LO0) | t)];
     constexpr int P1 = G::inv_phase1_off();
 #pragma unroll
     for (int b = LOG_V; b < LOG_N; ++b) {
@@ -222,8 +218,7 @@ LC_D void transform_slot(typename A::T* slot, const typename A::Tw* tw, const A&
   }
 }
 
-// Persistent tile loop.  STAGES == 2 double-buffers the tiles: the bulk load
-// of the next tile is in flight while the current one is transformed.
+// Persistent tile loop over a ring of STAGES shared-memory tile buffers.
 template <class A, int LOG_N, int LOG_V, int NT, int IT, int STAGES, bool INVERSE>
 __global__ void __launch_bounds__(NT) ntt_tile_kernel(const __grid_constant__ NttParams p) {
   using C = NttKernelCfg<A, LOG_N, LOG_V, NT, IT, STAGES, INVERSE>;
@@ -233,10 +228,10 @@ __global__ void __launch_bounds__(NT) ntt_tile_kernel(const __grid_constant__ Nt
   constexpr int N = G::N, TT = G::T, S = C::SL::S, P = C::P;
 
   extern __shared__ __align__(128) unsigned char smem_raw[];
+  // this modulus's twiddle table, then the stage ring, then the mbarriers
   Tw* tw = reinterpret_cast<Tw*>(smem_raw);
   T* data = reinterpret_cast<T*>(smem_raw + C::TW_BYTES);
-  uint64_t* bar =
-      reinterpret_cast<uint64_t*>(smem_raw + C::TW_BYTES + STAGES * C::STAGE_BYTES);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + C::TW_BYTES + STAGES * C::STAGE_BYTES);
 
   const uint32_t mi = blockIdx.y;
   const A ar = make_arith<A>(p, mi);
@@ -244,7 +239,6 @@ __global__ void __launch_bounds__(NT) ntt_tile_kernel(const __grid_constant__ Nt
   const int grp = tid / TT;
   const uint32_t t = (uint32_t)(tid % TT);
 
-  // twiddles for this modulus -> shared memory
   {
     const Tw* src = reinterpret_cast<const Tw*>(p.tw) + (size_t)mi * p.tw_stride;
     for (int i = tid; i < C::TW_ENTRIES; i += NT) tw[i] = src[i];
@@ -257,42 +251,51 @@ __global__ void __launch_bounds__(NT) ntt_tile_kernel(const __grid_constant__ Nt
 
   const T* in = reinterpret_cast<const T*>(p.in) + (size_t)mi * p.count * N;
   T* out = reinterpret_cast<T*>(p.out) + (size_t)mi * p.count * N;
-  const unsigned long long ntiles = (p.count + P - 1) / P;
+  const uint32_t ntiles = (uint32_t)((p.count + P - 1) / P);
+  const uint32_t stride = gridDim.x;
 
-  auto tile_valid = [&](unsigned long long tile) -> int {
-    const unsigned long long first = tile * P;
+  auto valid = [&](uint32_t tile) -> int {
+    const unsigned long long first = (unsigned long long)tile * P;
     return (int)((p.count - first) < (unsigned long long)P ? (p.count - first) : P);
   };
-  auto issue_load = [&](unsigned long long tile, int s) {
-    const unsigned long long first = tile * P;
-    const int nv = tile_valid(tile);
+  auto issue_load = [&](uint32_t tile, int s) {
+    const T* src = in + (size_t)tile * P * N;
+    const int nv = valid(tile);
     T* dst = data + (size_t)s * (C::STAGE_BYTES / sizeof(T));
     mbar_arrive_expect_tx(&bar[s], (uint32_t)(nv * N * sizeof(T)));
-    for (int q = 0; q < nv; ++q) bulk_g2s(dst + q * S, in + (first + q) * N, N * sizeof(T), &bar[s]);
+    for (int q = 0; q < nv; ++q) bulk_g2s(dst + q * S, src + (size_t)q * N, N * sizeof(T), &bar[s]);
   };
 
-  unsigned long long tile = blockIdx.x;
-  if (STAGES == 2 && tid == 0 && tile < ntiles) issue_load(tile, 0);
-  uint32_t parity = 0;   // bit s: parity of the next completion of stage s
-  int other_inflight = -1;  // (thread 0) stage whose prefetch was issued this iteration
-  bool failed = false;
-  for (int i = 0; tile < ntiles; ++i, tile += gridDim.x) {
-    const int s = (STAGES == 1) ? 0 : (i & 1);
+  // Ring of STAGES tile buffers.  Iteration i consumes stage i % STAGES; at
+  // its start thread 0 refills the stage consumed by iteration i-1 with the
+  // tile STAGES-1 strides ahead once that stage's stores have finished
+  // reading it, so up to STAGES-1 tile loads stay in flight behind the
+  // transforms.
+  if (tid == 0) {
+    for (int k = 0; k < STAGES - 1; ++k) {
+      const unsigned long long tk = blockIdx.x + (unsigned long long)k * stride;
+      if (tk < ntiles) issue_load((uint32_t)tk, k);
+    }
+  }
+  uint32_t parity = 0;  // bit s: parity of the next completion of stage s
+  bool refilled = false;  // (thread 0) whether this iteration issued a prefetch
+  int failed_at = -1;     // iteration whose wait timed out
+  uint32_t tile = blockIdx.x;
+  for (int i = 0; tile < ntiles; ++i, tile += stride) {
+    const int s = i % STAGES;
     if (tid == 0) {
-      other_inflight = -1;
-      if (STAGES == 1) {
-        bulk_wait_read<0>();  // the previous tile's stores have read the slots
-        issue_load(tile, 0);
-      } else if (tile + gridDim.x < ntiles) {
-        bulk_wait_read<0>();  // stores of the previous iteration (stage s^1) are done reading
-        issue_load(tile + gridDim.x, s ^ 1);
-        other_inflight = s ^ 1;
+      refilled = false;
+      const unsigned long long ahead = tile + (unsigned long long)(STAGES - 1) * stride;
+      if (ahead < ntiles) {
+        bulk_wait_read<0>();  // stores of iteration i-1 (the refilled stage) are done reading
+        issue_load((uint32_t)ahead, (i + STAGES - 1) % STAGES);
+        refilled = true;
       }
     }
     const bool ok = mbar_wait(&bar[s], (parity >> s) & 1u);
     parity ^= 1u << s;
     if (__syncthreads_or(!ok)) {
-      failed = true;
+      failed_at = i;
       break;
     }
 
@@ -304,18 +307,153 @@ __global__ void __launch_bounds__(NT) ntt_tile_kernel(const __grid_constant__ Nt
     fence_proxy_async_smem();
     __syncthreads();
     if (tid == 0) {
-      const unsigned long long first = tile * P;
-      const int nv = tile_valid(tile);
-      for (int q = 0; q < nv; ++q) bulk_s2g(out + (first + q) * N, stage + q * S, N * sizeof(T));
+      T* dst = out + (size_t)tile * P * N;
+      const int nv = valid(tile);
+      for (int q = 0; q < nv; ++q) bulk_s2g(dst + (size_t)q * N, stage + q * S, N * sizeof(T));
       bulk_commit();
     }
   }
   if (tid == 0) {
-    if (failed) {
+    if (failed_at >= 0) {
       record_error(p.err, LC_DEVERR_TIMEOUT);
-      // a prefetch issued into the other stage must land before the CTA exits
-      // (bounded wait; the timed-out stage itself is not waited for again)
-      if (other_inflight >= 0) mbar_wait(&bar[other_inflight], (parity >> other_inflight) & 1u);
+      // Loads still in flight must land before the CTA exits: the tiles
+      // 1 .. STAGES-2 strides ahead (issued earlier) and STAGES-1 ahead
+      // (issued in the failed iteration when `refilled`).  Bounded waits;
+      // the timed-out stage is not waited for again.
+      for (int k = 1; k < STAGES; ++k) {
+        const unsigned long long tk = tile + (unsigned long long)k * stride;
+        const bool issued = (k < STAGES - 1) || refilled;
+        if (tk >= ntiles || !issued) continue;
+        const int sk = (failed_at + k) % STAGES;
+        mbar_wait(&bar[sk], (parity >> sk) & 1u);
+      }
+    }
+    bulk_wait<0>();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Warp-autonomous variant: every warp runs its own ring of STAGES tiles of
+// 32/T * IT polynomials (its own mbarriers; lane 0 issues its bulk copies), so
+// the steady-state loop has no CTA-wide barrier at all.  Warps take tiles
+// strided over the whole grid.
+template <class A, int LOG_N, int LOG_V, int WARPS, int IT, int STAGES, bool INVERSE>
+struct NttWarpCfg {
+  using G = Geo<LOG_N, LOG_V>;
+  using SL = Slots<A, LOG_N, LOG_V>;
+  using T = typename A::T;
+  using Tw = typename A::Tw;
+  static constexpr int NT = 32 * WARPS;
+  static constexpr int GROUPS = 32 / G::T;      // polynomials per warp per pass
+  static constexpr int P = GROUPS * IT;          // polynomials per warp tile
+  static constexpr int TW_ENTRIES = INVERSE ? G::inv_entries() : G::fwd_entries();
+  static constexpr size_t TW_BYTES = ((size_t)TW_ENTRIES * sizeof(Tw) + 15) / 16 * 16;
+  static constexpr size_t STAGE_BYTES = (size_t)P * SL::S * sizeof(T);
+  static constexpr size_t WARP_BYTES = STAGES * STAGE_BYTES;
+  static constexpr size_t SMEM = TW_BYTES + WARPS * WARP_BYTES + 8 * STAGES * WARPS;
+  static_assert(G::T <= 32 && 32 % G::T == 0, "a polynomial group lives in one warp");
+  static_assert(STAGES >= 2 && STAGES <= 4, "stages");
+  static_assert(STAGE_BYTES % 16 == 0, "stage alignment");
+};
+
+template <class A, int LOG_N, int LOG_V, int WARPS, int IT, int STAGES, bool INVERSE>
+__global__ void __launch_bounds__(32 * WARPS) ntt_warp_kernel(const __grid_constant__ NttParams p) {
+  using C = NttWarpCfg<A, LOG_N, LOG_V, WARPS, IT, STAGES, INVERSE>;
+  using G = typename C::G;
+  using T = typename C::T;
+  using Tw = typename C::Tw;
+  constexpr int N = G::N, TT = G::T, S = C::SL::S, P = C::P;
+
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  Tw* tw = reinterpret_cast<Tw*>(smem_raw);
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  T* data = reinterpret_cast<T*>(smem_raw + C::TW_BYTES + warp * C::WARP_BYTES);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + C::TW_BYTES + WARPS * C::WARP_BYTES) +
+                  warp * STAGES;
+
+  const uint32_t mi = blockIdx.y;
+  const A ar = make_arith<A>(p, mi);
+  const int grp = lane / TT;
+  const uint32_t t = (uint32_t)(lane % TT);
+  {
+    const Tw* src = reinterpret_cast<const Tw*>(p.tw) + (size_t)mi * p.tw_stride;
+    for (int i = tid; i < C::TW_ENTRIES; i += C::NT) tw[i] = src[i];
+  }
+  if (lane == 0) {
+    for (int s = 0; s < STAGES; ++s) mbar_init(&bar[s], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();  // twiddles and barriers ready; the only CTA-wide barrier
+
+  const T* in = reinterpret_cast<const T*>(p.in) + (size_t)mi * p.count * N;
+  T* out = reinterpret_cast<T*>(p.out) + (size_t)mi * p.count * N;
+  const uint32_t ntiles = (uint32_t)((p.count + P - 1) / P);
+  const uint32_t stride = gridDim.x * WARPS;
+  const uint32_t first_tile = blockIdx.x * WARPS + warp;
+
+  auto valid = [&](uint32_t tile) -> int {
+    const unsigned long long first = (unsigned long long)tile * P;
+    return (int)((p.count - first) < (unsigned long long)P ? (p.count - first) : P);
+  };
+  auto issue_load = [&](uint32_t tile, int s) {
+    const T* src = in + (size_t)tile * P * N;
+    const int nv = valid(tile);
+    T* dst = data + (size_t)s * (C::STAGE_BYTES / sizeof(T));
+    mbar_arrive_expect_tx(&bar[s], (uint32_t)(nv * N * sizeof(T)));
+    for (int q = 0; q < nv; ++q) bulk_g2s(dst + q * S, src + (size_t)q * N, N * sizeof(T), &bar[s]);
+  };
+
+  if (lane == 0) {
+    for (int k = 0; k < STAGES - 1; ++k) {
+      const unsigned long long tk = first_tile + (unsigned long long)k * stride;
+      if (tk < ntiles) issue_load((uint32_t)tk, k);
+    }
+  }
+  uint32_t parity = 0;
+  bool refilled = false;
+  int failed_at = -1;
+  uint32_t tile = first_tile;
+  for (int i = 0; tile < ntiles; ++i, tile += stride) {
+    const int s = i % STAGES;
+    if (lane == 0) {
+      refilled = false;
+      const unsigned long long ahead = tile + (unsigned long long)(STAGES - 1) * stride;
+      if (ahead < ntiles) {
+        bulk_wait_read<0>();  // this warp's stores of iteration i-1 are done reading
+        issue_load((uint32_t)ahead, (i + STAGES - 1) % STAGES);
+        refilled = true;
+      }
+    }
+    const bool ok = mbar_wait(&bar[s], (parity >> s) & 1u);
+    parity ^= 1u << s;
+    if (__any_sync(0xffffffffu, !ok)) {
+      failed_at = i;
+      break;
+    }
+    T* stage = data + (size_t)s * (C::STAGE_BYTES / sizeof(T));
+#pragma unroll 1
+    for (int it = 0; it < IT; ++it)
+      transform_slot<A, LOG_N, LOG_V, INVERSE>(stage + (it * C::GROUPS + grp) * S, tw, ar, t);
+    fence_proxy_async_smem();
+    __syncwarp();
+    if (lane == 0) {
+      T* dst = out + (size_t)tile * P * N;
+      const int nv = valid(tile);
+      for (int q = 0; q < nv; ++q) bulk_s2g(dst + (size_t)q * N, stage + q * S, N * sizeof(T));
+      bulk_commit();
+    }
+  }
+  if (lane == 0) {
+    if (failed_at >= 0) {
+      record_error(p.err, LC_DEVERR_TIMEOUT);
+      for (int k = 1; k < STAGES; ++k) {
+        const unsigned long long tk = tile + (unsigned long long)k * stride;
+        const bool issued = (k < STAGES - 1) || refilled;
+        if (tk >= ntiles || !issued) continue;
+        const int sk = (failed_at + k) % STAGES;
+        mbar_wait(&bar[sk], (parity >> sk) & 1u);
+      }
     }
     bulk_wait<0>();
   }

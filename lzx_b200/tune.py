@@ -14,11 +14,11 @@ from . import _lib
 
 NUM_VARIANTS = 5
 VARIANT_SHAPES = {
-    0: "256 threads, ~18 KB tiles, 2-stage TMA pipeline",
-    1: "256 threads, ~36 KB tiles, 1 stage",
-    2: "256 threads, ~36 KB tiles, 2 stages",
-    3: "128 threads, ~18 KB tiles, 2 stages",
-    4: "512 threads, ~18 KB tiles, 2 stages",
+    0: "CTA-wide TMA ring: 128 threads, 2 stages",
+    1: "CTA-wide TMA ring: 128 threads, 3 stages",
+    2: "CTA-wide TMA ring: 256 threads, 2 stages",
+    3: "warp-autonomous TMA rings: 4 warps/CTA, 2 stages",
+    4: "warp-autonomous TMA rings: 4 warps/CTA, 3 stages",
 }
 _cache: dict = {}
 

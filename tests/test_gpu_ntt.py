@@ -196,3 +196,23 @@ def test_ring_element_api():
     assert RingElement.from_ntt(c, ev) == a
     u = c.uniform_from_seed(b"ajtai-A", bytes([42]) * 32, 7)
     assert np.array_equal(u.coeffs(), oracle.uniform_from_seed(om, 6, b"ajtai-A", bytes([42]) * 32, 7))
+
+
+@pytest.mark.parametrize("variant", range(5))
+def test_every_kernel_variant_is_bit_exact(variant):
+    """The tuner may pick any instantiated kernel shape; all must agree with the oracle."""
+    count = 1000  # not a multiple of any tile size
+    a = synth.crt_batch(31, CRT_SET_30BIT, count, 256)
+    t = NttTables(CRT_SET_30BIT, 8)
+    assert _lib.lib().lc_ntt_plan_set_variant(t.handle, variant) == 0
+    got = t.forward_fast(a.copy())
+    for i, m in enumerate(CRT_SET_30BIT):
+        assert np.array_equal(got[i], ora_tables(m, 8).forward_batch(a[i]))
+    assert np.array_equal(t.inverse_fast(got.copy()), a)
+    g = synth.synth_gl(32, 0, 777 * 64).reshape(777, 64)
+    tg = GoldilocksNttTables(6)
+    assert _lib.lib().lc_ntt_plan_set_variant(tg.handle, variant) == 0
+    fg = tg.forward_fast(g.copy())
+    assert np.array_equal(fg, oracle.NttTablesGl(6).forward_batch(g))
+    assert np.array_equal(tg.inverse_fast(fg.copy()), g)
+    assert _lib.lib().lc_ntt_plan_set_variant(t.handle, 5) == _lib.LC_ERR_INVALID_ARGUMENT
