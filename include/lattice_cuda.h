@@ -111,6 +111,45 @@ LC_API int lc_ntt_inverse_host(lc_ntt_plan *plan, const void *in, void *out, siz
  * CUDA error (LC_ERR_CUDA). */
 LC_API int lc_ntt_plan_check(lc_ntt_plan *plan, lc_stream stream);
 
+/* ------------------------------------------------------------------------
+ * Ajtai commitment keys and commits (lattice-commitment/src/ajtai.rs).
+ * A key holds the cached forward NTT of A resident on the device, as
+ * AjtaiPublicKey::from_seed does (ajtai.rs:87-103), for one modulus: a u32
+ * plan with num_moduli == 1 (e.g. Modulus32::Q_32) or a Goldilocks plan.
+ * Supported: log_n 1..10 (u32) / 1..9 (Goldilocks), k <= 16 rows, any m.
+ * A key is used by one thread
+ * at a time (it owns its scratch buffers).
+ * ---------------------------------------------------------------------- */
+typedef struct lc_ajtai_key lc_ajtai_key;
+
+/* `matrix`: the k*m entries A[i][j] in coefficient form, row-major
+ * (entry (i,j) at (i*m + j)*n), residues of the plan's element type; host
+ * memory, or device memory when matrix_on_device != 0.  Replaces the
+ * cached-NTT part of AjtaiPublicKey::from_seed (ajtai.rs:91-96); the seed
+ * expansion itself (uniform_from_seed, ring.rs:102-180) stays on the host. */
+LC_API int lc_ajtai_key_create(const lc_ntt_plan *plan, uint32_t k, uint32_t m, const void *matrix,
+                               int matrix_on_device, lc_ajtai_key **out);
+LC_API void lc_ajtai_key_destroy(lc_ajtai_key *key);
+LC_API int lc_ajtai_key_info(const lc_ajtai_key *key, uint32_t *k, uint32_t *m, uint32_t *log_n);
+
+/* Commit `batch` witnesses, device pointers: s = [batch][m][n] canonical
+ * residues, out = [batch][k][n].  For each witness this is
+ * AjtaiPublicKey::commit (ajtai.rs:118-153): forward NTT of every s_j,
+ * pointwise multiply-accumulate against the cached NTT(A), one inverse NTT
+ * per row.  Bit-identical to the reference. */
+LC_API int lc_ajtai_commit(lc_ajtai_key *key, const void *s, size_t batch, void *out,
+                           lc_stream stream);
+/* Same with witness coefficients given as int8 digits in [-128, 127] (a digit
+ * x < 0 stands for the residue q - |x|, as NeoRing::small does,
+ * lattice-folding/src/neo.rs:98-109). */
+LC_API int lc_ajtai_commit_i8(lc_ajtai_key *key, const int8_t *s, size_t batch, void *out,
+                              lc_stream stream);
+/* Host-buffer variants (synchronous). */
+LC_API int lc_ajtai_commit_host(lc_ajtai_key *key, const void *s, size_t batch, void *out);
+LC_API int lc_ajtai_commit_i8_host(lc_ajtai_key *key, const int8_t *s, size_t batch, void *out);
+/* Wait for `stream` and report device-side errors of this key's kernels. */
+LC_API int lc_ajtai_key_check(lc_ajtai_key *key, lc_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -66,6 +66,14 @@ def _declare(L):
         "lc_ntt_inverse_host": (i32, [P, P, P, sz]),
         "lc_ntt_plan_check": (i32, [P, P]),
         "lc_ntt_plan_set_variant": (i32, [P, i32]),
+        "lc_ajtai_key_create": (i32, [P, u32, u32, P, i32, C.POINTER(P)]),
+        "lc_ajtai_key_destroy": (None, [P]),
+        "lc_ajtai_key_info": (i32, [P, U32P, U32P, U32P]),
+        "lc_ajtai_commit": (i32, [P, P, sz, P, P]),
+        "lc_ajtai_commit_i8": (i32, [P, P, sz, P, P]),
+        "lc_ajtai_commit_host": (i32, [P, P, sz, P]),
+        "lc_ajtai_commit_i8_host": (i32, [P, P, sz, P]),
+        "lc_ajtai_key_check": (i32, [P, P]),
     }
     optional = {
     }

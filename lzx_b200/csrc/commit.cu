@@ -1,0 +1,703 @@
+// commit.cu -- Ajtai commitment c = A.w, cached-NTT form (sm_100a).
+//
+// Restates AjtaiPublicKey::commit (lattice-commitment/src/ajtai.rs:118-153):
+//   t_i = INTT( sum_j NTT(A_ij) (.) NTT(s_j) ),  i < k, j < m,
+// for a batch of B witnesses at once, over a u32 modulus (Modulus32, e.g.
+// Q_32) or over Goldilocks.  Zero witness elements contribute nothing, which
+// is exactly the reference's skip (ajtai.rs:128-137); every output is a
+// canonical residue, bit-identical to the reference.
+//
+// Device layouts (t = NTT slot, j = witness element, i = row, b = witness):
+//   key   Ahat_T[t][j][i_pad]      cached NTT(A), i padded to 16 with zeros
+//   Ŵ     What_T[t][j][b_pad]      witness NTT, written frequency-major
+//   parts partial[split][t][i][b] K-split partial sums, canonical residues
+//   Ĉ     Chat[b][i][t]            summed evaluations -> inverse NTT -> out
+// so that the per-frequency products C_t = A_t^T . W_t read contiguous rows.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <new>
+#include <type_traits>
+#include <vector>
+
+#include "../../include/lattice_cuda.h"
+#include "internal.h"
+#include "ntt_kernels.cuh"
+
+namespace lc {
+
+constexpr int kIPad = 16;    // rows of A per MAC tile (padded)
+constexpr int kBTile = 128;  // witnesses per MAC tile
+
+// ------------------------------------------------------------------ element traits
+
+template <class E>
+struct Field;
+
+template <>
+struct Field<uint64_t> {  // Goldilocks
+  LC_D static uint64_t reduce160(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3, uint32_t r4,
+                                 uint32_t) {
+    // x = (r3 r2)*2^64 + (r1 r0) + r4*2^128;  2^128 == -2^32 (mod p)
+    uint64_t lo = ((uint64_t)r1 << 32) | r0;
+    uint64_t hi = ((uint64_t)r3 << 32) | r2;
+    uint64_t y = gl_canon(gl_reduce128_lazy(hi, lo));
+    uint64_t z = gl_canon(((uint64_t)r4 << 32) % kGlP);  // r4 * 2^32 < 2^64
+    return gl_sub(y, z);
+  }
+  LC_D static uint64_t add(uint64_t a, uint64_t b, uint32_t) { return gl_add(a, b); }
+};
+
+template <>
+struct Field<uint32_t> {  // any odd u32 modulus q
+  LC_D static uint32_t reduce160(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3, uint32_t r4,
+                                 uint32_t q) {
+    // products are < 2^64 and at most 2^32 of them are summed: r3 = r4 = 0 is
+    // not assumed; fold limb by limb from the top with 64-bit remainders.
+    uint64_t acc = r4 % q;
+    acc = ((acc << 32) | r3) % q;
+    acc = ((acc << 32) | r2) % q;
+    acc = ((acc << 32) | r1) % q;
+    acc = ((acc << 32) | r0) % q;
+    return (uint32_t)acc;
+  }
+  LC_D static uint32_t add(uint32_t a, uint32_t b, uint32_t q) {
+    uint32_t s = a + b;
+    return (s < a || s >= q) ? s - q : s;
+  }
+};
+
+// 160-bit accumulator: outer products a0*b0 and a1*b1 into r0..r4, the two
+// middle products into m0..m2 (added at 2^32 when the sum is reduced).
+struct Acc160 {
+  uint32_t r0 = 0, r1 = 0, r2 = 0, r3 = 0, r4 = 0, m0 = 0, m1 = 0, m2 = 0;
+};
+
+LC_D void mac64(Acc160& c, uint64_t a, uint64_t b) {
+  const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32);
+  const uint32_t b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
+  asm("mad.lo.cc.u32 %0, %5, %7, %0;\n\t"
+      "madc.hi.cc.u32 %1, %5, %7, %1;\n\t"
+      "madc.lo.cc.u32 %2, %6, %8, %2;\n\t"
+      "madc.hi.cc.u32 %3, %6, %8, %3;\n\t"
+      "addc.u32 %4, %4, 0;"
+      : "+r"(c.r0), "+r"(c.r1), "+r"(c.r2), "+r"(c.r3), "+r"(c.r4)
+      : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
+  asm("mad.lo.cc.u32 %0, %3, %6, %0;\n\t"
+      "madc.hi.cc.u32 %1, %3, %6, %1;\n\t"
+      "addc.u32 %2, %2, 0;\n\t"
+      "mad.lo.cc.u32 %0, %4, %5, %0;\n\t"
+      "madc.hi.cc.u32 %1, %4, %5, %1;\n\t"
+      "addc.u32 %2, %2, 0;"
+      : "+r"(c.m0), "+r"(c.m1), "+r"(c.m2)
+      : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
+}
+
+LC_D void mac32(Acc160& c, uint32_t a, uint32_t b) {
+  asm("mad.lo.cc.u32 %0, %3, %4, %0;\n\t"
+      "madc.hi.cc.u32 %1, %3, %4, %1;\n\t"
+      "addc.u32 %2, %2, 0;"
+      : "+r"(c.r0), "+r"(c.r1), "+r"(c.r2)
+      : "r"(a), "r"(b));
+}
+
+template <class E>
+LC_D void mac(Acc160& c, E a, E b);
+template <>
+LC_D void mac<uint64_t>(Acc160& c, uint64_t a, uint64_t b) {
+  mac64(c, a, b);
+}
+template <>
+LC_D void mac<uint32_t>(Acc160& c, uint32_t a, uint32_t b) {
+  mac32(c, a, b);
+}
+
+template <class E>
+LC_D E acc_reduce(const Acc160& c, uint32_t q) {
+  uint32_t r1, r2, r3, r4;
+  asm("add.cc.u32 %0, %4, %7;\n\t"
+      "addc.cc.u32 %1, %5, %8;\n\t"
+      "addc.cc.u32 %2, %6, %9;\n\t"
+      "addc.u32 %3, %10, 0;"
+      : "=r"(r1), "=r"(r2), "=r"(r3), "=r"(r4)
+      : "r"(c.r1), "r"(c.r2), "r"(c.r3), "r"(c.m0), "r"(c.m1), "r"(c.m2), "r"(c.r4));
+  return Field<E>::reduce160(c.r0, r1, r2, r3, r4, q);
+}
+
+// ------------------------------------------------------------------ kernels
+
+// Cached-key layout: Ahat[i][j][t] (k x m ring elements, natural NTT output)
+// -> Ahat_T[t][j][i_pad], rows i >= k zero.  One CTA per witness slot j.
+template <class E>
+__global__ void key_transpose_kernel(const E* __restrict__ ahat, E* __restrict__ out, uint32_t k,
+                                     uint32_t m, uint32_t n) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  E* tile = reinterpret_cast<E*>(smem_raw);  // [kIPad][n]
+  const uint32_t j = blockIdx.x;
+  for (uint32_t e = threadIdx.x; e < (uint32_t)kIPad * n; e += blockDim.x) {
+    const uint32_t i = e / n, t = e % n;
+    tile[e] = i < k ? ahat[((size_t)i * m + j) * n + t] : E(0);
+  }
+  __syncthreads();
+  for (uint32_t e = threadIdx.x; e < (uint32_t)kIPad * n; e += blockDim.x) {
+    const uint32_t t = e / kIPad, i = e % kIPad;
+    out[((size_t)t * m + j) * kIPad + i] = tile[i * n + t];
+  }
+}
+
+// Input element conversion for the witness: residues pass through, int8
+// digits map to their residue (NeoRing::small, lattice-folding/src/neo.rs:98-109).
+template <class E, class S>
+LC_D E to_residue(S x, uint32_t q);
+template <>
+LC_D uint64_t to_residue<uint64_t, uint64_t>(uint64_t x, uint32_t) {
+  return x;
+}
+template <>
+LC_D uint32_t to_residue<uint32_t, uint32_t>(uint32_t x, uint32_t) {
+  return x;
+}
+template <>
+LC_D uint64_t to_residue<uint64_t, int8_t>(int8_t x, uint32_t) {
+  return x >= 0 ? (uint64_t)x : kGlP - (uint64_t)(-(int)x);
+}
+template <>
+LC_D uint32_t to_residue<uint32_t, int8_t>(int8_t x, uint32_t q) {
+  return x >= 0 ? (uint32_t)x : q - (uint32_t)(-(int)x);
+}
+
+// Witness NTT, frequency-major output.  CTA (j, b-block): loads the BB
+// polynomials w[b][j][*], transforms them in shared memory and writes
+// What_T[t][j][b0 + b] (zeros for b >= batch, so the padded columns of the
+// MAC tiles are exact zeros).
+template <class A, class S, int LOG_N, int LOG_V, int NT, int BB>
+__global__ void __launch_bounds__(NT)
+    witness_ntt_kernel(const S* __restrict__ w, typename A::T* __restrict__ what_t, uint32_t m,
+                       uint32_t batch, uint32_t b_pad, const typename A::Tw* __restrict__ twg,
+                       uint32_t q, uint32_t qinv) {
+  using G = Geo<LOG_N, LOG_V>;
+  using SL = Slots<A, LOG_N, LOG_V>;
+  using T = typename A::T;
+  using Tw = typename A::Tw;
+  constexpr int N = G::N, GROUPS = NT / G::T, IT = BB / GROUPS;
+  static_assert(BB % GROUPS == 0, "tile");
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  Tw* tw = reinterpret_cast<Tw*>(smem_raw);
+  T* slots = reinterpret_cast<T*>(smem_raw + ((G::fwd_entries() * sizeof(Tw) + 15) / 16 * 16));
+  const uint32_t j = blockIdx.x;
+  const uint32_t b0 = blockIdx.y * BB;
+  for (int i = threadIdx.x; i < G::fwd_entries(); i += NT) tw[i] = twg[i];
+  for (int e = threadIdx.x; e < BB * N; e += NT) {
+    const int b = e / N, c = e % N;
+    T v = 0;
+    if (b0 + b < batch) v = to_residue<T, S>(w[((size_t)(b0 + b) * m + j) * N + c], q);
+    slots[b * SL::S + c] = v;
+  }
+  __syncthreads();
+  const A ar = make_arith_q<A>(q, qinv);
+  const int grp = threadIdx.x / G::T;
+  const uint32_t t = threadIdx.x % G::T;
+#pragma unroll 1
+  for (int it = 0; it < IT; ++it)
+    transform_slot<A, LOG_N, LOG_V, false>(slots + (it * GROUPS + grp) * SL::S, tw, ar, t);
+  __syncthreads();
+  for (int e = threadIdx.x; e < BB * N; e += NT) {
+    const int tt = e / BB, b = e % BB;
+    if (b0 + b < b_pad) what_t[((size_t)tt * m + j) * b_pad + b0 + b] = slots[b * SL::S + tt];
+  }
+}
+
+// Generic witness path (ring degrees without a fused kernel): element
+// conversion into [b][j][t] residues, then the batched NTT, then this
+// transpose into What_T[t][j][b_pad] (zero columns b >= batch).
+template <class E, class S>
+__global__ void witness_convert_kernel(const S* __restrict__ w, E* __restrict__ out, size_t count,
+                                       uint32_t q) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count;
+       i += (size_t)gridDim.x * blockDim.x)
+    out[i] = to_residue<E, S>(w[i], q);
+}
+
+template <class E>
+__global__ void witness_transpose_kernel(const E* __restrict__ in, E* __restrict__ what_t, uint32_t m,
+                                         uint32_t n, uint32_t batch, uint32_t b_pad) {
+  __shared__ E tile[32][33];
+  const uint32_t j = blockIdx.z;
+  const uint32_t t0 = blockIdx.x * 32, b0 = blockIdx.y * 32;
+  for (uint32_t k = threadIdx.y; k < 32; k += blockDim.y) {
+    const uint32_t b = b0 + k, t = t0 + threadIdx.x;
+    tile[k][threadIdx.x] = (b < batch && t < n) ? in[((size_t)b * m + j) * n + t] : E(0);
+  }
+  __syncthreads();
+  for (uint32_t k = threadIdx.y; k < 32; k += blockDim.y) {
+    const uint32_t t = t0 + k, b = b0 + threadIdx.x;
+    if (t < n && b < b_pad) what_t[((size_t)t * m + j) * b_pad + b] = tile[threadIdx.x][k];
+  }
+}
+
+// Per-frequency product, tiled: CTA (t, b-tile, split) accumulates
+// C_t[i][b] = sum_j Ahat_T[t][j][i] What_T[t][j][b] over its j-range for all
+// 16 (padded) rows and 128 witnesses; 256 threads, each 2 rows x 4 witnesses
+// (witnesses tb, tb+32, tb+64, tb+96).  Shared-memory rows are double-buffered
+// with TMA bulk copies.
+template <class E, int JB>
+struct MacCfg {
+  static constexpr int NT = 256;
+  static constexpr size_t A_BYTES = (size_t)JB * kIPad * sizeof(E);
+  static constexpr size_t W_BYTES = (size_t)JB * kBTile * sizeof(E);
+  static constexpr size_t STAGE = A_BYTES + W_BYTES;
+  static constexpr size_t SMEM = 2 * STAGE + 16;
+};
+
+template <class E, int JB>
+__global__ void __launch_bounds__(256)
+    mac_tiled_kernel(const E* __restrict__ ahat_t, const E* __restrict__ what_t, E* __restrict__ partial,
+                     uint32_t m, uint32_t b_pad, uint32_t n, uint32_t splits, uint32_t q,
+                     uint32_t* err) {
+  using C = MacCfg<E, JB>;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + 2 * C::STAGE);
+  const uint32_t t = blockIdx.x, bt = blockIdx.y, split = blockIdx.z;
+  const uint32_t per = (m + splits - 1) / splits;
+  const uint32_t j0 = split * per, j1 = min(m, j0 + per);
+  const int tid = threadIdx.x;
+  const int ti = tid >> 5, tb = tid & 31;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  auto stage_a = [&](int s) { return reinterpret_cast<E*>(smem_raw + s * C::STAGE); };
+  auto stage_w = [&](int s) { return reinterpret_cast<E*>(smem_raw + s * C::STAGE + C::A_BYTES); };
+  auto issue = [&](uint32_t jb, int s) {
+    const uint32_t rows = min((uint32_t)JB, j1 - jb);
+    const uint32_t a_bytes = rows * kIPad * sizeof(E);
+    mbar_arrive_expect_tx(&bar[s], a_bytes + rows * kBTile * (uint32_t)sizeof(E));
+    bulk_g2s(stage_a(s), ahat_t + ((size_t)t * m + jb) * kIPad, a_bytes, &bar[s]);
+    if (b_pad == kBTile) {
+      bulk_g2s(stage_w(s), what_t + ((size_t)t * m + jb) * b_pad, rows * kBTile * sizeof(E), &bar[s]);
+    } else {
+      for (uint32_t r = 0; r < rows; ++r)
+        bulk_g2s(stage_w(s) + r * kBTile, what_t + ((size_t)t * m + jb + r) * b_pad + bt * kBTile,
+                 kBTile * sizeof(E), &bar[s]);
+    }
+  };
+  Acc160 acc[2][4];
+  const uint32_t nblk = (j1 > j0) ? (j1 - j0 + JB - 1) / JB : 0;
+  if (tid == 0 && nblk > 0) issue(j0, 0);
+  uint32_t parity = 0;
+  bool failed = false;
+  uint32_t failed_blk = 0;
+  for (uint32_t k = 0; k < nblk; ++k) {
+    const int s = k & 1;
+    if (tid == 0 && k + 1 < nblk) issue(j0 + (k + 1) * JB, s ^ 1);
+    const bool ok = mbar_wait(&bar[s], (parity >> s) & 1u);
+    parity ^= 1u << s;
+    if (__syncthreads_or(!ok)) {
+      failed = true;
+      failed_blk = k;
+      break;
+    }
+    const E* As = stage_a(s);
+    const E* Ws = stage_w(s);
+    const uint32_t rows = min((uint32_t)JB, j1 - (j0 + k * JB));
+#pragma unroll 2
+    for (uint32_t r = 0; r < rows; ++r) {
+      const E a0 = As[r * kIPad + 2 * ti], a1 = As[r * kIPad + 2 * ti + 1];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const E wv = Ws[r * kBTile + tb + 32 * u];
+        mac<E>(acc[0][u], a0, wv);
+        mac<E>(acc[1][u], a1, wv);
+      }
+    }
+    __syncthreads();  // stage s is refilled by the next iteration's issue
+  }
+  if (failed) {
+    if (tid == 0) {
+      record_error(err, LC_DEVERR_TIMEOUT);
+      // the prefetch of the following block may still be landing (bounded wait)
+      if (failed_blk + 1 < nblk) {
+        const int o = (failed_blk & 1) ^ 1;
+        mbar_wait(&bar[o], (parity >> o) & 1u);
+      }
+    }
+    return;
+  }
+  // partial[split][t][i][b]
+  for (int ii = 0; ii < 2; ++ii)
+    for (int u = 0; u < 4; ++u) {
+      const uint32_t i = 2 * ti + ii, b = bt * kBTile + tb + 32 * u;
+      partial[(((size_t)split * n + t) * kIPad + i) * b_pad + b] = acc_reduce<E>(acc[ii][u], q);
+    }
+}
+
+// Small-batch product: one thread per (split, t, i, b).
+template <class E>
+__global__ void mac_small_kernel(const E* __restrict__ ahat_t, const E* __restrict__ what_t,
+                                 E* __restrict__ partial, uint32_t m, uint32_t b_pad, uint32_t n,
+                                 uint32_t splits, uint32_t kappa, uint32_t batch, uint32_t q) {
+  const size_t total = (size_t)splits * n * kappa * batch;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t b = idx % batch;
+    const uint32_t i = (idx / batch) % kappa;
+    const uint32_t t = (idx / ((size_t)batch * kappa)) % n;
+    const uint32_t split = idx / ((size_t)batch * kappa * n);
+    const uint32_t per = (m + splits - 1) / splits;
+    const uint32_t j0 = split * per, j1 = min(m, j0 + per);
+    Acc160 acc;
+    for (uint32_t j = j0; j < j1; ++j)
+      mac<E>(acc, ahat_t[((size_t)t * m + j) * kIPad + i], what_t[((size_t)t * m + j) * b_pad + b]);
+    partial[(((size_t)split * n + t) * kIPad + i) * b_pad + b] = acc_reduce<E>(acc, q);
+  }
+}
+
+// Chat[b][i][t] = sum_split partial[split][t][i][b]  (mod q)
+template <class E>
+__global__ void reduce_partials_kernel(const E* __restrict__ partial, E* __restrict__ chat,
+                                       uint32_t splits, uint32_t n, uint32_t kappa, uint32_t batch,
+                                       uint32_t b_pad, uint32_t q) {
+  const size_t total = (size_t)batch * kappa * n;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t t = idx % n;
+    const uint32_t i = (idx / n) % kappa;
+    const uint32_t b = idx / ((size_t)n * kappa);
+    E s = 0;
+    for (uint32_t sp = 0; sp < splits; ++sp)
+      s = Field<E>::add(s, partial[(((size_t)sp * n + t) * kIPad + i) * b_pad + b], q);
+    chat[idx] = s;
+  }
+}
+
+}  // namespace lc
+
+using namespace lc;
+
+// ------------------------------------------------------------------ key object
+
+struct lc_ajtai_key {
+  lc_ntt_plan* plan = nullptr;  // owned copy of the ring's plan
+  uint32_t k = 0, m = 0, n = 0, log_n = 0;
+  bool wide = false;           // Goldilocks (u64) or u32
+  void* d_ahat_t = nullptr;    // [n][m][16]
+  // scratch, grown on demand
+  void* d_what_t = nullptr;
+  size_t what_bytes = 0;
+  void* d_partial = nullptr;
+  size_t partial_bytes = 0;
+  void* d_chat = nullptr;
+  size_t chat_bytes = 0;
+  void* d_wtmp = nullptr;  // generic witness path: converted + transformed witnesses
+  size_t wtmp_bytes = 0;
+  void* d_in = nullptr;  // host-API staging
+  size_t in_bytes = 0;
+  void* d_out = nullptr;
+  size_t out_bytes = 0;
+  cudaStream_t host_stream = nullptr;
+  uint32_t* d_err = nullptr;
+};
+
+namespace lc {
+
+static int grow(void** p, size_t* have, size_t need) {
+  if (need <= *have) return LC_OK;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *have = 0;
+  if (cudaMalloc(p, need) != cudaSuccess) {
+    cudaGetLastError();
+    return LC_ERR_OUT_OF_MEMORY;
+  }
+  *have = need;
+  return LC_OK;
+}
+
+static uint32_t choose_splits(uint32_t n, uint32_t btiles, uint32_t m) {
+  const int sms = device_sm_count();
+  const uint32_t target = (uint32_t)std::max(1, sms * 3);  // about three CTAs per SM
+  uint32_t s = std::max<uint32_t>(1, target / std::max<uint32_t>(1, n * btiles));
+  s = std::min<uint32_t>(s, std::max<uint32_t>(1, m / 64));
+  return std::max<uint32_t>(s, 1);
+}
+
+template <class A, int LOG_N, int LOG_V, class S>
+static int launch_witness_ntt(lc_ajtai_key* key, const S* w, size_t batch, uint32_t b_pad,
+                              cudaStream_t st) {
+  using G = Geo<LOG_N, LOG_V>;
+  using SL = Slots<A, LOG_N, LOG_V>;
+  using T = typename A::T;
+  constexpr int NT = 128;
+  constexpr int GROUPS = NT / G::T;
+  constexpr int BB = (GROUPS >= 32) ? GROUPS : 32;
+  const size_t smem = ((G::fwd_entries() * sizeof(typename A::Tw) + 15) / 16 * 16) +
+                      (size_t)BB * SL::S * sizeof(T);
+  auto kern = witness_ntt_kernel<A, S, LOG_N, LOG_V, NT, BB>;
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+      return map_cuda(cudaGetLastError());
+    attr = true;
+  }
+  dim3 grid(key->m, (unsigned)((b_pad + BB - 1) / BB));
+  const lc_ntt_plan* plan = key->plan;
+  kern<<<grid, NT, smem, st>>>(w, reinterpret_cast<T*>(key->d_what_t), key->m, (uint32_t)batch,
+                               b_pad, reinterpret_cast<const typename A::Tw*>(plan->d_tw_fwd),
+                               plan->q[0], plan->qinv[0]);
+  return map_cuda(cudaGetLastError());
+}
+
+template <class E, class S>
+static int witness_ntt_generic(lc_ajtai_key* key, const S* w, size_t batch, uint32_t b_pad,
+                               cudaStream_t st) {
+  const size_t count = batch * key->m * key->n;
+  int rc = grow(&key->d_wtmp, &key->wtmp_bytes, count * sizeof(E));
+  if (rc) return rc;
+  E* tmp = reinterpret_cast<E*>(key->d_wtmp);
+  const unsigned blocks = (unsigned)std::min<size_t>((count + 255) / 256, 65535);
+  witness_convert_kernel<E, S><<<blocks, 256, 0, st>>>(w, tmp, count, key->plan->q[0]);
+  rc = map_cuda(cudaGetLastError());
+  if (rc) return rc;
+  rc = run_ntt(key->plan, tmp, tmp, batch * key->m, false, st);
+  if (rc) return rc;
+  dim3 grid((key->n + 31) / 32, (b_pad + 31) / 32, key->m);
+  witness_transpose_kernel<E><<<grid, dim3(32, 8), 0, st>>>(tmp, reinterpret_cast<E*>(key->d_what_t),
+                                                             key->m, key->n, (uint32_t)batch, b_pad);
+  return map_cuda(cudaGetLastError());
+}
+
+template <class A, class S>
+static int witness_ntt_as(lc_ajtai_key* key, const S* w, size_t batch, uint32_t b_pad, cudaStream_t st) {
+  switch (key->log_n) {
+    case 6: return launch_witness_ntt<A, 6, 3, S>(key, w, batch, b_pad, st);
+    case 7: return launch_witness_ntt<A, 7, 4, S>(key, w, batch, b_pad, st);
+    case 8: return launch_witness_ntt<A, 8, 4, S>(key, w, batch, b_pad, st);
+    default: return witness_ntt_generic<typename A::T, S>(key, w, batch, b_pad, st);
+  }
+}
+
+template <class S>
+static int witness_ntt(lc_ajtai_key* key, const S* w, size_t batch, uint32_t b_pad, cudaStream_t st) {
+  const PlanKind kind = key->plan->kind;
+  if constexpr (!std::is_same<S, uint32_t>::value) {
+    if (kind == PlanKind::Goldilocks) return witness_ntt_as<Goldilocks, S>(key, w, batch, b_pad, st);
+  }
+  if constexpr (!std::is_same<S, uint64_t>::value) {
+    if (kind == PlanKind::U32Lazy) return witness_ntt_as<ShoupLazy, S>(key, w, batch, b_pad, st);
+    if (kind == PlanKind::U32Mont) return witness_ntt_as<MontCanon, S>(key, w, batch, b_pad, st);
+  }
+  return LC_ERR_INVALID_ARGUMENT;
+}
+
+template <class E>
+static int commit_core(lc_ajtai_key* key, size_t batch, uint32_t b_pad, void* out, cudaStream_t st) {
+  const uint32_t n = key->n, m = key->m, kappa = key->k;
+  const uint32_t q = key->plan->q[0];
+  const bool tiled = b_pad % kBTile == 0;
+  const uint32_t btiles = tiled ? b_pad / kBTile : 1;
+  // small batches: about 2^18 threads, each summing a contiguous j-range
+  const size_t outs = (size_t)n * kappa * batch;
+  const uint32_t splits =
+      tiled ? choose_splits(n, btiles, m)
+            : (uint32_t)std::max<size_t>(1, std::min<size_t>(m, ((size_t)1 << 18) / std::max<size_t>(1, outs)));
+  int rc = grow(&key->d_partial, &key->partial_bytes, (size_t)splits * n * kIPad * b_pad * sizeof(E));
+  if (rc) return rc;
+  rc = grow(&key->d_chat, &key->chat_bytes, (size_t)batch * kappa * n * sizeof(E));
+  if (rc) return rc;
+  const E* ahat = reinterpret_cast<const E*>(key->d_ahat_t);
+  const E* what = reinterpret_cast<const E*>(key->d_what_t);
+  E* part = reinterpret_cast<E*>(key->d_partial);
+  if (tiled) {
+    constexpr int JB = sizeof(E) == 8 ? 16 : 32;
+    using MC = MacCfg<E, JB>;
+    auto kern = mac_tiled_kernel<E, JB>;
+    static bool attr = false;
+    if (!attr) {
+      if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MC::SMEM) != cudaSuccess)
+        return map_cuda(cudaGetLastError());
+      attr = true;
+    }
+    kern<<<dim3(n, btiles, splits), MC::NT, MC::SMEM, st>>>(ahat, what, part, m, b_pad, n, splits, q,
+                                                           key->d_err);
+  } else {
+    const size_t total = (size_t)splits * n * kappa * batch;
+    const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, 65535);
+    mac_small_kernel<E><<<blocks, 256, 0, st>>>(ahat, what, part, m, b_pad, n, splits, kappa,
+                                                (uint32_t)batch, q);
+  }
+  rc = map_cuda(cudaGetLastError());
+  if (rc) return rc;
+  {
+    const size_t total = (size_t)batch * kappa * n;
+    const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, 65535);
+    reduce_partials_kernel<E><<<blocks, 256, 0, st>>>(part, reinterpret_cast<E*>(key->d_chat), splits,
+                                                      n, kappa, (uint32_t)batch, b_pad, q);
+    rc = map_cuda(cudaGetLastError());
+    if (rc) return rc;
+  }
+  // inverse NTT of the batch*kappa summed rows, straight into the output
+  return run_ntt(key->plan, key->d_chat, out, (size_t)batch * kappa, true, st);
+}
+
+template <class S>
+static int commit_any(lc_ajtai_key* key, const S* w, size_t batch, void* out, cudaStream_t st) {
+  if (batch == 0) return LC_OK;
+  if (batch > (1u << 24)) return LC_ERR_INVALID_ARGUMENT;
+  const uint32_t b_pad = batch >= 64 ? (uint32_t)((batch + kBTile - 1) / kBTile * kBTile) : (uint32_t)batch;
+  const size_t eb = key->wide ? 8 : 4;
+  int rc = grow(&key->d_what_t, &key->what_bytes, (size_t)key->n * key->m * b_pad * eb);
+  if (rc) return rc;
+  rc = witness_ntt<S>(key, w, batch, b_pad, st);
+  if (rc) return rc;
+  return key->wide ? commit_core<uint64_t>(key, batch, b_pad, out, st)
+                   : commit_core<uint32_t>(key, batch, b_pad, out, st);
+}
+
+}  // namespace lc
+
+extern "C" {
+
+LC_API int lc_ajtai_key_create(const lc_ntt_plan* plan, uint32_t k, uint32_t m, const void* matrix,
+                               int matrix_on_device, lc_ajtai_key** out) {
+  if (!plan || !matrix || !out || k == 0 || m == 0) return LC_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (plan->num_moduli != 1) return LC_ERR_UNSUPPORTED;
+  if (k > (uint32_t)kIPad) return LC_ERR_UNSUPPORTED;
+  if (plan->log_n > (plan->kind == PlanKind::Goldilocks ? 9u : 10u)) return LC_ERR_UNSUPPORTED;
+  lc_ajtai_key* key = new (std::nothrow) lc_ajtai_key();
+  if (!key) return LC_ERR_OUT_OF_MEMORY;
+  key->k = k;
+  key->m = m;
+  key->log_n = plan->log_n;
+  key->n = 1u << plan->log_n;
+  key->wide = plan->kind == PlanKind::Goldilocks;
+  int rc;
+  if (key->wide)
+    rc = lc_ntt_plan_create_goldilocks(plan->log_n, &key->plan);
+  else
+    rc = lc_ntt_plan_create_u32(plan->log_n, plan->q, plan->two_adicity, plan->generator, 1, &key->plan);
+  if (rc) {
+    delete key;
+    return rc;
+  }
+  const size_t eb = key->wide ? 8 : 4;
+  const size_t elems = (size_t)k * m * key->n;
+  void* tmp = nullptr;
+  if (cudaMalloc(&tmp, elems * eb) != cudaSuccess ||
+      cudaMalloc(&key->d_ahat_t, (size_t)key->n * m * kIPad * eb) != cudaSuccess ||
+      cudaMalloc(&key->d_err, 4) != cudaSuccess) {
+    cudaGetLastError();
+    if (tmp) cudaFree(tmp);
+    lc_ajtai_key_destroy(key);
+    return LC_ERR_OUT_OF_MEMORY;
+  }
+  cudaMemset(key->d_err, 0, 4);
+  cudaMemcpy(tmp, matrix, elems * eb, matrix_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice);
+  // cached NTT of every entry (AjtaiPublicKey::from_seed, ajtai.rs:91-96)
+  rc = run_ntt(key->plan, tmp, tmp, (size_t)k * m, false, nullptr);
+  if (!rc) {
+    const size_t smem = (size_t)kIPad * key->n * eb;
+    if (smem > 48 * 1024) {
+      cudaFuncSetAttribute(key_transpose_kernel<uint64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+      cudaFuncSetAttribute(key_transpose_kernel<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+    }
+    if (key->wide)
+      key_transpose_kernel<uint64_t><<<m, 256, smem>>>((const uint64_t*)tmp, (uint64_t*)key->d_ahat_t,
+                                                        k, m, key->n);
+    else
+      key_transpose_kernel<uint32_t><<<m, 256, smem>>>((const uint32_t*)tmp, (uint32_t*)key->d_ahat_t,
+                                                        k, m, key->n);
+    rc = map_cuda(cudaGetLastError());
+  }
+  cudaFree(tmp);
+  if (!rc) rc = map_cuda(cudaDeviceSynchronize());
+  if (rc) {
+    lc_ajtai_key_destroy(key);
+    return rc;
+  }
+  *out = key;
+  return LC_OK;
+}
+
+LC_API void lc_ajtai_key_destroy(lc_ajtai_key* key) {
+  if (!key) return;
+  for (void* p : {key->d_ahat_t, key->d_what_t, key->d_partial, key->d_chat, key->d_wtmp, key->d_in,
+                  key->d_out, (void*)key->d_err})
+    if (p) cudaFree(p);
+  if (key->host_stream) cudaStreamDestroy(key->host_stream);
+  if (key->plan) lc_ntt_plan_destroy(key->plan);
+  delete key;
+}
+
+LC_API int lc_ajtai_commit(lc_ajtai_key* key, const void* s, size_t batch, void* out, lc_stream stream) {
+  if (!key || (!s && batch) || (!out && batch)) return LC_ERR_INVALID_ARGUMENT;
+  if (((uintptr_t)out) & 15) return LC_ERR_INVALID_ARGUMENT;
+  if (key->wide) return commit_any<uint64_t>(key, (const uint64_t*)s, batch, out, (cudaStream_t)stream);
+  return commit_any<uint32_t>(key, (const uint32_t*)s, batch, out, (cudaStream_t)stream);
+}
+
+LC_API int lc_ajtai_commit_i8(lc_ajtai_key* key, const int8_t* s, size_t batch, void* out,
+                              lc_stream stream) {
+  if (!key || (!s && batch) || (!out && batch)) return LC_ERR_INVALID_ARGUMENT;
+  if (((uintptr_t)out) & 15) return LC_ERR_INVALID_ARGUMENT;
+  return commit_any<int8_t>(key, s, batch, out, (cudaStream_t)stream);
+}
+
+static int commit_host(lc_ajtai_key* key, const void* s, size_t in_elem, size_t batch, void* out,
+                       bool i8) {
+  if (!key || (!s && batch) || (!out && batch)) return LC_ERR_INVALID_ARGUMENT;
+  if (batch == 0) return LC_OK;
+  const size_t eb = key->wide ? 8 : 4;
+  const size_t in_bytes = batch * key->m * key->n * in_elem;
+  const size_t out_bytes = batch * key->k * key->n * eb;
+  int rc = grow(&key->d_in, &key->in_bytes, in_bytes);
+  if (!rc) rc = grow(&key->d_out, &key->out_bytes, out_bytes);
+  if (rc) return rc;
+  if (!key->host_stream && cudaStreamCreateWithFlags(&key->host_stream, cudaStreamNonBlocking) != cudaSuccess)
+    return map_cuda(cudaGetLastError());
+  cudaStream_t st = key->host_stream;
+  if (cudaMemcpyAsync(key->d_in, s, in_bytes, cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return map_cuda(cudaGetLastError());
+  rc = i8 ? lc_ajtai_commit_i8(key, (const int8_t*)key->d_in, batch, key->d_out, st)
+          : lc_ajtai_commit(key, key->d_in, batch, key->d_out, st);
+  if (rc) return rc;
+  if (cudaMemcpyAsync(out, key->d_out, out_bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    return map_cuda(cudaGetLastError());
+  return lc_ajtai_key_check(key, st);
+}
+
+LC_API int lc_ajtai_commit_host(lc_ajtai_key* key, const void* s, size_t batch, void* out) {
+  return commit_host(key, s, key ? (key->wide ? 8 : 4) : 0, batch, out, false);
+}
+
+LC_API int lc_ajtai_commit_i8_host(lc_ajtai_key* key, const int8_t* s, size_t batch, void* out) {
+  return commit_host(key, s, 1, batch, out, true);
+}
+
+LC_API int lc_ajtai_key_check(lc_ajtai_key* key, lc_stream stream) {
+  if (!key) return LC_ERR_INVALID_ARGUMENT;
+  cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+  if (e != cudaSuccess) return map_cuda(e);
+  uint32_t flag = 0;
+  if (cudaMemcpy(&flag, key->d_err, 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return map_cuda(cudaGetLastError());
+  if (flag) {
+    cudaMemset(key->d_err, 0, 4);
+    return LC_ERR_TIMEOUT;
+  }
+  return lc_ntt_plan_check(key->plan, stream);
+}
+
+LC_API int lc_ajtai_key_info(const lc_ajtai_key* key, uint32_t* k, uint32_t* m, uint32_t* log_n) {
+  if (!key) return LC_ERR_INVALID_ARGUMENT;
+  if (k) *k = key->k;
+  if (m) *m = key->m;
+  if (log_n) *log_n = key->log_n;
+  return LC_OK;
+}
+
+}  // extern "C"

@@ -91,6 +91,21 @@ LC_D Goldilocks make_arith<Goldilocks>(const NttParams&, uint32_t) {
   return Goldilocks();
 }
 
+template <class A>
+LC_D A make_arith_q(uint32_t q, uint32_t qinv);
+template <>
+LC_D ShoupLazy make_arith_q<ShoupLazy>(uint32_t q, uint32_t) {
+  return ShoupLazy(q);
+}
+template <>
+LC_D MontCanon make_arith_q<MontCanon>(uint32_t q, uint32_t qinv) {
+  return MontCanon(q, qinv);
+}
+template <>
+LC_D Goldilocks make_arith_q<Goldilocks>(uint32_t, uint32_t) {
+  return Goldilocks();
+}
+
 // Shared-memory slot geometry for a tile.
 template <class A, int LOG_N, int LOG_V>
 struct Slots {
