@@ -74,6 +74,7 @@ def _declare(L):
         "lc_ajtai_commit_host": (i32, [P, P, sz, P]),
         "lc_ajtai_commit_i8_host": (i32, [P, P, sz, P]),
         "lc_ajtai_key_check": (i32, [P, P]),
+        "lc_ajtai_commit_noalloc": (i32, [P, P, sz, P, P]),
     }
     optional = {
     }

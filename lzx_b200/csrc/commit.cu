@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 #include <new>
 #include <type_traits>
 #include <vector>
@@ -555,6 +556,135 @@ static int commit_any(lc_ajtai_key* key, const S* w, size_t batch, void* out, cu
                    : commit_core<uint32_t>(key, batch, b_pad, out, st);
 }
 
+// ------------------------------------------------------------------ no-allocation commit
+//
+// Scratch of lc_ajtai_commit_noalloc: one fixed array in device memory, part
+// of this library's module, so a commit through that entry point never calls
+// cudaMalloc/cudaFree.  Every GPU that loads the library holds these bytes
+// until the process exits.  In host code the symbol is only a stand-in; its
+// device address comes from cudaGetSymbolAddress, once per device.
+constexpr size_t kNoAllocScratchBytes = (size_t)16 << 20;  // 16 MiB
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+static void* g_noalloc_addr[kNoAllocMaxDevices];
+static std::mutex g_noalloc_mu;
+
+// Device address of the scratch array on the current device (set up on the
+// first call per device).
+static int noalloc_scratch_addr(unsigned char** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return map_cuda(e);
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return LC_ERR_UNSUPPORTED;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return map_cuda(e);
+    g_noalloc_addr[dev] = p;
+  }
+  *out = static_cast<unsigned char*>(g_noalloc_addr[dev]);
+  return LC_OK;
+}
+
+static size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
+// Witness NTT of the fused path into an explicit destination.
+template <class A, int LOG_N, int LOG_V, class S>
+static int noalloc_witness_ntt(const lc_ajtai_key* key, const S* w, size_t batch, uint32_t b_pad,
+                               typename A::T* dst, cudaStream_t st) {
+  using G = Geo<LOG_N, LOG_V>;
+  using SL = Slots<A, LOG_N, LOG_V>;
+  using T = typename A::T;
+  constexpr int NT = 128;
+  constexpr int GROUPS = NT / G::T;
+  constexpr int BB = (GROUPS >= 32) ? GROUPS : 32;
+  const size_t smem = ((G::fwd_entries() * sizeof(typename A::Tw) + 15) / 16 * 16) +
+                      (size_t)BB * SL::S * sizeof(T);
+  auto kern = witness_ntt_kernel<A, S, LOG_N, LOG_V, NT, BB>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return map_cuda(e);
+  dim3 grid(key->m, (unsigned)((b_pad + BB - 1) / BB));
+  kern<<<grid, NT, smem, st>>>(w, dst, key->m, (uint32_t)batch, b_pad,
+                               reinterpret_cast<const typename A::Tw*>(key->plan->d_tw_fwd),
+                               key->plan->q[0], key->plan->qinv[0]);
+  return map_cuda(cudaGetLastError());
+}
+
+template <class A, class S>
+static int noalloc_witness_as(const lc_ajtai_key* key, const S* w, size_t batch, uint32_t b_pad,
+                              typename A::T* dst, cudaStream_t st) {
+  switch (key->log_n) {
+    case 6: return noalloc_witness_ntt<A, 6, 3, S>(key, w, batch, b_pad, dst, st);
+    case 7: return noalloc_witness_ntt<A, 7, 4, S>(key, w, batch, b_pad, dst, st);
+    case 8: return noalloc_witness_ntt<A, 8, 4, S>(key, w, batch, b_pad, dst, st);
+    default: return LC_ERR_UNSUPPORTED;
+  }
+}
+
+// The commit of commit_any/commit_core with every scratch buffer carved out
+// of the fixed array; rejects requests that do not fit.
+template <class E>
+static int noalloc_commit(const lc_ajtai_key* key, const E* s, size_t batch, void* out, cudaStream_t st) {
+  if (batch == 0) return LC_OK;
+  if (key->log_n < 6 || key->log_n > 8) return LC_ERR_UNSUPPORTED;
+  const uint32_t n = key->n, m = key->m, kappa = key->k;
+  const uint32_t b_pad = batch >= 64 ? (uint32_t)((batch + kBTile - 1) / kBTile * kBTile) : (uint32_t)batch;
+  const bool tiled = b_pad % kBTile == 0;
+  const uint32_t btiles = tiled ? b_pad / kBTile : 1;
+  const size_t what_bytes = align256((size_t)n * m * b_pad * sizeof(E));
+  const size_t chat_bytes = align256((size_t)batch * kappa * n * sizeof(E));
+  const size_t part_unit = (size_t)n * kIPad * b_pad * sizeof(E);  // one K-split
+  if (what_bytes + chat_bytes + part_unit > kNoAllocScratchBytes) return LC_ERR_INVALID_ARGUMENT;
+  const size_t outs = (size_t)n * kappa * batch;
+  uint32_t splits =
+      tiled ? choose_splits(n, btiles, m)
+            : (uint32_t)std::max<size_t>(1, std::min<size_t>(m, ((size_t)1 << 18) / std::max<size_t>(1, outs)));
+  const size_t fit = (kNoAllocScratchBytes - what_bytes - chat_bytes) / part_unit;
+  splits = (uint32_t)std::max<size_t>(1, std::min<size_t>(splits, fit));
+
+  unsigned char* base = nullptr;
+  int rc = noalloc_scratch_addr(&base);
+  if (rc) return rc;
+  E* what = reinterpret_cast<E*>(base);
+  E* chat = reinterpret_cast<E*>(base + what_bytes);
+  E* part = reinterpret_cast<E*>(base + what_bytes + chat_bytes);
+
+  const PlanKind kind = key->plan->kind;
+  if constexpr (std::is_same<E, uint64_t>::value) {
+    rc = noalloc_witness_as<Goldilocks, E>(key, s, batch, b_pad, what, st);
+  } else {
+    rc = kind == PlanKind::U32Lazy ? noalloc_witness_as<ShoupLazy, E>(key, s, batch, b_pad, what, st)
+                                   : noalloc_witness_as<MontCanon, E>(key, s, batch, b_pad, what, st);
+  }
+  if (rc) return rc;
+  const uint32_t q = key->plan->q[0];
+  if (tiled) {
+    constexpr int JB = sizeof(E) == 8 ? 16 : 32;
+    using MC = MacCfg<E, JB>;
+    auto kern = mac_tiled_kernel<E, JB>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MC::SMEM);
+    if (e != cudaSuccess) return map_cuda(e);
+    kern<<<dim3(n, btiles, splits), MC::NT, MC::SMEM, st>>>(
+        reinterpret_cast<const E*>(key->d_ahat_t), what, part, m, b_pad, n, splits, q, key->d_err);
+  } else {
+    const size_t total = (size_t)splits * n * kappa * batch;
+    const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, 65535);
+    mac_small_kernel<E><<<blocks, 256, 0, st>>>(reinterpret_cast<const E*>(key->d_ahat_t), what, part,
+                                                m, b_pad, n, splits, kappa, (uint32_t)batch, q);
+  }
+  rc = map_cuda(cudaGetLastError());
+  if (rc) return rc;
+  const size_t total = (size_t)batch * kappa * n;
+  const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, 65535);
+  reduce_partials_kernel<E><<<blocks, 256, 0, st>>>(part, chat, splits, n, kappa, (uint32_t)batch,
+                                                    b_pad, q);
+  rc = map_cuda(cudaGetLastError());
+  if (rc) return rc;
+  return run_ntt(key->plan, chat, out, (size_t)batch * kappa, true, st);
+}
+
 }  // namespace lc
 
 extern "C" {
@@ -698,6 +828,16 @@ LC_API int lc_ajtai_key_info(const lc_ajtai_key* key, uint32_t* k, uint32_t* m, 
   if (m) *m = key->m;
   if (log_n) *log_n = key->log_n;
   return LC_OK;
+}
+
+LC_API int lc_ajtai_commit_noalloc(const lc_ajtai_key* key, const void* s, size_t batch, void* out,
+                                   lc_stream stream) {
+  if (!key || (!s && batch) || (!out && batch)) return LC_ERR_INVALID_ARGUMENT;
+  if (((uintptr_t)out) & 15) return LC_ERR_INVALID_ARGUMENT;
+  if (batch > (1u << 24)) return LC_ERR_INVALID_ARGUMENT;
+  if (key->wide)
+    return noalloc_commit<uint64_t>(key, (const uint64_t*)s, batch, out, (cudaStream_t)stream);
+  return noalloc_commit<uint32_t>(key, (const uint32_t*)s, batch, out, (cudaStream_t)stream);
 }
 
 }  // extern "C"
