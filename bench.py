@@ -58,6 +58,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-commit", action="store_true", help="skip the Ajtai commit measurement")
+    ap.add_argument("--commit-steps", type=int, default=5)
+    ap.add_argument("--commit-m", type=int, default=1 << 16,
+                    help="witness ring elements per commitment (profiling runs use fewer)")
     ap.add_argument("--variant", type=int, default=None,
                     help="NTT kernel variant (default: autotune on the workload)")
     return ap.parse_args()
@@ -194,6 +198,85 @@ class ClockSampler:
                 if any(r[3].replace('.', '', 1).isdigit() for r in rows) else None}
 
 
+# ------------------------------------------------------------------ commit (second half of the metric)
+
+C_KAPPA, C_M, C_D, C_B = 16, 1 << 16, 64, 128
+C_WORKLOAD = ("Ajtai commit, d=64 Goldilocks, kappa=16, n=2^16 ring elements, B=128 witnesses of "
+              "int8 digits; cached-NTT form")
+
+
+def bench_commit(args, rank, max_over_ranks, barrier, world):
+    """Committed ring elements/s for the 128-witness Goldilocks batch."""
+    C_M = args.commit_m
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from lzx_b200 import GoldilocksAjtaiKey, _lib, synth
+    A = torch.empty(C_KAPPA * C_M * C_D, dtype=torch.int64, device="cuda")
+    synth.fill_device(A, "gl", 4321 + rank, 0)
+    key = GoldilocksAjtaiKey(6, C_KAPPA, C_M, A)
+    del A
+    W = torch.empty(C_B * C_M * C_D, dtype=torch.int8, device="cuda")
+    synth.fill_device(W, "i8", 4321 + rank, 1)
+    out = torch.empty((C_B, C_KAPPA, C_D), dtype=torch.int64, device="cuda")
+    L = _lib.lib()
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    h, wp, op = key.handle, C.c_void_p(W.data_ptr()), C.c_void_p(out.data_ptr())
+    for _ in range(2):
+        _lib.check(L.lc_ajtai_commit_i8(h, wp, C_B, op, st), "commit")
+    torch.cuda.synchronize()
+    K = max(1, args.commit_steps)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(K):
+        L.lc_ajtai_commit_i8(h, wp, C_B, op, st)
+    b.record()
+    torch.cuda.synchronize()
+    _lib.check(L.lc_ajtai_key_check(h, st), "commit check")
+    ms = max_over_ranks(a.elapsed_time(b) / K)
+    elems = C_B * C_M
+    # end to end from pinned host memory (witness in, commitments out)
+    hw = torch.empty(C_B * C_M * C_D, dtype=torch.int8).pin_memory()
+    hw.copy_(W.cpu())
+    hout = torch.empty((C_B, C_KAPPA, C_D), dtype=torch.int64).pin_memory()
+    del W
+    hp, hop = C.c_void_p(hw.data_ptr()), C.c_void_p(hout.data_ptr())
+    _lib.check(L.lc_ajtai_commit_i8_host(h, hp, C_B, hop), "commit host")
+    assert torch.equal(hout, out.cpu())
+    KE = 2
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(KE):
+        L.lc_ajtai_commit_i8_host(h, hp, C_B, hop)
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / KE)
+    res = {"workload": C_WORKLOAD, "unit": "ring-elems/s",
+           "plain": {"value": world * elems / (ms / 1e3), "ms_per_batch": ms, "steps": K,
+                     "e2e": {"value": world * elems / e2e_s, "unit": "ring-elems/s",
+                             "h2d_bytes_per_step": C_B * C_M * C_D,
+                             "d2h_bytes_per_step": C_B * C_KAPPA * C_D * 8}},
+           "alg_mul_adds_per_batch": C_KAPPA * C_M * C_D * C_B}
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracle
+        oracle.prefer_native(True)
+        nt = host_threads()
+        t = oracle.NttTablesGl(6)
+        a_host = synth.synth_gl(4321, 0, C_KAPPA * C_M * C_D)
+        a_ntt = t.forward_batch(a_host, nthreads=nt)
+        wb = synth.synth_i8(4321, 1, 4 * C_M * C_D).reshape(4, C_M, C_D)
+        t0 = time.perf_counter()
+        oracle.ajtaigl_commit_batch(t, a_ntt, C_KAPPA, C_M, wb, nthreads=nt, simd=True, native=True)
+        dt = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": 4 * C_M / dt, "unit": "ring-elems/s", "cores": nt,
+                               "kind": "port",
+                               "sample": f"4 of the 128 witnesses, full n=2^16, {nt} threads, "
+                                         "AVX-512 Goldilocks MAC where available"}
+    return res
+
+
 # ------------------------------------------------------------------ our arm
 
 def run_ours(args):
@@ -306,6 +389,8 @@ def run_ours(args):
     assert torch.equal(hout, hin)
     e2e_value = world * TRANSFORMS_PER_STEP * COEFFS * KE / e2e_s
 
+    commit = None if args.no_commit else bench_commit(args, rank, max_over_ranks, barrier, world)
+
     if dist is not None:
         dist.destroy_process_group()
     if rank != 0:
@@ -359,6 +444,7 @@ def run_ours(args):
                 "steps": KE, "api": "lc_ntt_forward_host + lc_ntt_inverse_host, pinned host memory"},
         "gpu_launches": 2 * K,
         "clocks": clocks,
+        "commit": commit,
     }
     print(json.dumps(line), flush=True)
     return 0

@@ -172,6 +172,14 @@ LC_API int lc_ajtai_key_check(lc_ajtai_key *key, lc_stream stream);
 LC_API int lc_ajtai_commit_noalloc(const lc_ajtai_key *key, const void *s, size_t batch, void *out,
                                    lc_stream stream);
 
+/* Benchmark/test utility, no counterpart in the reference: fill `count`
+ * elements of `out` (device) with the seeded counter-based synthetic stream
+ * x_i = H(seed, stream, offset + i): kind 0 raw u64, 1 u32 residues mod q
+ * (rejection below 2^32 - 2^32 mod q, as ring.rs:123), 2 Goldilocks residues,
+ * 3 int8 digits.  Bit-identical to lzx_b200/synth.py. */
+LC_API int lc_synth_fill(int kind, uint64_t seed, uint64_t stream, uint32_t q, void *out,
+                         size_t count, size_t offset, lc_stream stream_handle);
+
 #ifdef __cplusplus
 }
 #endif

@@ -75,6 +75,7 @@ def _declare(L):
         "lc_ajtai_commit_i8_host": (i32, [P, P, sz, P]),
         "lc_ajtai_key_check": (i32, [P, P]),
         "lc_ajtai_commit_noalloc": (i32, [P, P, sz, P, P]),
+        "lc_synth_fill": (i32, [i32, C.c_uint64, C.c_uint64, u32, P, sz, sz, P]),
     }
     optional = {
     }

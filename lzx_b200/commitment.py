@@ -57,12 +57,15 @@ def _map_status(st: int, where: str):
 class _DeviceKey:
     """Owns one ``lc_ajtai_key``."""
 
-    def __init__(self, plan, k: int, m: int, matrix: np.ndarray):
+    def __init__(self, plan, k: int, m: int, matrix):
         h = C.c_void_p()
-        matrix = np.ascontiguousarray(matrix)
-        _map_status(_lib.lib().lc_ajtai_key_create(plan.handle, k, m,
-                                                   matrix.ctypes.data_as(C.c_void_p), 0,
-                                                   C.byref(h)), "lc_ajtai_key_create")
+        if _is_torch_cuda(matrix):
+            ptr, on_dev = C.c_void_p(matrix.contiguous().data_ptr()), 1
+        else:
+            matrix = np.ascontiguousarray(matrix)
+            ptr, on_dev = matrix.ctypes.data_as(C.c_void_p), 0
+        _map_status(_lib.lib().lc_ajtai_key_create(plan.handle, k, m, ptr, on_dev, C.byref(h)),
+                    "lc_ajtai_key_create")
         self._h = h
         self.k, self.m, self.n = k, m, plan.n
         self.elem_dtype = plan.elem_dtype
@@ -235,9 +238,14 @@ class GoldilocksAjtaiKey:
     def __init__(self, log_d: int, kappa: int, m: int, matrix):
         self.tables = GoldilocksNttTables(log_d)
         self.d, self.kappa, self.m = 1 << log_d, kappa, m
-        mat = np.ascontiguousarray(matrix, dtype=np.uint64)
-        if mat.size != kappa * m * self.d:
-            raise AjtaiError("DimensionMismatch", expected=kappa * m * self.d, got=mat.size)
+        if _is_torch_cuda(matrix):
+            size = matrix.numel()
+            mat = matrix
+        else:
+            mat = np.ascontiguousarray(matrix, dtype=np.uint64)
+            size = mat.size
+        if size != kappa * m * self.d:
+            raise AjtaiError("DimensionMismatch", expected=kappa * m * self.d, got=size)
         self._dev = _DeviceKey(self.tables, kappa, m, mat)
 
     @property

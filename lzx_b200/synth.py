@@ -86,3 +86,24 @@ def crt_batch(seed: int, moduli, count: int, n: int) -> np.ndarray:
         q = m.q if hasattr(m, "q") else int(m)
         out[i] = synth_mod32(seed, i, q, count * n).reshape(count, n)
     return out
+
+
+# ----------------------------------------------------------------- on the device
+
+_KIND = {"u64": 0, "mod32": 1, "gl": 2, "i8": 3}
+
+
+def fill_device(tensor, kind: str, seed: int, stream: int, q: int = 0, offset: int = 0):
+    """Fill a contiguous CUDA tensor with the same stream on the GPU
+    (``lc_synth_fill``); int32/int64/int8 tensors hold u32/u64/int8 values."""
+    import ctypes as C
+
+    import torch
+
+    from . import _lib
+    assert tensor.is_cuda and tensor.is_contiguous()
+    st = _lib.lib().lc_synth_fill(_KIND[kind], seed & 0xFFFFFFFFFFFFFFFF, stream & 0xFFFFFFFFFFFFFFFF,
+                                  q, C.c_void_p(tensor.data_ptr()), tensor.numel(), offset,
+                                  C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    _lib.check(st, "lc_synth_fill")
+    return tensor

@@ -216,3 +216,20 @@ def test_every_kernel_variant_is_bit_exact(variant):
     assert np.array_equal(fg, oracle.NttTablesGl(6).forward_batch(g))
     assert np.array_equal(tg.inverse_fast(fg.copy()), g)
     assert _lib.lib().lc_ntt_plan_set_variant(t.handle, 5) == _lib.LC_ERR_INVALID_ARGUMENT
+
+
+def test_device_synth_matches_host_generator():
+    """lc_synth_fill reproduces the seeded host stream bit for bit."""
+    n = 100_003
+    for kind, q, dt, host in (("u64", 0, torch.int64, lambda: synth.synth_u64(7, 3, n, 11)),
+                              ("mod32", Modulus32.Q_32.q, torch.int32,
+                               lambda: synth.synth_mod32(7, 3, Modulus32.Q_32.q, n, 11)),
+                              ("mod32", CRT_SET_30BIT[0].q, torch.int32,
+                               lambda: synth.synth_mod32(7, 3, CRT_SET_30BIT[0].q, n, 11)),
+                              ("gl", 0, torch.int64, lambda: synth.synth_gl(7, 3, n, 11)),
+                              ("i8", 0, torch.int8, lambda: synth.synth_i8(7, 3, n, 11))):
+        t = torch.empty(n, dtype=dt, device="cuda")
+        synth.fill_device(t, kind, 7, 3, q, offset=11)
+        got = t.cpu().numpy()
+        want = host()
+        assert np.array_equal(got.view(want.dtype), want), kind
