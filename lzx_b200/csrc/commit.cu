@@ -167,32 +167,71 @@ LC_D uint32_t to_residue<uint32_t, int8_t>(int8_t x, uint32_t q) {
   return x >= 0 ? (uint32_t)x : q - (uint32_t)(-(int)x);
 }
 
-// Witness NTT, frequency-major output.  CTA (j, b-block): loads the BB
-// polynomials w[b][j][*], transforms them in shared memory and writes
-// What_T[t][j][b0 + b] (zeros for b >= batch, so the padded columns of the
-// MAC tiles are exact zeros).
+// Witness NTT, frequency-major output.  CTA (j, b-block of BB witnesses):
+// loads the BB polynomials w[b][j][*] (16-byte vector loads when aligned),
+// transforms them in shared memory and writes What_T[t][j][b0 + b] -- for
+// each NTT slot t one contiguous run of BB values -- with zeros for
+// b >= batch so the padded columns of the product tiles are exact zeros.
+// Slots are SS elements apart: odd strides keep the transposed store
+// bank-conflict free.
+template <class A, int LOG_N>
+struct WitnessSlotStride;
+template <class A>
+struct WitnessSlotStride<A, 6> {
+  static constexpr int value = sizeof(typename A::T) == 8 ? 73 : 75;
+};
+template <class A>
+struct WitnessSlotStride<A, 7> {
+  static constexpr int value = 137;
+};
+template <class A>
+struct WitnessSlotStride<A, 8> {
+  static constexpr int value = 273;
+};
+
 template <class A, class S, int LOG_N, int LOG_V, int NT, int BB>
 __global__ void __launch_bounds__(NT)
     witness_ntt_kernel(const S* __restrict__ w, typename A::T* __restrict__ what_t, uint32_t m,
                        uint32_t batch, uint32_t b_pad, const typename A::Tw* __restrict__ twg,
                        uint32_t q, uint32_t qinv) {
   using G = Geo<LOG_N, LOG_V>;
-  using SL = Slots<A, LOG_N, LOG_V>;
   using T = typename A::T;
   using Tw = typename A::Tw;
   constexpr int N = G::N, GROUPS = NT / G::T, IT = BB / GROUPS;
+  constexpr int SS = WitnessSlotStride<A, LOG_N>::value;
   static_assert(BB % GROUPS == 0, "tile");
+  static_assert(SS >= Slots<A, LOG_N, LOG_V>::S, "slot stride");
   extern __shared__ __align__(128) unsigned char smem_raw[];
   Tw* tw = reinterpret_cast<Tw*>(smem_raw);
   T* slots = reinterpret_cast<T*>(smem_raw + ((G::fwd_entries() * sizeof(Tw) + 15) / 16 * 16));
   const uint32_t j = blockIdx.x;
   const uint32_t b0 = blockIdx.y * BB;
   for (int i = threadIdx.x; i < G::fwd_entries(); i += NT) tw[i] = twg[i];
-  for (int e = threadIdx.x; e < BB * N; e += NT) {
-    const int b = e / N, c = e % N;
-    T v = 0;
-    if (b0 + b < batch) v = to_residue<T, S>(w[((size_t)(b0 + b) * m + j) * N + c], q);
-    slots[b * SL::S + c] = v;
+  constexpr int EPC = 16 / sizeof(S);  // elements per 16-byte chunk
+  constexpr int CH = N / EPC;          // chunks per polynomial
+  const bool vec = (N * sizeof(S)) % 16 == 0 && (reinterpret_cast<uintptr_t>(w) & 15) == 0;
+  if (vec) {
+    for (int e = threadIdx.x; e < BB * CH; e += NT) {
+      const int b = e / CH, k = e % CH;
+      T* dst = slots + b * SS + k * EPC;
+      if (b0 + b < batch) {
+        const uint4 v =
+            *reinterpret_cast<const uint4*>(w + ((size_t)(b0 + b) * m + j) * N + (size_t)k * EPC);
+        const S* x = reinterpret_cast<const S*>(&v);
+#pragma unroll
+        for (int u = 0; u < EPC; ++u) dst[u] = to_residue<T, S>(x[u], q);
+      } else {
+#pragma unroll
+        for (int u = 0; u < EPC; ++u) dst[u] = 0;
+      }
+    }
+  } else {
+    for (int e = threadIdx.x; e < BB * N; e += NT) {
+      const int b = e / N, c = e % N;
+      T v = 0;
+      if (b0 + b < batch) v = to_residue<T, S>(w[((size_t)(b0 + b) * m + j) * N + c], q);
+      slots[b * SS + c] = v;
+    }
   }
   __syncthreads();
   const A ar = make_arith_q<A>(q, qinv);
@@ -200,11 +239,11 @@ __global__ void __launch_bounds__(NT)
   const uint32_t t = threadIdx.x % G::T;
 #pragma unroll 1
   for (int it = 0; it < IT; ++it)
-    transform_slot<A, LOG_N, LOG_V, false>(slots + (it * GROUPS + grp) * SL::S, tw, ar, t);
+    transform_slot<A, LOG_N, LOG_V, false>(slots + (it * GROUPS + grp) * SS, tw, ar, t);
   __syncthreads();
   for (int e = threadIdx.x; e < BB * N; e += NT) {
     const int tt = e / BB, b = e % BB;
-    if (b0 + b < b_pad) what_t[((size_t)tt * m + j) * b_pad + b0 + b] = slots[b * SL::S + tt];
+    if (b0 + b < b_pad) what_t[((size_t)tt * m + j) * b_pad + b0 + b] = slots[b * SS + tt];
   }
 }
 
@@ -424,30 +463,46 @@ static uint32_t choose_splits(uint32_t n, uint32_t btiles, uint32_t m) {
   return std::max<uint32_t>(s, 1);
 }
 
+template <class A, int LOG_N, int LOG_V, class S, int NT, int BB>
+static int launch_witness_cfg(const lc_ajtai_key* key, const S* w, size_t batch, uint32_t b_pad,
+                              typename A::T* dst, cudaStream_t st) {
+  using G = Geo<LOG_N, LOG_V>;
+  using T = typename A::T;
+  constexpr int SS = WitnessSlotStride<A, LOG_N>::value;
+  const size_t smem = ((G::fwd_entries() * sizeof(typename A::Tw) + 15) / 16 * 16) +
+                      (size_t)BB * SS * sizeof(T);
+  auto kern = witness_ntt_kernel<A, S, LOG_N, LOG_V, NT, BB>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return map_cuda(e);
+  dim3 grid(key->m, (unsigned)((b_pad + BB - 1) / BB));
+  const lc_ntt_plan* plan = key->plan;
+  kern<<<grid, NT, smem, st>>>(w, dst, key->m, (uint32_t)batch, b_pad,
+                               reinterpret_cast<const typename A::Tw*>(plan->d_tw_fwd), plan->q[0],
+                               plan->qinv[0]);
+  return map_cuda(cudaGetLastError());
+}
+
+// 128 witnesses per CTA when the batch is tiled and 128 slots fit in 160 KB of
+// shared memory (64 otherwise), 32 for small batches.
+template <class A, int LOG_N, int LOG_V, class S>
+static int launch_witness_to(const lc_ajtai_key* key, const S* w, size_t batch, uint32_t b_pad,
+                             typename A::T* dst, cudaStream_t st) {
+  constexpr bool fits128 =
+      (size_t)128 * WitnessSlotStride<A, LOG_N>::value * sizeof(typename A::T) <= 160 * 1024;
+  if (b_pad % 128 == 0) {
+    if constexpr (fits128)
+      return launch_witness_cfg<A, LOG_N, LOG_V, S, 256, 128>(key, w, batch, b_pad, dst, st);
+    else
+      return launch_witness_cfg<A, LOG_N, LOG_V, S, 256, 64>(key, w, batch, b_pad, dst, st);
+  }
+  return launch_witness_cfg<A, LOG_N, LOG_V, S, 128, 32>(key, w, batch, b_pad, dst, st);
+}
+
 template <class A, int LOG_N, int LOG_V, class S>
 static int launch_witness_ntt(lc_ajtai_key* key, const S* w, size_t batch, uint32_t b_pad,
                               cudaStream_t st) {
-  using G = Geo<LOG_N, LOG_V>;
-  using SL = Slots<A, LOG_N, LOG_V>;
-  using T = typename A::T;
-  constexpr int NT = 128;
-  constexpr int GROUPS = NT / G::T;
-  constexpr int BB = (GROUPS >= 32) ? GROUPS : 32;
-  const size_t smem = ((G::fwd_entries() * sizeof(typename A::Tw) + 15) / 16 * 16) +
-                      (size_t)BB * SL::S * sizeof(T);
-  auto kern = witness_ntt_kernel<A, S, LOG_N, LOG_V, NT, BB>;
-  static bool attr = false;
-  if (!attr) {
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-      return map_cuda(cudaGetLastError());
-    attr = true;
-  }
-  dim3 grid(key->m, (unsigned)((b_pad + BB - 1) / BB));
-  const lc_ntt_plan* plan = key->plan;
-  kern<<<grid, NT, smem, st>>>(w, reinterpret_cast<T*>(key->d_what_t), key->m, (uint32_t)batch,
-                               b_pad, reinterpret_cast<const typename A::Tw*>(plan->d_tw_fwd),
-                               plan->q[0], plan->qinv[0]);
-  return map_cuda(cudaGetLastError());
+  return launch_witness_to<A, LOG_N, LOG_V, S>(key, w, batch, b_pad,
+                                               reinterpret_cast<typename A::T*>(key->d_what_t), st);
 }
 
 template <class E, class S>
@@ -594,22 +649,7 @@ static size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 template <class A, int LOG_N, int LOG_V, class S>
 static int noalloc_witness_ntt(const lc_ajtai_key* key, const S* w, size_t batch, uint32_t b_pad,
                                typename A::T* dst, cudaStream_t st) {
-  using G = Geo<LOG_N, LOG_V>;
-  using SL = Slots<A, LOG_N, LOG_V>;
-  using T = typename A::T;
-  constexpr int NT = 128;
-  constexpr int GROUPS = NT / G::T;
-  constexpr int BB = (GROUPS >= 32) ? GROUPS : 32;
-  const size_t smem = ((G::fwd_entries() * sizeof(typename A::Tw) + 15) / 16 * 16) +
-                      (size_t)BB * SL::S * sizeof(T);
-  auto kern = witness_ntt_kernel<A, S, LOG_N, LOG_V, NT, BB>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return map_cuda(e);
-  dim3 grid(key->m, (unsigned)((b_pad + BB - 1) / BB));
-  kern<<<grid, NT, smem, st>>>(w, dst, key->m, (uint32_t)batch, b_pad,
-                               reinterpret_cast<const typename A::Tw*>(key->plan->d_tw_fwd),
-                               key->plan->q[0], key->plan->qinv[0]);
-  return map_cuda(cudaGetLastError());
+  return launch_witness_to<A, LOG_N, LOG_V, S>(key, w, batch, b_pad, dst, st);
 }
 
 template <class A, class S>
