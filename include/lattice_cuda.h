@@ -150,6 +150,31 @@ LC_API int lc_ajtai_commit_i8_host(lc_ajtai_key *key, const int8_t *s, size_t ba
 /* Wait for `stream` and report device-side errors of this key's kernels. */
 LC_API int lc_ajtai_key_check(lc_ajtai_key *key, lc_stream stream);
 
+/* Key creation flags. */
+#define LC_KEY_TENSOR_I8 1u /* also build the INT8 tensor-core commit tables */
+
+/* lc_ajtai_key_create with flags.  LC_KEY_TENSOR_I8 (Goldilocks plans with
+ * log_n == 6 only, else LC_ERR_UNSUPPORTED) additionally stores every entry
+ * of A as byte limbs of its negacyclic rotation (16 KiB per j for every 16
+ * rows i, twice the size of A) for the tensor-core engine of
+ * lc_ajtai_commit_i8, and makes that engine the key's default.  This is the
+ * limb-split form of the coefficient-domain commit
+ * (lattice-folding/src/neo.rs:138-158, 419-441); the results are identical
+ * to the NTT engine's. */
+LC_API int lc_ajtai_key_create_ex(const lc_ntt_plan *plan, uint32_t k, uint32_t m, const void *matrix,
+                                  int matrix_on_device, uint32_t flags, lc_ajtai_key **out);
+
+/* Which engine lc_ajtai_commit_i8 (and lc_ajtai_commit_i8_host) uses:
+ * LC_ENGINE_NTT (cached-NTT multiply-accumulate, every key) or
+ * LC_ENGINE_TENSOR_I8 (keys created with LC_KEY_TENSOR_I8; exact s8 x u8
+ * products on the tensor cores, per-limb int32 sums of at most 1024 ring
+ * elements, exact 128-bit reduction).  Residue witnesses (lc_ajtai_commit)
+ * always use the NTT engine. */
+#define LC_ENGINE_NTT 0
+#define LC_ENGINE_TENSOR_I8 1
+LC_API int lc_ajtai_key_set_engine(lc_ajtai_key *key, int engine);
+LC_API int lc_ajtai_key_get_engine(const lc_ajtai_key *key);
+
 /* Commit without allocating any device memory.  No counterpart in the
  * reference: it exists for callers that cannot call cudaMalloc while they
  * commit -- code that records work into a CUDA graph, processes whose device

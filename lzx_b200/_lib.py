@@ -28,6 +28,10 @@ LC_ERR_OUT_OF_MEMORY = 10
 LC_ERR_TIMEOUT = 11
 LC_ERR_NO_DEVICE = 12
 
+LC_KEY_TENSOR_I8 = 1
+LC_ENGINE_NTT = 0
+LC_ENGINE_TENSOR_I8 = 1
+
 
 class LatticeCudaError(RuntimeError):
     """A non-zero lc_status returned by the C ABI."""
@@ -75,6 +79,9 @@ def _declare(L):
         "lc_ajtai_commit_i8_host": (i32, [P, P, sz, P]),
         "lc_ajtai_key_check": (i32, [P, P]),
         "lc_ajtai_commit_noalloc": (i32, [P, P, sz, P, P]),
+        "lc_ajtai_key_create_ex": (i32, [P, u32, u32, P, i32, u32, C.POINTER(P)]),
+        "lc_ajtai_key_set_engine": (i32, [P, i32]),
+        "lc_ajtai_key_get_engine": (i32, [P]),
         "lc_synth_fill": (i32, [i32, C.c_uint64, C.c_uint64, u32, P, sz, sz, P]),
     }
     optional = {

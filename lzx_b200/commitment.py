@@ -57,15 +57,16 @@ def _map_status(st: int, where: str):
 class _DeviceKey:
     """Owns one ``lc_ajtai_key``."""
 
-    def __init__(self, plan, k: int, m: int, matrix):
+    def __init__(self, plan, k: int, m: int, matrix, flags: int = 0):
         h = C.c_void_p()
         if _is_torch_cuda(matrix):
-            ptr, on_dev = C.c_void_p(matrix.contiguous().data_ptr()), 1
+            matrix = matrix.contiguous()
+            ptr, on_dev = C.c_void_p(matrix.data_ptr()), 1
         else:
             matrix = np.ascontiguousarray(matrix)
             ptr, on_dev = matrix.ctypes.data_as(C.c_void_p), 0
-        _map_status(_lib.lib().lc_ajtai_key_create(plan.handle, k, m, ptr, on_dev, C.byref(h)),
-                    "lc_ajtai_key_create")
+        _map_status(_lib.lib().lc_ajtai_key_create_ex(plan.handle, k, m, ptr, on_dev, flags, C.byref(h)),
+                    "lc_ajtai_key_create_ex")
         self._h = h
         self.k, self.m, self.n = k, m, plan.n
         self.elem_dtype = plan.elem_dtype
@@ -73,6 +74,14 @@ class _DeviceKey:
     @property
     def handle(self):
         return self._h
+
+    @property
+    def engine(self) -> int:
+        return _lib.lib().lc_ajtai_key_get_engine(self._h)
+
+    @engine.setter
+    def engine(self, value: int):
+        check(_lib.lib().lc_ajtai_key_set_engine(self._h, int(value)), "lc_ajtai_key_set_engine")
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -235,7 +244,12 @@ class GoldilocksAjtaiKey:
     ``NeoAjtaiKey::commit_naive`` (lattice-folding/src/neo.rs:419-441).
     """
 
-    def __init__(self, log_d: int, kappa: int, m: int, matrix):
+    ENGINE_NTT = _lib.LC_ENGINE_NTT
+    ENGINE_TENSOR_I8 = _lib.LC_ENGINE_TENSOR_I8
+
+    def __init__(self, log_d: int, kappa: int, m: int, matrix, tensor_cores: bool = False):
+        """``tensor_cores=True`` (d = 64 only) also builds the INT8 tensor-core
+        tables and makes that engine the default for int8 witnesses."""
         self.tables = GoldilocksNttTables(log_d)
         self.d, self.kappa, self.m = 1 << log_d, kappa, m
         if _is_torch_cuda(matrix):
@@ -246,11 +260,21 @@ class GoldilocksAjtaiKey:
             size = mat.size
         if size != kappa * m * self.d:
             raise AjtaiError("DimensionMismatch", expected=kappa * m * self.d, got=size)
-        self._dev = _DeviceKey(self.tables, kappa, m, mat)
+        self._dev = _DeviceKey(self.tables, kappa, m, mat,
+                               _lib.LC_KEY_TENSOR_I8 if tensor_cores else 0)
 
     @property
     def handle(self):
         return self._dev.handle
+
+    @property
+    def engine(self) -> int:
+        """Engine for int8 witnesses: ENGINE_NTT or ENGINE_TENSOR_I8."""
+        return self._dev.engine
+
+    @engine.setter
+    def engine(self, value: int):
+        self._dev.engine = value
 
     def commit(self, w, out=None):
         return self._dev.commit_array(w, out)

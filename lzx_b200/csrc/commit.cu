@@ -438,6 +438,8 @@ struct lc_ajtai_key {
   size_t out_bytes = 0;
   cudaStream_t host_stream = nullptr;
   uint32_t* d_err = nullptr;
+  lc_tc_tables* tc = nullptr;  // tensor-core engine tables (LC_KEY_TENSOR_I8)
+  int engine = LC_ENGINE_NTT;
 };
 
 namespace lc {
@@ -731,9 +733,17 @@ extern "C" {
 
 LC_API int lc_ajtai_key_create(const lc_ntt_plan* plan, uint32_t k, uint32_t m, const void* matrix,
                                int matrix_on_device, lc_ajtai_key** out) {
+  return lc_ajtai_key_create_ex(plan, k, m, matrix, matrix_on_device, 0, out);
+}
+
+LC_API int lc_ajtai_key_create_ex(const lc_ntt_plan* plan, uint32_t k, uint32_t m, const void* matrix,
+                                  int matrix_on_device, uint32_t flags, lc_ajtai_key** out) {
   if (!plan || !matrix || !out || k == 0 || m == 0) return LC_ERR_INVALID_ARGUMENT;
   *out = nullptr;
+  if (flags & ~LC_KEY_TENSOR_I8) return LC_ERR_INVALID_ARGUMENT;
   if (plan->num_moduli != 1) return LC_ERR_UNSUPPORTED;
+  if ((flags & LC_KEY_TENSOR_I8) && (plan->kind != PlanKind::Goldilocks || plan->log_n != 6))
+    return LC_ERR_UNSUPPORTED;
   if (k > (uint32_t)kIPad) return LC_ERR_UNSUPPORTED;
   if (plan->log_n > (plan->kind == PlanKind::Goldilocks ? 9u : 10u)) return LC_ERR_UNSUPPORTED;
   lc_ajtai_key* key = new (std::nothrow) lc_ajtai_key();
@@ -765,6 +775,16 @@ LC_API int lc_ajtai_key_create(const lc_ntt_plan* plan, uint32_t k, uint32_t m, 
   }
   cudaMemset(key->d_err, 0, 4);
   cudaMemcpy(tmp, matrix, elems * eb, matrix_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice);
+  // rotation-limb tables from the coefficient form (before it is transformed in place)
+  if (flags & LC_KEY_TENSOR_I8) {
+    rc = tc_tables_create(static_cast<const uint64_t*>(tmp), k, m, &key->tc);
+    if (rc) {
+      cudaFree(tmp);
+      lc_ajtai_key_destroy(key);
+      return rc;
+    }
+    key->engine = LC_ENGINE_TENSOR_I8;
+  }
   // cached NTT of every entry (AjtaiPublicKey::from_seed, ajtai.rs:91-96)
   rc = run_ntt(key->plan, tmp, tmp, (size_t)k * m, false, nullptr);
   if (!rc) {
@@ -800,8 +820,18 @@ LC_API void lc_ajtai_key_destroy(lc_ajtai_key* key) {
     if (p) cudaFree(p);
   if (key->host_stream) cudaStreamDestroy(key->host_stream);
   if (key->plan) lc_ntt_plan_destroy(key->plan);
+  tc_tables_destroy(key->tc);
   delete key;
 }
+
+LC_API int lc_ajtai_key_set_engine(lc_ajtai_key* key, int engine) {
+  if (!key || (engine != LC_ENGINE_NTT && engine != LC_ENGINE_TENSOR_I8)) return LC_ERR_INVALID_ARGUMENT;
+  if (engine == LC_ENGINE_TENSOR_I8 && !key->tc) return LC_ERR_UNSUPPORTED;
+  key->engine = engine;
+  return LC_OK;
+}
+
+LC_API int lc_ajtai_key_get_engine(const lc_ajtai_key* key) { return key ? key->engine : -1; }
 
 LC_API int lc_ajtai_commit(lc_ajtai_key* key, const void* s, size_t batch, void* out, lc_stream stream) {
   if (!key || (!s && batch) || (!out && batch)) return LC_ERR_INVALID_ARGUMENT;
@@ -814,6 +844,8 @@ LC_API int lc_ajtai_commit_i8(lc_ajtai_key* key, const int8_t* s, size_t batch, 
                               lc_stream stream) {
   if (!key || (!s && batch) || (!out && batch)) return LC_ERR_INVALID_ARGUMENT;
   if (((uintptr_t)out) & 15) return LC_ERR_INVALID_ARGUMENT;
+  if (key->engine == LC_ENGINE_TENSOR_I8)
+    return tc_commit_i8(key->tc, s, batch, static_cast<uint64_t*>(out), key->d_err, (cudaStream_t)stream);
   return commit_any<int8_t>(key, s, batch, out, (cudaStream_t)stream);
 }
 

@@ -1,0 +1,471 @@
+// tc_commit.cu -- Ajtai commitment over Goldilocks (d = 64) on the INT8
+// tensor cores (tcgen05.mma .kind::i8, sm_100a), exact.
+//
+// Coefficient-domain form of the commitment (lattice-folding/src/neo.rs:
+// 138-158 and 419-441; the same map as AjtaiPublicKey::commit, ajtai.rs:
+// 118-153):
+//   c_{b,i}[r] = sum_j sum_s R_ij[r][s] * w_{b,j}[s]   (mod p),
+//   R_ij = rot(a_ij),  R[r][s] = a[r-s] (r >= s),  p - a[r-s+64] (r < s),
+// with witness digits w in [-128, 127].  Every residue R[r][s] in [0, p) is
+// split into 8 byte limbs, R = sum_l 2^(8l) R_l, so each limb is an exact
+// integer GEMM
+//   D_l[b][(i,r)] = sum_(j,s) W[b][(j,s)] * R_l[(i,r)][(j,s)]   (s8 x u8 -> s32)
+// with K = 64 per ring element.  A CTA sums at most 1024 ring elements
+// (K <= 65536), so |D_l| <= 65536 * 128 * 255 < 2^31 and the int32
+// accumulator is exact.  The reduction kernel forms sum_l 2^(8l) D_l over all
+// K-splits in 128-bit integers and reduces mod p.
+//
+// CTA tile: 128 witnesses (MMA M; the W tile comes from HBM by TMA with the
+// 128-byte swizzle), 4 rows i x 64 coefficients r (MMA N = 256, built in
+// shared memory), two limbs (two 128 x 256 int32 accumulators = all 512 TMEM
+// columns).  The rotation tiles are Toeplitz: row r of the 64-byte K block of
+// ring element j is the window F[63-r .. 126-r] of the 127-byte source
+//   F[v] = limb(a[63-v]) (v < 64),  limb(p - a[127-v]) (64 <= v < 127),
+// so the key is stored as F rows (128 bytes, zero tail) and builder threads
+// expand them: rows r = 4q+3 start 4-byte aligned, one thread loads 5 words
+// and emits rows 4q..4q+3 with compile-time funnel shifts.
+//
+// Warp roles: 0-7 build rotation tiles (and drain TMEM at the end), 8 issues
+// the TMA loads, 9 owns TMEM and issues the MMAs.  Rings: 4 slots of
+// (W tile + F rows), 2 slots of rotation tiles; mbarrier hand-offs, every
+// wait bounded (on expiry the kernel records LC_DEVERR_TIMEOUT, waits --
+// again bounded -- for its copies and MMAs in flight, frees TMEM, returns).
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <mutex>
+#include <new>
+
+#include "../../include/lattice_cuda.h"
+#include "arith.cuh"
+#include "common.cuh"
+#include "internal.h"
+
+namespace lc {
+
+constexpr int kTcJPer = 1024;            // ring elements per CTA (K = 64 each)
+constexpr int kTcFRow = 128;             // bytes per F row
+constexpr int kTcWBytes = 128 * 128;     // W tile: 128 witnesses x 128 bytes (2 ring elements)
+constexpr int kTcRotBytes = 256 * 128;   // one limb's rotation tile: 256 rows x 128 bytes
+constexpr int kTcFHalf = 8 * kTcFRow + 64;  // rows of one ring element; +64 B skews banks
+constexpr int kTcFSlot = 2 * kTcFHalf;
+constexpr int kTcWSlots = 4, kTcRotSlots = 2;
+constexpr int kTcOffRot = kTcWSlots * kTcWBytes;
+constexpr int kTcOffF = kTcOffRot + kTcRotSlots * 2 * kTcRotBytes;
+constexpr int kTcOffBar = kTcOffF + kTcWSlots * kTcFSlot;
+constexpr size_t kTcSmem = 1024 + kTcOffBar + 256;
+constexpr int kTcThreads = 320;
+constexpr uint32_t kTcLoadBytes = kTcWBytes + 2 * 8 * kTcFRow;
+static_assert(kTcOffRot % 1024 == 0 && kTcOffF % 16 == 0 && kTcFHalf % 16 == 0, "alignment");
+static_assert(kTcSmem <= 227 * 1024, "shared memory");
+
+// ------------------------------------------------------------------ device helpers
+
+// K-major operand, 128-byte swizzle: 8-row groups of 1024 bytes (SBO), start
+// address advanced by 32 bytes per K step inside the swizzle atom.
+LC_D uint64_t umma_desc_sw128(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);  // start address
+  d |= (uint64_t)1 << 16;                   // leading byte offset (unused here)
+  d |= (uint64_t)(1024 >> 4) << 32;         // stride byte offset
+  d |= (uint64_t)1 << 46;                   // descriptor version
+  d |= (uint64_t)2 << 61;                   // layout: 128-byte swizzle
+  return d;
+}
+
+// D = s32 (4), A = s8 (7), B = u8 (10), both K-major, N = 256 (17), M = 128 (24)
+constexpr uint32_t kTcIdesc = (2u << 4) | (1u << 7) | (0u << 10) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
+
+LC_D void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+LC_D void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(kTcIdesc), "r"(accumulate));
+}
+
+LC_D void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+
+LC_D void tmem_ld16(uint32_t addr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+        "=r"(v[15])
+      : "r"(addr));
+}
+
+LC_D void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+LC_D void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+LC_D void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// ------------------------------------------------------------------ key tables
+
+// fkey[g][lp][j][ll][ii][128]: F row of limb 2*lp+ll of A[4g+ii][j] (zero for
+// i >= k or j >= m).  One thread writes 16 bytes.
+__global__ void tc_key_tables_kernel(const uint64_t* __restrict__ a, uint8_t* __restrict__ fkey, uint32_t k,
+                                     uint32_t m, uint32_t m_pad, uint32_t groups) {
+  const size_t total16 = (size_t)groups * 4 * m_pad * 8 * (kTcFRow / 16);
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total16;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t v0 = (uint32_t)(e % 8) * 16;
+    size_t rest = e / 8;
+    const uint32_t ii = rest % 4;
+    rest /= 4;
+    const uint32_t ll = rest % 2;
+    rest /= 2;
+    const uint32_t j = rest % m_pad;
+    rest /= m_pad;
+    const uint32_t lp = rest % 4;
+    const uint32_t g = (uint32_t)(rest / 4);
+    const uint32_t i = 4 * g + ii, shift = 8 * (2 * lp + ll);
+    uint32_t wv[4] = {0, 0, 0, 0};
+    if (i < k && j < m) {
+      const uint64_t* ae = a + ((size_t)i * m + j) * 64;
+      for (int t = 0; t < 16; ++t) {
+        const uint32_t v = v0 + t;
+        uint64_t x = 0;
+        if (v < 64) {
+          x = ae[63 - v];
+        } else if (v < 127) {
+          x = ae[127 - v];
+          x = x == 0 ? 0 : kGlP - x;
+        }
+        wv[t >> 2] |= (uint32_t)((x >> shift) & 0xFF) << (8 * (t & 3));
+      }
+    }
+    reinterpret_cast<uint4*>(fkey)[e] = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+  }
+}
+
+// ------------------------------------------------------------------ the product kernel
+
+struct TcParams {
+  const uint8_t* fkey;
+  int64_t* partial;  // [split][lp][g][bt][256][128]
+  uint32_t m_pad, groups, splits, btiles;
+  uint32_t* err;
+};
+
+__global__ void __launch_bounds__(kTcThreads, 1)
+    tc_commit_kernel(const __grid_constant__ CUtensorMap wmap, const __grid_constant__ TcParams p) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char* base =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + kTcOffBar);
+  uint64_t* loaded = bars;         // [4] W + F of a stage landed (tx bytes)
+  uint64_t* mma_done = bars + 4;   // [4] tcgen05.commit of a stage
+  uint64_t* built = bars + 8;      // [2] 8 builder-warp arrivals
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 10);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 11);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t lp = blockIdx.x, g = blockIdx.y;
+  const uint32_t split = blockIdx.z % p.splits, bt = blockIdx.z / p.splits;
+  const uint32_t j0 = split * kTcJPer;
+  const uint32_t j1 = min(p.m_pad, j0 + kTcJPer);
+  const int nst = (int)((j1 - j0) / 2);  // stages of two ring elements; m_pad is even
+
+  if (tid == 0) {
+    for (int s = 0; s < 4; ++s) {
+      mbar_init(&loaded[s], 1);
+      mbar_init(&mma_done[s], 1);
+    }
+    mbar_init(&built[0], 8);
+    mbar_init(&built[1], 8);
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 9) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(512));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  auto w_slot = [&](int s) { return base + (s & 3) * kTcWBytes; };
+  auto rot_slot = [&](int s, int ll) { return base + kTcOffRot + ((s & 1) * 2 + ll) * kTcRotBytes; };
+  auto f_slot = [&](int s) { return base + kTcOffF + (s & 3) * kTcFSlot; };
+  auto fail = [&]() {
+    record_error(p.err, LC_DEVERR_TIMEOUT);
+    *abort_flag = 1;
+  };
+
+  int last_loaded = -1;  // TMA thread: last stage whose load was issued
+  int last_mma = -1;     // MMA thread: last stage whose MMAs were committed
+
+  if (warp == 8) {
+    // ---------------- TMA producer
+    if (lane == 0) {
+      const uint8_t* fsrc = p.fkey + (((size_t)g * 4 + lp) * p.m_pad) * 8 * kTcFRow;
+      for (int s = 0; s < nst && !*abort_flag; ++s) {
+        if (s >= 4 && !mbar_wait(&mma_done[s & 3], ((s - 4) >> 2) & 1)) {  // slot free again
+          fail();
+          break;
+        }
+        const uint32_t j = j0 + 2 * s;
+        mbar_arrive_expect_tx(&loaded[s & 3], kTcLoadBytes);
+        tma_load_2d(w_slot(s), &wmap, (int)(j * 64), (int)(bt * 128), &loaded[s & 3]);
+        bulk_g2s(f_slot(s), fsrc + (size_t)j * 8 * kTcFRow, 8 * kTcFRow, &loaded[s & 3]);
+        bulk_g2s(f_slot(s) + kTcFHalf, fsrc + (size_t)(j + 1) * 8 * kTcFRow, 8 * kTcFRow, &loaded[s & 3]);
+        last_loaded = s;
+      }
+    }
+  } else if (warp == 9) {
+    // ---------------- MMA issuer
+    if (lane == 0) {
+      for (int s = 0; s < nst && !*abort_flag; ++s) {
+        if (!mbar_wait(&loaded[s & 3], (s >> 2) & 1) || !mbar_wait(&built[s & 1], (s >> 1) & 1)) {
+          fail();
+          break;
+        }
+        tc_fence_after();
+        const uint32_t wa = smem_u32(w_slot(s));
+#pragma unroll
+        for (int ll = 0; ll < 2; ++ll) {
+          const uint32_t ra = smem_u32(rot_slot(s, ll));
+#pragma unroll
+          for (int ks = 0; ks < 4; ++ks)
+            mma_i8(tmem + ll * 256, umma_desc_sw128(wa + 32 * ks), umma_desc_sw128(ra + 32 * ks),
+                   (s > 0 || ks > 0) ? 1u : 0u);
+        }
+        mma_commit(&mma_done[s & 3]);
+        last_mma = s;
+      }
+    }
+  } else {
+    // ---------------- builders
+    // lane: c_lo = 16-byte chunk within the ring element's 64 bytes, q_lo =
+    // low two bits of the 4-row group q, jj = ring element of the stage.
+    const uint32_t c_lo = lane & 3, q_lo = (lane >> 2) & 3, jj = lane >> 4;
+    for (int s = 0; s < nst; ++s) {
+      bool ok = true;
+      if (s >= 2) ok = mbar_wait(&mma_done[(s - 2) & 3], ((s - 2) >> 2) & 1);  // rotation slot free
+      ok = ok && mbar_wait(&loaded[s & 3], (s >> 2) & 1);
+      if (!ok) fail();
+      if (*abort_flag) break;
+      const unsigned char* fbase = f_slot(s) + jj * kTcFHalf;
+#pragma unroll
+      for (int it = 0; it < 4; ++it) {
+        // wc: bits 0-1 = q_hi, 2-3 = ii, 4 = ll
+        const uint32_t wc = warp * 4 + it;
+        const uint32_t q = (wc & 3) * 4 + q_lo, ii = (wc >> 2) & 3, ll = wc >> 4;
+        const unsigned char* frow = fbase + (ll * 4 + ii) * kTcFRow;
+        const uint32_t off = 60 - 4 * q + 16 * c_lo;  // window of row 4q+3, 4-byte aligned
+        uint32_t w[5];
+#pragma unroll
+        for (int e = 0; e < 5; ++e) w[e] = *reinterpret_cast<const uint32_t*>(frow + off + 4 * e);
+        unsigned char* tile = rot_slot(s, ll);
+        const uint32_t c = jj * 4 + c_lo;
+#pragma unroll
+        for (int rho = 0; rho < 4; ++rho) {
+          const int delta = 3 - rho;  // row 4q+rho starts delta bytes later
+          uint32_t o[4];
+#pragma unroll
+          for (int t = 0; t < 4; ++t) o[t] = delta == 0 ? w[t] : __funnelshift_r(w[t], w[t + 1], 8 * delta);
+          const uint32_t n = ii * 64 + 4 * q + rho;
+          *reinterpret_cast<uint4*>(tile + n * 128 + ((c ^ (n & 7)) << 4)) = make_uint4(o[0], o[1], o[2], o[3]);
+        }
+      }
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&built[s & 1]);
+    }
+  }
+
+  // ---------------- drain the accumulators (builder warps)
+  __syncthreads();
+  if (!*abort_flag && nst > 0 && warp < 8) {
+    const int ls = nst - 1;
+    if (!mbar_wait(&mma_done[ls & 3], (ls >> 2) & 1)) {
+      fail();
+    } else {
+      tc_fence_after();
+      const uint32_t lane_base = 32 * (warp & 3), col_half = warp >> 2;
+      const uint32_t b_local = lane_base + lane;
+      int64_t* out = p.partial + ((((size_t)split * 4 + lp) * p.groups + g) * p.btiles + bt) * 256 * 128;
+#pragma unroll 1
+      for (int cc = 0; cc < 8; ++cc) {
+        const uint32_t col = col_half * 128 + cc * 16;
+        uint32_t d0[16], d1[16];
+        tmem_ld16(tmem + (lane_base << 16) + col, d0);
+        tmem_ld16(tmem + (lane_base << 16) + 256 + col, d1);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int u = 0; u < 16; ++u)
+          out[(size_t)(col + u) * 128 + b_local] = (int64_t)(int32_t)d0[u] + 256 * (int64_t)(int32_t)d1[u];
+      }
+    }
+  }
+  // ---------------- nothing may be in flight when TMEM and shared memory go
+  // (these waits return at once on the normal path)
+  if (warp == 8 && lane == 0) {
+    for (int s = max(0, last_loaded - 3); s <= last_loaded; ++s) mbar_wait(&loaded[s & 3], (s >> 2) & 1);
+  }
+  if (warp == 9 && lane == 0 && last_mma >= 0) mbar_wait(&mma_done[last_mma & 3], (last_mma >> 2) & 1);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 9) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+  }
+}
+
+// out[b][i][r] = sum_split sum_lp 2^(16 lp) partial[split][lp][g][bt][n][bl]  mod p,
+// i = 4g + n/64, r = n%64, b = 128 bt + bl.  Threads run along bl (coalesced reads).
+__global__ void tc_reduce_kernel(const int64_t* __restrict__ partial, uint64_t* __restrict__ out,
+                                 uint32_t batch, uint32_t k, uint32_t groups, uint32_t splits,
+                                 uint32_t btiles) {
+  const size_t total = (size_t)groups * btiles * 256 * 128;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t bl = idx % 128;
+    const uint32_t n = (idx / 128) % 256;
+    const uint32_t bt = (uint32_t)((idx / (128 * 256)) % btiles);
+    const uint32_t g = (uint32_t)(idx / ((size_t)128 * 256 * btiles));
+    const uint32_t b = bt * 128 + bl, i = 4 * g + n / 64;
+    if (b >= batch || i >= k) continue;
+    __int128 acc = 0;
+    for (uint32_t lp = 0; lp < 4; ++lp) {
+      int64_t s = 0;
+      for (uint32_t sp = 0; sp < splits; ++sp) s += partial[((size_t)sp * 4 + lp) * total + idx];
+      acc += (__int128)s << (16 * lp);
+    }
+    const bool neg = acc < 0;
+    const unsigned __int128 u = neg ? (unsigned __int128)(-acc) : (unsigned __int128)acc;
+    uint64_t res = gl_canon(gl_reduce128_lazy((uint64_t)(u >> 64), (uint64_t)u));
+    if (neg && res) res = kGlP - res;
+    out[((size_t)b * k + i) * 64 + n % 64] = res;
+  }
+}
+
+// ------------------------------------------------------------------ host side
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* ptr = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(ptr);
+    cudaGetLastError();
+  });
+  return fn;
+}
+
+}  // namespace lc
+
+struct lc_tc_tables {
+  uint8_t* fkey = nullptr;
+  uint32_t k = 0, m = 0, m_pad = 0, groups = 0;
+  int64_t* partial = nullptr;
+  size_t partial_bytes = 0;
+};
+
+namespace lc {
+
+void tc_tables_destroy(lc_tc_tables* t) {
+  if (!t) return;
+  if (t->fkey) cudaFree(t->fkey);
+  if (t->partial) cudaFree(t->partial);
+  delete t;
+}
+
+int tc_tables_create(const uint64_t* matrix_dev, uint32_t k, uint32_t m, lc_tc_tables** out) {
+  lc_tc_tables* t = new (std::nothrow) lc_tc_tables();
+  if (!t) return LC_ERR_OUT_OF_MEMORY;
+  t->k = k;
+  t->m = m;
+  t->m_pad = (m + 1) & ~1u;
+  t->groups = (k + 3) / 4;
+  const size_t bytes = (size_t)t->groups * 4 * t->m_pad * 8 * kTcFRow;
+  if (cudaMalloc(&t->fkey, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    delete t;
+    return LC_ERR_OUT_OF_MEMORY;
+  }
+  const int sms = device_sm_count();
+  tc_key_tables_kernel<<<std::max(sms, 1) * 8, 256>>>(matrix_dev, t->fkey, k, m, t->m_pad, t->groups);
+  const int rc = map_cuda(cudaGetLastError());
+  if (rc) {
+    tc_tables_destroy(t);
+    return rc;
+  }
+  *out = t;
+  return LC_OK;
+}
+
+size_t tc_tables_bytes(const lc_tc_tables* t) {
+  return t ? (size_t)t->groups * 4 * t->m_pad * 8 * kTcFRow : 0;
+}
+
+int tc_commit_i8(lc_tc_tables* t, const int8_t* w, size_t batch, uint64_t* out, uint32_t* err,
+                 cudaStream_t st) {
+  if (batch == 0) return LC_OK;
+  if (reinterpret_cast<uintptr_t>(w) & 15) return LC_ERR_INVALID_ARGUMENT;
+  if (batch > (1u << 24)) return LC_ERR_INVALID_ARGUMENT;
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return LC_ERR_UNSUPPORTED;
+  const uint32_t btiles = (uint32_t)((batch + 127) / 128);
+  const uint32_t splits = (t->m_pad + kTcJPer - 1) / kTcJPer;
+  // grid z = splits * btiles; TMA x coordinate j*64 is a signed 32-bit int
+  if ((size_t)splits * btiles > 65535 || (size_t)t->m_pad * 64 > 0x7FFFFFFF) return LC_ERR_UNSUPPORTED;
+  const size_t pbytes = (size_t)splits * 4 * t->groups * btiles * 256 * 128 * sizeof(int64_t);
+  if (pbytes > t->partial_bytes) {
+    if (t->partial) cudaFree(t->partial);
+    t->partial = nullptr;
+    t->partial_bytes = 0;
+    if (cudaMalloc(&t->partial, pbytes) != cudaSuccess) {
+      cudaGetLastError();
+      return LC_ERR_OUT_OF_MEMORY;
+    }
+    t->partial_bytes = pbytes;
+  }
+  // W as a 2-D byte array [batch][m*64]; box 128 bytes x 128 rows, 128-byte
+  // swizzle; columns past m*64 (odd m) and rows past batch read as zero.
+  CUtensorMap map;
+  const cuuint64_t dims[2] = {(cuuint64_t)t->m * 64, (cuuint64_t)batch};
+  const cuuint64_t strides[1] = {(cuuint64_t)t->m * 64};
+  const cuuint32_t box[2] = {128, 128};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult cr = enc(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<int8_t*>(w), dims, strides, box,
+                          estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (cr != CUDA_SUCCESS) return LC_ERR_INVALID_ARGUMENT;
+  cudaError_t e = cudaFuncSetAttribute(tc_commit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
+  if (e != cudaSuccess) return map_cuda(e);
+  const TcParams prm{t->fkey, t->partial, t->m_pad, t->groups, splits, btiles, err};
+  tc_commit_kernel<<<dim3(4, t->groups, splits * btiles), kTcThreads, kTcSmem, st>>>(map, prm);
+  int rc = map_cuda(cudaGetLastError());
+  if (rc) return rc;
+  const size_t total = (size_t)t->groups * btiles * 256 * 128;
+  const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, (size_t)device_sm_count() * 16);
+  tc_reduce_kernel<<<blocks, 256, 0, st>>>(t->partial, out, (uint32_t)batch, t->k, t->groups, splits, btiles);
+  return map_cuda(cudaGetLastError());
+}
+
+}  // namespace lc
