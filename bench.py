@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-commit", action="store_true", help="skip the Ajtai commit measurement")
+    ap.add_argument("--commit-only", action="store_true",
+                    help="run only the commit measurement (1 GPU) and print its JSON object")
     ap.add_argument("--commit-steps", type=int, default=5)
     ap.add_argument("--commit-m", type=int, default=1 << 16,
                     help="witness ring elements per commitment (profiling runs use fewer)")
@@ -75,6 +77,15 @@ def peaks():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def bf16_peak():
+    """Measured dense bf16 burst TFLOP/s (fallback 1590)."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        return 1590.0, "fallback"
 
 
 # ------------------------------------------------------------------ CPU legs
@@ -206,59 +217,74 @@ C_WORKLOAD = ("Ajtai commit, d=64 Goldilocks, kappa=16, n=2^16 ring elements, B=
 
 
 def bench_commit(args, rank, max_over_ranks, barrier, world):
-    """Committed ring elements/s for the 128-witness Goldilocks batch."""
+    """Committed ring elements/s for the 128-witness Goldilocks batch, with the
+    NTT engine ("plain") and the INT8 tensor-core engine ("tensor") of one key."""
     C_M = args.commit_m
     import ctypes as C
 
-    import numpy as np
     import torch
 
     from lzx_b200 import GoldilocksAjtaiKey, _lib, synth
     A = torch.empty(C_KAPPA * C_M * C_D, dtype=torch.int64, device="cuda")
     synth.fill_device(A, "gl", 4321 + rank, 0)
-    key = GoldilocksAjtaiKey(6, C_KAPPA, C_M, A)
+    key = GoldilocksAjtaiKey(6, C_KAPPA, C_M, A, tensor_cores=True)
     del A
     W = torch.empty(C_B * C_M * C_D, dtype=torch.int8, device="cuda")
     synth.fill_device(W, "i8", 4321 + rank, 1)
-    out = torch.empty((C_B, C_KAPPA, C_D), dtype=torch.int64, device="cuda")
     L = _lib.lib()
     st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
-    h, wp, op = key.handle, C.c_void_p(W.data_ptr()), C.c_void_p(out.data_ptr())
-    for _ in range(2):
-        _lib.check(L.lc_ajtai_commit_i8(h, wp, C_B, op, st), "commit")
-    torch.cuda.synchronize()
-    K = max(1, args.commit_steps)
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    barrier()
-    torch.cuda.synchronize()
-    a.record()
-    for _ in range(K):
-        L.lc_ajtai_commit_i8(h, wp, C_B, op, st)
-    b.record()
-    torch.cuda.synchronize()
-    _lib.check(L.lc_ajtai_key_check(h, st), "commit check")
-    ms = max_over_ranks(a.elapsed_time(b) / K)
-    elems = C_B * C_M
-    # end to end from pinned host memory (witness in, commitments out)
+    h, wp = key.handle, C.c_void_p(W.data_ptr())
     hw = torch.empty(C_B * C_M * C_D, dtype=torch.int8).pin_memory()
     hw.copy_(W.cpu())
-    hout = torch.empty((C_B, C_KAPPA, C_D), dtype=torch.int64).pin_memory()
-    del W
-    hp, hop = C.c_void_p(hw.data_ptr()), C.c_void_p(hout.data_ptr())
-    _lib.check(L.lc_ajtai_commit_i8_host(h, hp, C_B, hop), "commit host")
-    assert torch.equal(hout, out.cpu())
-    KE = 2
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(KE):
-        L.lc_ajtai_commit_i8_host(h, hp, C_B, hop)
-    e2e_s = max_over_ranks((time.perf_counter() - t0) / KE)
+    elems = C_B * C_M
+    outs = {}
     res = {"workload": C_WORKLOAD, "unit": "ring-elems/s",
-           "plain": {"value": world * elems / (ms / 1e3), "ms_per_batch": ms, "steps": K,
+           "alg_mul_adds_per_batch": C_KAPPA * C_M * C_D * C_B}
+    for name, engine in (("plain", GoldilocksAjtaiKey.ENGINE_NTT), ("tensor", GoldilocksAjtaiKey.ENGINE_TENSOR_I8)):
+        key.engine = engine
+        out = torch.empty((C_B, C_KAPPA, C_D), dtype=torch.int64, device="cuda")
+        op = C.c_void_p(out.data_ptr())
+        for _ in range(3):
+            _lib.check(L.lc_ajtai_commit_i8(h, wp, C_B, op, st), "commit")
+        torch.cuda.synchronize()
+        K = max(1, args.commit_steps)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(K):
+            L.lc_ajtai_commit_i8(h, wp, C_B, op, st)
+        b.record()
+        torch.cuda.synchronize()
+        _lib.check(L.lc_ajtai_key_check(h, st), "commit check")
+        ms = max_over_ranks(a.elapsed_time(b) / K)
+        outs[name] = out
+        # end to end from pinned host memory (witness in, commitments out)
+        hout = torch.empty((C_B, C_KAPPA, C_D), dtype=torch.int64).pin_memory()
+        hp, hop = C.c_void_p(hw.data_ptr()), C.c_void_p(hout.data_ptr())
+        _lib.check(L.lc_ajtai_commit_i8_host(h, hp, C_B, hop), "commit host")
+        assert torch.equal(hout, out.cpu())
+        KE = 2
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(KE):
+            L.lc_ajtai_commit_i8_host(h, hp, C_B, hop)
+        e2e_s = max_over_ranks((time.perf_counter() - t0) / KE)
+        res[name] = {"value": world * elems / (ms / 1e3), "ms_per_batch": ms, "steps": K,
                      "e2e": {"value": world * elems / e2e_s, "unit": "ring-elems/s",
                              "h2d_bytes_per_step": C_B * C_M * C_D,
-                             "d2h_bytes_per_step": C_B * C_KAPPA * C_D * 8}},
-           "alg_mul_adds_per_batch": C_KAPPA * C_M * C_D * C_B}
+                             "d2h_bytes_per_step": C_B * C_KAPPA * C_D * 8}}
+    assert torch.equal(outs["plain"], outs["tensor"]), "tensor engine differs from the NTT engine"
+    # tensor engine: 8 byte-limb GEMMs of B x (kappa*64) x (m*64) int8 multiply-adds
+    ops = 2 * 8 * C_B * (C_KAPPA * C_D) * (C_M * C_D)
+    bf16, kind = bf16_peak()
+    peak = 2 * bf16
+    ach = ops / (res["tensor"]["ms_per_batch"] / 1e3) / 1e12
+    res["tensor"]["roofline"] = {"bound": "tensor", "achieved": ach, "peak": peak, "unit": "TOP/s",
+                                 "frac": ach / peak, "int8_ops_per_batch": ops,
+                                 "peak_source": f"2 x {kind} bf16 burst (dense INT8 rate is twice bf16)"}
+    res["speedup_tensor_vs_plain"] = res["plain"]["ms_per_batch"] / res["tensor"]["ms_per_batch"]
+    del W
     if rank == 0 and not args.no_cpu_baseline:
         import oracle
         oracle.prefer_native(True)
@@ -450,10 +476,20 @@ def run_ours(args):
     return 0
 
 
+def run_commit_only(args):
+    import torch
+    torch.cuda.set_device(0)
+    res = bench_commit(args, 0, lambda x: x, lambda: None, 1)
+    print(json.dumps(res), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.commit_only:
+        return run_commit_only(args)
     return run_ours(args)
 
 
