@@ -144,9 +144,14 @@ LC_API int lc_ajtai_commit(lc_ajtai_key *key, const void *s, size_t batch, void 
  * lattice-folding/src/neo.rs:98-109). */
 LC_API int lc_ajtai_commit_i8(lc_ajtai_key *key, const int8_t *s, size_t batch, void *out,
                               lc_stream stream);
+/* Same with unsigned byte digits in [0, 255] (the rows of decomp_b with
+ * b <= 8, lattice-folding/src/neo.rs:253-266, each row one witness). */
+LC_API int lc_ajtai_commit_u8(lc_ajtai_key *key, const uint8_t *s, size_t batch, void *out,
+                              lc_stream stream);
 /* Host-buffer variants (synchronous). */
 LC_API int lc_ajtai_commit_host(lc_ajtai_key *key, const void *s, size_t batch, void *out);
 LC_API int lc_ajtai_commit_i8_host(lc_ajtai_key *key, const int8_t *s, size_t batch, void *out);
+LC_API int lc_ajtai_commit_u8_host(lc_ajtai_key *key, const uint8_t *s, size_t batch, void *out);
 /* Wait for `stream` and report device-side errors of this key's kernels. */
 LC_API int lc_ajtai_key_check(lc_ajtai_key *key, lc_stream stream);
 
@@ -164,12 +169,12 @@ LC_API int lc_ajtai_key_check(lc_ajtai_key *key, lc_stream stream);
 LC_API int lc_ajtai_key_create_ex(const lc_ntt_plan *plan, uint32_t k, uint32_t m, const void *matrix,
                                   int matrix_on_device, uint32_t flags, lc_ajtai_key **out);
 
-/* Which engine lc_ajtai_commit_i8 (and lc_ajtai_commit_i8_host) uses:
- * LC_ENGINE_NTT (cached-NTT multiply-accumulate, every key) or
- * LC_ENGINE_TENSOR_I8 (keys created with LC_KEY_TENSOR_I8; exact s8 x u8
- * products on the tensor cores, per-limb int32 sums of at most 1024 ring
- * elements, exact 128-bit reduction).  Residue witnesses (lc_ajtai_commit)
- * always use the NTT engine. */
+/* Which engine the byte-digit commits (lc_ajtai_commit_i8 / _u8 and their
+ * host variants) use: LC_ENGINE_NTT (cached-NTT multiply-accumulate, every
+ * key) or LC_ENGINE_TENSOR_I8 (keys created with LC_KEY_TENSOR_I8; exact
+ * s8 x u8 (u8 x u8) products on the tensor cores, per-limb int32 sums of at
+ * most 1024 (512) ring elements, exact 128-bit reduction).  Residue
+ * witnesses (lc_ajtai_commit) always use the NTT engine. */
 #define LC_ENGINE_NTT 0
 #define LC_ENGINE_TENSOR_I8 1
 LC_API int lc_ajtai_key_set_engine(lc_ajtai_key *key, int engine);
@@ -196,6 +201,27 @@ LC_API int lc_ajtai_key_get_engine(const lc_ajtai_key *key);
  * because every word a call reads is written earlier in the same call. */
 LC_API int lc_ajtai_commit_noalloc(const lc_ajtai_key *key, const void *s, size_t batch, void *out,
                                    lc_stream stream);
+
+/* ------------------------------------------------------------------------
+ * Digit decompositions of Goldilocks vectors (device pointers).
+ * ---------------------------------------------------------------------- */
+
+/* decomp_b (lattice-folding/src/neo.rs:253-266): for each of the `count`
+ * residues z[e] (reduced to canonical first, as to_canonical_u64 does), its
+ * unsigned base-2^b_bits digits; out = [rows][count] bytes with
+ * rows = ceil(64 / b_bits), row r holding digit r of every element.
+ * b_bits in 1..8. */
+LC_API int lc_decomp_b(const uint64_t *z, size_t count, uint32_t b_bits, uint8_t *out, lc_stream stream);
+
+/* GadgetDecomposition::decompose (lattice-core/src/decomposition.rs:48-70) of
+ * each u64 z[e] in base 2^log_base (1..15) into num_digits balanced digits
+ * (a digit t > base/2 becomes t - base and borrows); out = [num_digits][count]
+ * int16.  The reference returns ValueTooLarge for a value whose remainder is
+ * not zero after num_digits digits: here the digits are still written and the
+ * number of such values is added to *too_large (a device counter; may be
+ * NULL). */
+LC_API int lc_gadget_decompose(const uint64_t *z, size_t count, uint32_t log_base, uint32_t num_digits,
+                               int16_t *out, uint32_t *too_large, lc_stream stream);
 
 /* Benchmark/test utility, no counterpart in the reference: fill `count`
  * elements of `out` (device) with the seeded counter-based synthetic stream

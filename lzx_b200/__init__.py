@@ -9,6 +9,7 @@ the reference's ring/commitment API.
 from ._lib import LatticeCudaError, lib  # noqa: F401
 from .commitment import (AjtaiCommitment, AjtaiError, AjtaiParams, AjtaiPublicKey,  # noqa: F401
                          GoldilocksAjtaiKey, sample_small_secret)
+from .decomposition import GadgetDecomposition, decomp_b  # noqa: F401
 from .ring import (CRT_SET_30BIT, GoldilocksNttTables, Modulus32, NttError, NttTables,  # noqa: F401
                    RingConfig, RingElement, RingError)
 

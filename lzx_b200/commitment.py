@@ -90,7 +90,7 @@ class _DeviceKey:
             self._h = None
 
     def commit_array(self, w, out=None):
-        """Batch commit: w [B][m][n] (residues or int8) -> [B][k][n]."""
+        """Batch commit: w [B][m][n] (residues, int8 or uint8 digits) -> [B][k][n]."""
         L = _lib.lib()
         if _is_torch_cuda(w):
             import torch
@@ -100,7 +100,8 @@ class _DeviceKey:
             if out is None:
                 dt = torch.int64 if self.elem_dtype == np.uint64 else torch.int32
                 out = torch.empty((batch, self.k, self.n), dtype=dt, device=w.device)
-            fn = L.lc_ajtai_commit_i8 if w.dtype == torch.int8 else L.lc_ajtai_commit
+            fn = {torch.int8: L.lc_ajtai_commit_i8, torch.uint8: L.lc_ajtai_commit_u8}.get(
+                w.dtype, L.lc_ajtai_commit)
             _map_status(fn(self._h, C.c_void_p(w.data_ptr()), batch, C.c_void_p(out.data_ptr()),
                            _current_stream()), "lc_ajtai_commit")
             return out
@@ -109,9 +110,9 @@ class _DeviceKey:
         if batch * self.m * self.n != w.size:
             raise AjtaiError("DimensionMismatch", expected=self.m * self.n, got=w.size)
         res = np.empty((batch, self.k, self.n), dtype=self.elem_dtype) if out is None else out
-        if w.dtype == np.int8:
-            st = L.lc_ajtai_commit_i8_host(self._h, w.ctypes.data_as(C.c_void_p), batch,
-                                           res.ctypes.data_as(C.c_void_p))
+        if w.dtype in (np.int8, np.uint8):
+            fn = L.lc_ajtai_commit_i8_host if w.dtype == np.int8 else L.lc_ajtai_commit_u8_host
+            st = fn(self._h, w.ctypes.data_as(C.c_void_p), batch, res.ctypes.data_as(C.c_void_p))
         else:
             w = w.astype(self.elem_dtype, copy=False)
             st = L.lc_ajtai_commit_host(self._h, w.ctypes.data_as(C.c_void_p), batch,

@@ -166,6 +166,16 @@ template <>
 LC_D uint32_t to_residue<uint32_t, int8_t>(int8_t x, uint32_t q) {
   return x >= 0 ? (uint32_t)x : q - (uint32_t)(-(int)x);
 }
+// unsigned digits (decomp_b rows, lattice-folding/src/neo.rs:253-266); every
+// supported modulus exceeds 255
+template <>
+LC_D uint64_t to_residue<uint64_t, uint8_t>(uint8_t x, uint32_t) {
+  return x;
+}
+template <>
+LC_D uint32_t to_residue<uint32_t, uint8_t>(uint8_t x, uint32_t) {
+  return x;
+}
 
 // Witness NTT, frequency-major output.  CTA (j, b-block of BB witnesses):
 // loads the BB polynomials w[b][j][*] (16-byte vector loads when aligned),
@@ -845,8 +855,17 @@ LC_API int lc_ajtai_commit_i8(lc_ajtai_key* key, const int8_t* s, size_t batch, 
   if (!key || (!s && batch) || (!out && batch)) return LC_ERR_INVALID_ARGUMENT;
   if (((uintptr_t)out) & 15) return LC_ERR_INVALID_ARGUMENT;
   if (key->engine == LC_ENGINE_TENSOR_I8)
-    return tc_commit_i8(key->tc, s, batch, static_cast<uint64_t*>(out), key->d_err, (cudaStream_t)stream);
+    return tc_commit(key->tc, s, true, batch, static_cast<uint64_t*>(out), key->d_err, (cudaStream_t)stream);
   return commit_any<int8_t>(key, s, batch, out, (cudaStream_t)stream);
+}
+
+LC_API int lc_ajtai_commit_u8(lc_ajtai_key* key, const uint8_t* s, size_t batch, void* out,
+                              lc_stream stream) {
+  if (!key || (!s && batch) || (!out && batch)) return LC_ERR_INVALID_ARGUMENT;
+  if (((uintptr_t)out) & 15) return LC_ERR_INVALID_ARGUMENT;
+  if (key->engine == LC_ENGINE_TENSOR_I8)
+    return tc_commit(key->tc, s, false, batch, static_cast<uint64_t*>(out), key->d_err, (cudaStream_t)stream);
+  return commit_any<uint8_t>(key, s, batch, out, (cudaStream_t)stream);
 }
 
 static int commit_host(lc_ajtai_key* key, const void* s, size_t in_elem, size_t batch, void* out,
@@ -864,8 +883,9 @@ static int commit_host(lc_ajtai_key* key, const void* s, size_t in_elem, size_t 
   cudaStream_t st = key->host_stream;
   if (cudaMemcpyAsync(key->d_in, s, in_bytes, cudaMemcpyHostToDevice, st) != cudaSuccess)
     return map_cuda(cudaGetLastError());
-  rc = i8 ? lc_ajtai_commit_i8(key, (const int8_t*)key->d_in, batch, key->d_out, st)
-          : lc_ajtai_commit(key, key->d_in, batch, key->d_out, st);
+  rc = in_elem == 1 ? (i8 ? lc_ajtai_commit_i8(key, (const int8_t*)key->d_in, batch, key->d_out, st)
+                          : lc_ajtai_commit_u8(key, (const uint8_t*)key->d_in, batch, key->d_out, st))
+                    : lc_ajtai_commit(key, key->d_in, batch, key->d_out, st);
   if (rc) return rc;
   if (cudaMemcpyAsync(out, key->d_out, out_bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess)
     return map_cuda(cudaGetLastError());
@@ -878,6 +898,10 @@ LC_API int lc_ajtai_commit_host(lc_ajtai_key* key, const void* s, size_t batch, 
 
 LC_API int lc_ajtai_commit_i8_host(lc_ajtai_key* key, const int8_t* s, size_t batch, void* out) {
   return commit_host(key, s, 1, batch, out, true);
+}
+
+LC_API int lc_ajtai_commit_u8_host(lc_ajtai_key* key, const uint8_t* s, size_t batch, void* out) {
+  return commit_host(key, s, 1, batch, out, false);
 }
 
 LC_API int lc_ajtai_key_check(lc_ajtai_key* key, lc_stream stream) {

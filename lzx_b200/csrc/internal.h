@@ -81,11 +81,12 @@ int run_ntt(const lc_ntt_plan* plan, const void* in, void* out, size_t count, bo
             cudaStream_t s);
 
 // Goldilocks, d = 64: build the rotation-limb tables from the coefficient
-// matrix [k][m][64] on the device (default stream); commit int8 witnesses
-// [batch][m][64] -> residues [batch][k][64] on `st`.
+// matrix [k][m][64] on the device (default stream); commit byte-digit
+// witnesses [batch][m][64] -> residues [batch][k][64] on `st`.
 int tc_tables_create(const uint64_t* matrix_dev, uint32_t k, uint32_t m, lc_tc_tables** out);
 void tc_tables_destroy(lc_tc_tables* t);
 size_t tc_tables_bytes(const lc_tc_tables* t);
-int tc_commit_i8(lc_tc_tables* t, const int8_t* w, size_t batch, uint64_t* out, uint32_t* err,
-                 cudaStream_t st);
+// w: int8 digits (s8 = true) or unsigned byte digits (s8 = false)
+int tc_commit(lc_tc_tables* t, const void* w, bool s8, size_t batch, uint64_t* out, uint32_t* err,
+              cudaStream_t st);
 }  // namespace lc

@@ -12,7 +12,9 @@
 //   D_l[b][(i,r)] = sum_(j,s) W[b][(j,s)] * R_l[(i,r)][(j,s)]   (s8 x u8 -> s32)
 // with K = 64 per ring element.  A CTA sums at most 1024 ring elements
 // (K <= 65536), so |D_l| <= 65536 * 128 * 255 < 2^31 and the int32
-// accumulator is exact.  The reduction kernel forms sum_l 2^(8l) D_l over all
+// accumulator is exact.  Unsigned byte digits (decomp_b rows,
+// lattice-folding/src/neo.rs:253-266) run the same kernel as u8 x u8 with
+// at most 512 ring elements per CTA: 32768 * 255 * 255 < 2^31.  The reduction kernel forms sum_l 2^(8l) D_l over all
 // K-splits in 128-bit integers and reduces mod p.
 //
 // CTA tile: 128 witnesses (MMA M; the W tile comes from HBM by TMA with the
@@ -44,7 +46,11 @@
 
 namespace lc {
 
-constexpr int kTcJPer = 1024;            // ring elements per CTA (K = 64 each)
+// ring elements per CTA (K = 64 each): the int32 bound above
+template <bool S8>
+struct TcJPer {
+  static constexpr int value = S8 ? 1024 : 512;
+};
 constexpr int kTcFRow = 128;             // bytes per F row
 constexpr int kTcWBytes = 128 * 128;     // W tile: 128 witnesses x 128 bytes (2 ring elements)
 constexpr int kTcRotBytes = 256 * 128;   // one limb's rotation tile: 256 rows x 128 bytes
@@ -74,8 +80,12 @@ LC_D uint64_t umma_desc_sw128(uint32_t saddr) {
   return d;
 }
 
-// D = s32 (4), A = s8 (7), B = u8 (10), both K-major, N = 256 (17), M = 128 (24)
-constexpr uint32_t kTcIdesc = (2u << 4) | (1u << 7) | (0u << 10) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
+// D = s32 (4), A = s8 or u8 (7), B = u8 (10), both K-major, N = 256 (17), M = 128 (24)
+template <bool S8>
+struct TcIdesc {
+  static constexpr uint32_t value =
+      (2u << 4) | ((S8 ? 1u : 0u) << 7) | (0u << 10) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
+};
 
 LC_D void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
   asm volatile(
@@ -85,11 +95,11 @@ LC_D void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t*
       : "memory");
 }
 
-LC_D void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+LC_D void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-      "l"(adesc), "l"(bdesc), "r"(kTcIdesc), "r"(accumulate));
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 
 LC_D void mma_commit(uint64_t* bar) {
@@ -162,8 +172,10 @@ struct TcParams {
   uint32_t* err;
 };
 
+template <bool S8>
 __global__ void __launch_bounds__(kTcThreads, 1)
     tc_commit_kernel(const __grid_constant__ CUtensorMap wmap, const __grid_constant__ TcParams p) {
+  constexpr int kTcJPer = TcJPer<S8>::value;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* base =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -245,7 +257,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 #pragma unroll
           for (int ks = 0; ks < 4; ++ks)
             mma_i8(tmem + ll * 256, umma_desc_sw128(wa + 32 * ks), umma_desc_sw128(ra + 32 * ks),
-                   (s > 0 || ks > 0) ? 1u : 0u);
+                   TcIdesc<S8>::value, (s > 0 || ks > 0) ? 1u : 0u);
         }
         mma_commit(&mma_done[s & 3]);
         last_mma = s;
@@ -423,15 +435,16 @@ size_t tc_tables_bytes(const lc_tc_tables* t) {
   return t ? (size_t)t->groups * 4 * t->m_pad * 8 * kTcFRow : 0;
 }
 
-int tc_commit_i8(lc_tc_tables* t, const int8_t* w, size_t batch, uint64_t* out, uint32_t* err,
-                 cudaStream_t st) {
+int tc_commit(lc_tc_tables* t, const void* w, bool s8, size_t batch, uint64_t* out, uint32_t* err,
+              cudaStream_t st) {
   if (batch == 0) return LC_OK;
+  const int jper = s8 ? TcJPer<true>::value : TcJPer<false>::value;
   if (reinterpret_cast<uintptr_t>(w) & 15) return LC_ERR_INVALID_ARGUMENT;
   if (batch > (1u << 24)) return LC_ERR_INVALID_ARGUMENT;
   EncodeTiledFn enc = encode_fn();
   if (!enc) return LC_ERR_UNSUPPORTED;
   const uint32_t btiles = (uint32_t)((batch + 127) / 128);
-  const uint32_t splits = (t->m_pad + kTcJPer - 1) / kTcJPer;
+  const uint32_t splits = (t->m_pad + jper - 1) / jper;
   // grid z = splits * btiles; TMA x coordinate j*64 is a signed 32-bit int
   if ((size_t)splits * btiles > 65535 || (size_t)t->m_pad * 64 > 0x7FFFFFFF) return LC_ERR_UNSUPPORTED;
   const size_t pbytes = (size_t)splits * 4 * t->groups * btiles * 256 * 128 * sizeof(int64_t);
@@ -452,14 +465,15 @@ int tc_commit_i8(lc_tc_tables* t, const int8_t* w, size_t batch, uint64_t* out, 
   const cuuint64_t strides[1] = {(cuuint64_t)t->m * 64};
   const cuuint32_t box[2] = {128, 128};
   const cuuint32_t estr[2] = {1, 1};
-  const CUresult cr = enc(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<int8_t*>(w), dims, strides, box,
+  const CUresult cr = enc(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(w), dims, strides, box,
                           estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (cr != CUDA_SUCCESS) return LC_ERR_INVALID_ARGUMENT;
-  cudaError_t e = cudaFuncSetAttribute(tc_commit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
+  auto kern = s8 ? tc_commit_kernel<true> : tc_commit_kernel<false>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
   if (e != cudaSuccess) return map_cuda(e);
   const TcParams prm{t->fkey, t->partial, t->m_pad, t->groups, splits, btiles, err};
-  tc_commit_kernel<<<dim3(4, t->groups, splits * btiles), kTcThreads, kTcSmem, st>>>(map, prm);
+  kern<<<dim3(4, t->groups, splits * btiles), kTcThreads, kTcSmem, st>>>(map, prm);
   int rc = map_cuda(cudaGetLastError());
   if (rc) return rc;
   const size_t total = (size_t)t->groups * btiles * 256 * 128;
