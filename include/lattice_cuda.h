@@ -223,6 +223,41 @@ LC_API int lc_decomp_b(const uint64_t *z, size_t count, uint32_t b_bits, uint8_t
 LC_API int lc_gadget_decompose(const uint64_t *z, size_t count, uint32_t log_base, uint32_t num_digits,
                                int16_t *out, uint32_t *too_large, lc_stream stream);
 
+/* ------------------------------------------------------------------------
+ * CRT residues and the folding-step pipeline.
+ * ---------------------------------------------------------------------- */
+
+/* out[i][e] = z[e] mod q_i for every u32 modulus q_i of `plan`
+ * (Modulus32::reduce_u64, lattice-ring/src/modulus.rs:65, per prime): maps
+ * 64-bit coefficients into the plan's CRT set ([num_moduli][count] u32, the
+ * layout lc_ntt_forward takes). */
+LC_API int lc_crt_residues(const lc_ntt_plan *plan, const uint64_t *z, size_t count, uint32_t *out,
+                           lc_stream stream);
+
+/* One folding step over d = 64 Goldilocks as a single graph launch.  No
+ * single counterpart in the reference: it chains decomp_b(z, 8)
+ * (lattice-folding/src/neo.rs:253-266), the commitment of the 8 digit rows
+ * with `key` (AjtaiPublicKey::commit, ajtai.rs:118-153, as a batch of 8
+ * witnesses through lc_ajtai_commit_u8), and the forward NTT of z over the
+ * CRT set of `crt_plan` (lc_crt_residues + lc_ntt_forward).  `key`: Goldilocks,
+ * log_n 6, m ring elements; `crt_plan`: u32 moduli, log_n 6.  The pipeline owns
+ * its buffers (lc_fold_pipeline_buffers): z = [m][64] residues (written by the
+ * caller), digits = [8][m][64] bytes, commits = [8][k][64] residues,
+ * crt_ntt = [num_moduli][m][64] u32.  With use_graph != 0 the first run is
+ * eager (it sizes the key's scratch) and the second captures the four stages
+ * into a CUDA graph that every later run replays; if another commit on the
+ * same key reallocates that scratch, the next run captures again.  Runs of
+ * one pipeline, and other commits on its key, must not overlap on the GPU. */
+typedef struct lc_fold_pipeline lc_fold_pipeline;
+LC_API int lc_fold_pipeline_create(lc_ajtai_key *key, const lc_ntt_plan *crt_plan, int use_graph,
+                                   lc_fold_pipeline **out);
+LC_API int lc_fold_pipeline_buffers(lc_fold_pipeline *pipe, uint64_t **z, uint8_t **digits,
+                                    uint64_t **commits, uint32_t **crt_ntt);
+LC_API int lc_fold_pipeline_run(lc_fold_pipeline *pipe, lc_stream stream);
+/* Wait for `stream` and report device-side errors of the pipeline's kernels. */
+LC_API int lc_fold_pipeline_check(lc_fold_pipeline *pipe, lc_stream stream);
+LC_API void lc_fold_pipeline_destroy(lc_fold_pipeline *pipe);
+
 /* Benchmark/test utility, no counterpart in the reference: fill `count`
  * elements of `out` (device) with the seeded counter-based synthetic stream
  * x_i = H(seed, stream, offset + i): kind 0 raw u64, 1 u32 residues mod q

@@ -86,6 +86,12 @@ def _declare(L):
         "lc_ajtai_commit_u8_host": (i32, [P, P, sz, P]),
         "lc_decomp_b": (i32, [P, sz, u32, P, P]),
         "lc_gadget_decompose": (i32, [P, sz, u32, u32, P, P, P]),
+        "lc_crt_residues": (i32, [P, P, sz, P, P]),
+        "lc_fold_pipeline_create": (i32, [P, P, i32, C.POINTER(P)]),
+        "lc_fold_pipeline_buffers": (i32, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(P)]),
+        "lc_fold_pipeline_run": (i32, [P, P]),
+        "lc_fold_pipeline_check": (i32, [P, P]),
+        "lc_fold_pipeline_destroy": (None, [P]),
         "lc_synth_fill": (i32, [i32, C.c_uint64, C.c_uint64, u32, P, sz, sz, P]),
     }
     optional = {

@@ -843,6 +843,24 @@ LC_API int lc_ajtai_key_set_engine(lc_ajtai_key* key, int engine) {
 
 LC_API int lc_ajtai_key_get_engine(const lc_ajtai_key* key) { return key ? key->engine : -1; }
 
+}  // extern "C"
+
+namespace lc {
+// Identity of the scratch buffers a commit on this key writes; changes when
+// any of them is reallocated (a captured graph of a commit is only valid
+// while it stays the same).
+uint64_t commit_scratch_signature(const lc_ajtai_key* key) {
+  uint64_t h = 1469598103934665603ull;
+  for (uintptr_t v : {(uintptr_t)key->d_what_t, (uintptr_t)key->d_partial, (uintptr_t)key->d_chat,
+                      (uintptr_t)key->d_wtmp, (uintptr_t)key->what_bytes, (uintptr_t)key->partial_bytes,
+                      (uintptr_t)key->chat_bytes, (uintptr_t)key->wtmp_bytes})
+    h = (h ^ (uint64_t)v) * 1099511628211ull;
+  return h;
+}
+}  // namespace lc
+
+extern "C" {
+
 LC_API int lc_ajtai_commit(lc_ajtai_key* key, const void* s, size_t batch, void* out, lc_stream stream) {
   if (!key || (!s && batch) || (!out && batch)) return LC_ERR_INVALID_ARGUMENT;
   if (((uintptr_t)out) & 15) return LC_ERR_INVALID_ARGUMENT;

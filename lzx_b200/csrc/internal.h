@@ -86,6 +86,8 @@ int run_ntt(const lc_ntt_plan* plan, const void* in, void* out, size_t count, bo
 int tc_tables_create(const uint64_t* matrix_dev, uint32_t k, uint32_t m, lc_tc_tables** out);
 void tc_tables_destroy(lc_tc_tables* t);
 size_t tc_tables_bytes(const lc_tc_tables* t);
+uint64_t commit_scratch_signature(const lc_ajtai_key* key);
+int crt_residues(const lc_ntt_plan* plan, const uint64_t* z, size_t count, uint32_t* out, cudaStream_t st);
 // w: int8 digits (s8 = true) or unsigned byte digits (s8 = false)
 int tc_commit(lc_tc_tables* t, const void* w, bool s8, size_t batch, uint64_t* out, uint32_t* err,
               cudaStream_t st);
