@@ -61,6 +61,11 @@ def parse():
     ap.add_argument("--no-commit", action="store_true", help="skip the Ajtai commit measurement")
     ap.add_argument("--commit-only", action="store_true",
                     help="run only the commit measurement (1 GPU) and print its JSON object")
+    ap.add_argument("--only", choices=["commit", "fold", "single"], default=None,
+                    help="run only one secondary measurement (1 GPU) and print its JSON object")
+    ap.add_argument("--no-fold", action="store_true", help="skip the folding-step measurement")
+    ap.add_argument("--fold-m", type=int, default=1 << 20, help="ring elements of the folding-step witness")
+    ap.add_argument("--fold-steps", type=int, default=5)
     ap.add_argument("--commit-steps", type=int, default=5)
     ap.add_argument("--commit-m", type=int, default=1 << 16,
                     help="witness ring elements per commitment (profiling runs use fewer)")
@@ -303,6 +308,153 @@ def bench_commit(args, rank, max_over_ranks, barrier, world):
     return res
 
 
+# ------------------------------------------------------------------ folding step
+
+F_KAPPA = 16
+F_WORKLOAD = ("folding step, d=64 Goldilocks: z of m ring elements -> decomp_b(z, 8) -> 8 digit "
+              "commitments (kappa=16, cached NTT(A)) + forward NTT of z over the 4-prime 30-bit CRT set; "
+              "one CUDA-graph launch")
+
+
+def bench_fold(args, rank, max_over_ranks, barrier, world):
+    """Folding steps per second (witness ring elements/s) through lc_fold_pipeline."""
+    import ctypes as C
+
+    import torch
+
+    from lzx_b200 import CRT_SET_30BIT, GoldilocksAjtaiKey, NttTables, _lib, synth
+    from lzx_b200.pipeline import FoldPipeline
+    m = args.fold_m
+    A = torch.empty(F_KAPPA * m * 64, dtype=torch.int64, device="cuda")
+    synth.fill_device(A, "gl", 97 + rank, 0)
+    key = GoldilocksAjtaiKey(6, F_KAPPA, m, A)
+    del A
+    crt = NttTables(CRT_SET_30BIT, 6)
+    res = {"workload": F_WORKLOAD, "m": m, "unit": "witness ring-elems/s"}
+    K = max(1, args.fold_steps)
+    for name, graph in (("eager", False), ("graph", True)):
+        pipe = FoldPipeline(key, crt, use_graph=graph)
+        synth.fill_device(pipe.z, "gl", 97 + rank, 1)
+        for _ in range(3):
+            pipe.run()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(K):
+            pipe.run()
+        b.record()
+        torch.cuda.synchronize()
+        pipe.check()
+        ms = max_over_ranks(a.elapsed_time(b) / K)
+        res[name] = {"ms_per_step": ms, "value": world * m / (ms / 1e3), "steps": K}
+        if graph:
+            # end to end: z from pinned host memory in, commitments and CRT NTT out
+            hz = torch.empty((m, 64), dtype=torch.int64).pin_memory()
+            hz.copy_(pipe.z.cpu())
+            hc = torch.empty(tuple(pipe.commits.shape), dtype=torch.int64).pin_memory()
+            ht = torch.empty(tuple(pipe.crt_ntt.shape), dtype=torch.int32).pin_memory()
+            KE = 3
+            barrier()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(KE):
+                pipe.z.copy_(hz, non_blocking=True)
+                pipe.run()
+                hc.copy_(pipe.commits, non_blocking=True)
+                ht.copy_(pipe.crt_ntt, non_blocking=True)
+                torch.cuda.synchronize()
+            e2e_s = max_over_ranks((time.perf_counter() - t0) / KE)
+            res["graph"]["e2e"] = {"value": world * m / e2e_s, "unit": "witness ring-elems/s",
+                                   "h2d_bytes_per_step": m * 64 * 8,
+                                   "d2h_bytes_per_step": hc.numel() * 8 + ht.numel() * 4}
+        del pipe
+    if rank == 0 and not args.no_cpu_baseline:
+        import numpy as np
+
+        import oracle
+        oracle.prefer_native(True)
+        nt = host_threads()
+        ms_ = 1 << 12
+        a_host = synth.synth_gl(97, 0, F_KAPPA * ms_ * 64)
+        t = oracle.NttTablesGl(6)
+        a_ntt = t.forward_batch(a_host, nthreads=nt)
+        z = synth.synth_gl(97, 1, ms_ * 64)
+        tabs = [oracle.NttTables32(oracle.Modulus32(*q), 6) for q in oracle.CRT_PRIMES]
+        t0 = time.perf_counter()
+        digits = oracle.decomp_b(z, 8)
+        oracle.ajtaigl_commit_batch(t, a_ntt, F_KAPPA, ms_, digits.reshape(8, ms_, 64), nthreads=nt,
+                                    simd=True, native=True)
+        for tb, (q, _, _) in zip(tabs, oracle.CRT_PRIMES):
+            tb.forward_batch((z % np.uint64(q)).astype(np.uint32), nthreads=nt)
+        dt = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": ms_ / dt, "unit": "witness ring-elems/s", "cores": nt, "kind": "port",
+                               "sample": f"one folding step at m={ms_} (decomp_b, 8 digit commits with the "
+                                         f"AVX-512 MAC where available, 4-prime CRT NTT), {nt} threads"}
+    return res
+
+
+# ------------------------------------------------------------------ single commitment latency
+
+S_KAPPA, S_M = 8, 256
+
+
+def bench_single(args, rank, max_over_ranks, barrier, world):
+    """One d=64 Goldilocks commitment, kappa=8, n=256 int8 digits: microseconds per commitment."""
+    import ctypes as C
+
+    import torch
+
+    from lzx_b200 import GoldilocksAjtaiKey, _lib, synth
+    A = synth.synth_gl(5, 0, S_KAPPA * S_M * 64)
+    key = GoldilocksAjtaiKey(6, S_KAPPA, S_M, A.reshape(S_KAPPA, S_M, 64))
+    W = torch.empty(S_M * 64, dtype=torch.int8, device="cuda")
+    synth.fill_device(W, "i8", 5, 1)
+    out = torch.empty((1, S_KAPPA, 64), dtype=torch.int64, device="cuda")
+    L = _lib.lib()
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    h, wp, op = key.handle, C.c_void_p(W.data_ptr()), C.c_void_p(out.data_ptr())
+    for _ in range(20):
+        _lib.check(L.lc_ajtai_commit_i8(h, wp, 1, op, st), "commit")
+    torch.cuda.synchronize()
+    K = 200
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(K):
+        L.lc_ajtai_commit_i8(h, wp, 1, op, st)
+    b.record()
+    torch.cuda.synchronize()
+    dev_us = a.elapsed_time(b) / K * 1e3
+    hw = W.cpu().numpy()
+    hout = torch.empty((1, S_KAPPA, 64), dtype=torch.int64)
+    hp, hop = hw.ctypes.data_as(C.c_void_p), C.c_void_p(hout.data_ptr())
+    for _ in range(5):
+        _lib.check(L.lc_ajtai_commit_i8_host(h, hp, 1, hop), "commit host")
+    t0 = time.perf_counter()
+    for _ in range(50):
+        L.lc_ajtai_commit_i8_host(h, hp, 1, hop)
+    host_us = (time.perf_counter() - t0) / 50 * 1e6
+    assert torch.equal(hout, out.cpu())
+    res = {"workload": "single commitment, d=64 Goldilocks, kappa=8, n=256 int8 digits",
+           "device_us_per_commit": dev_us, "e2e_us_per_commit": host_us,
+           "e2e_api": "lc_ajtai_commit_i8_host (synchronous, pageable host buffers)"}
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracle
+        oracle.prefer_native(True)
+        t = oracle.NttTablesGl(6)
+        a_ntt = t.forward_batch(A)
+        wb = hw.reshape(1, S_M, 64)
+        reps = 200
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            oracle.ajtaigl_commit_batch(t, a_ntt, S_KAPPA, S_M, wb, nthreads=1, simd=True, native=True)
+        res["cpu_baseline"] = {"value": (time.perf_counter() - t0) / reps * 1e6, "unit": "us/commit",
+                               "cores": 1, "kind": "port",
+                               "sample": f"{reps} commitments, 1 thread, AVX-512 MAC where available"}
+    return res
+
+
 # ------------------------------------------------------------------ our arm
 
 def run_ours(args):
@@ -416,6 +568,8 @@ def run_ours(args):
     e2e_value = world * TRANSFORMS_PER_STEP * COEFFS * KE / e2e_s
 
     commit = None if args.no_commit else bench_commit(args, rank, max_over_ranks, barrier, world)
+    fold = None if args.no_fold else bench_fold(args, rank, max_over_ranks, barrier, world)
+    single = bench_single(args, rank, max_over_ranks, barrier, world)
 
     if dist is not None:
         dist.destroy_process_group()
@@ -471,15 +625,18 @@ def run_ours(args):
         "gpu_launches": 2 * K,
         "clocks": clocks,
         "commit": commit,
+        "fold": fold,
+        "single_commit": single,
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
-def run_commit_only(args):
+def run_only(args, which):
     import torch
     torch.cuda.set_device(0)
-    res = bench_commit(args, 0, lambda x: x, lambda: None, 1)
+    fn = {"commit": bench_commit, "fold": bench_fold, "single": bench_single}[which]
+    res = fn(args, 0, lambda x: x, lambda: None, 1)
     print(json.dumps(res), flush=True)
     return 0
 
@@ -488,8 +645,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
-    if args.commit_only:
-        return run_commit_only(args)
+    if args.commit_only or args.only:
+        return run_only(args, args.only or "commit")
     return run_ours(args)
 
 

@@ -199,7 +199,10 @@ struct WitnessSlotStride<A, 8> {
   static constexpr int value = 273;
 };
 
-template <class A, class S, int LOG_N, int LOG_V, int NT, int BB>
+// A CTA takes JB consecutive ring elements j of BB witnesses (JB = 1 for the
+// tiled batches; small batches take several j so that a CTA still holds about
+// a hundred polynomials).  Polynomial p = jj*BB + b of the tile sits in slot p.
+template <class A, class S, int LOG_N, int LOG_V, int NT, int BB, int JB = 1>
 __global__ void __launch_bounds__(NT)
     witness_ntt_kernel(const S* __restrict__ w, typename A::T* __restrict__ what_t, uint32_t m,
                        uint32_t batch, uint32_t b_pad, const typename A::Tw* __restrict__ twg,
@@ -207,26 +210,28 @@ __global__ void __launch_bounds__(NT)
   using G = Geo<LOG_N, LOG_V>;
   using T = typename A::T;
   using Tw = typename A::Tw;
-  constexpr int N = G::N, GROUPS = NT / G::T, IT = BB / GROUPS;
+  constexpr int PP = BB * JB;  // polynomials per CTA
+  constexpr int N = G::N, GROUPS = NT / G::T, IT = PP / GROUPS;
   constexpr int SS = WitnessSlotStride<A, LOG_N>::value;
-  static_assert(BB % GROUPS == 0, "tile");
+  static_assert(PP % GROUPS == 0, "tile");
   static_assert(SS >= Slots<A, LOG_N, LOG_V>::S, "slot stride");
   extern __shared__ __align__(128) unsigned char smem_raw[];
   Tw* tw = reinterpret_cast<Tw*>(smem_raw);
   T* slots = reinterpret_cast<T*>(smem_raw + ((G::fwd_entries() * sizeof(Tw) + 15) / 16 * 16));
-  const uint32_t j = blockIdx.x;
+  const uint32_t j0 = blockIdx.x * JB;
   const uint32_t b0 = blockIdx.y * BB;
   for (int i = threadIdx.x; i < G::fwd_entries(); i += NT) tw[i] = twg[i];
   constexpr int EPC = 16 / sizeof(S);  // elements per 16-byte chunk
   constexpr int CH = N / EPC;          // chunks per polynomial
   const bool vec = (N * sizeof(S)) % 16 == 0 && (reinterpret_cast<uintptr_t>(w) & 15) == 0;
   if (vec) {
-    for (int e = threadIdx.x; e < BB * CH; e += NT) {
-      const int b = e / CH, k = e % CH;
-      T* dst = slots + b * SS + k * EPC;
-      if (b0 + b < batch) {
+    for (int e = threadIdx.x; e < PP * CH; e += NT) {
+      const int pp = e / CH, k = e % CH;
+      const int jj = pp / BB, b = pp % BB;
+      T* dst = slots + pp * SS + k * EPC;
+      if (b0 + b < batch && j0 + jj < m) {
         const uint4 v =
-            *reinterpret_cast<const uint4*>(w + ((size_t)(b0 + b) * m + j) * N + (size_t)k * EPC);
+            *reinterpret_cast<const uint4*>(w + ((size_t)(b0 + b) * m + j0 + jj) * N + (size_t)k * EPC);
         const S* x = reinterpret_cast<const S*>(&v);
 #pragma unroll
         for (int u = 0; u < EPC; ++u) dst[u] = to_residue<T, S>(x[u], q);
@@ -236,11 +241,12 @@ __global__ void __launch_bounds__(NT)
       }
     }
   } else {
-    for (int e = threadIdx.x; e < BB * N; e += NT) {
-      const int b = e / N, c = e % N;
+    for (int e = threadIdx.x; e < PP * N; e += NT) {
+      const int pp = e / N, c = e % N;
+      const int jj = pp / BB, b = pp % BB;
       T v = 0;
-      if (b0 + b < batch) v = to_residue<T, S>(w[((size_t)(b0 + b) * m + j) * N + c], q);
-      slots[b * SS + c] = v;
+      if (b0 + b < batch && j0 + jj < m) v = to_residue<T, S>(w[((size_t)(b0 + b) * m + j0 + jj) * N + c], q);
+      slots[pp * SS + c] = v;
     }
   }
   __syncthreads();
@@ -251,9 +257,12 @@ __global__ void __launch_bounds__(NT)
   for (int it = 0; it < IT; ++it)
     transform_slot<A, LOG_N, LOG_V, false>(slots + (it * GROUPS + grp) * SS, tw, ar, t);
   __syncthreads();
-  for (int e = threadIdx.x; e < BB * N; e += NT) {
-    const int tt = e / BB, b = e % BB;
-    if (b0 + b < b_pad) what_t[((size_t)tt * m + j) * b_pad + b0 + b] = slots[b * SS + tt];
+  // for each slot tt the tile's (jj, b) values are one contiguous run when BB == b_pad
+  for (int e = threadIdx.x; e < PP * N; e += NT) {
+    const int tt = e / PP, pp = e % PP;
+    const int jj = pp / BB, b = pp % BB;
+    if (b0 + b < b_pad && j0 + jj < m)
+      what_t[((size_t)tt * m + j0 + jj) * b_pad + b0 + b] = slots[pp * SS + tt];
   }
 }
 
@@ -383,6 +392,48 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// Small-batch product for b_pad a multiple of 4: one thread per (split, t,
+// row pair, 4 witnesses), 8 accumulators, so each A pair and each witness
+// quad is loaded once per 8 multiply-adds.  Lanes run along the row pairs
+// (one 128-byte A row per slot), then the witness quads (broadcast loads).
+template <class E>
+__global__ void __launch_bounds__(256)
+    mac_quad_kernel(const E* __restrict__ ahat_t, const E* __restrict__ what_t, E* __restrict__ partial,
+                    uint32_t m, uint32_t b_pad, uint32_t n, uint32_t splits, uint32_t kappa, uint32_t q) {
+  const uint32_t npair = (kappa + 1) / 2, nquad = b_pad / 4;
+  const size_t total = (size_t)splits * n * nquad * npair;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t ip = idx % npair;
+    const uint32_t bq = (idx / npair) % nquad;
+    const uint32_t t = (idx / ((size_t)npair * nquad)) % n;
+    const uint32_t split = (uint32_t)(idx / ((size_t)npair * nquad * n));
+    const uint32_t per = (m + splits - 1) / splits;
+    const uint32_t j0 = split * per, j1 = min(m, j0 + per);
+    Acc160 acc[2][4];
+    const E* ap = ahat_t + ((size_t)t * m + j0) * kIPad + 2 * ip;
+    const E* wp = what_t + ((size_t)t * m + j0) * b_pad + 4 * bq;
+#pragma unroll 2
+    for (uint32_t j = j0; j < j1; ++j) {
+      const E a0 = ap[0], a1 = ap[1];
+      E wv[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) wv[u] = wp[u];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        mac<E>(acc[0][u], a0, wv[u]);
+        mac<E>(acc[1][u], a1, wv[u]);
+      }
+      ap += kIPad;
+      wp += b_pad;
+    }
+    for (int ii = 0; ii < 2; ++ii)
+      for (int u = 0; u < 4; ++u)
+        partial[(((size_t)split * n + t) * kIPad + 2 * ip + ii) * b_pad + 4 * bq + u] =
+            acc_reduce<E>(acc[ii][u], q);
+  }
+}
+
 // Small-batch product: one thread per (split, t, i, b).
 template <class E>
 __global__ void mac_small_kernel(const E* __restrict__ ahat_t, const E* __restrict__ what_t,
@@ -475,18 +526,18 @@ static uint32_t choose_splits(uint32_t n, uint32_t btiles, uint32_t m) {
   return std::max<uint32_t>(s, 1);
 }
 
-template <class A, int LOG_N, int LOG_V, class S, int NT, int BB>
+template <class A, int LOG_N, int LOG_V, class S, int NT, int BB, int JB = 1>
 static int launch_witness_cfg(const lc_ajtai_key* key, const S* w, size_t batch, uint32_t b_pad,
                               typename A::T* dst, cudaStream_t st) {
   using G = Geo<LOG_N, LOG_V>;
   using T = typename A::T;
   constexpr int SS = WitnessSlotStride<A, LOG_N>::value;
   const size_t smem = ((G::fwd_entries() * sizeof(typename A::Tw) + 15) / 16 * 16) +
-                      (size_t)BB * SS * sizeof(T);
-  auto kern = witness_ntt_kernel<A, S, LOG_N, LOG_V, NT, BB>;
+                      (size_t)BB * JB * SS * sizeof(T);
+  auto kern = witness_ntt_kernel<A, S, LOG_N, LOG_V, NT, BB, JB>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return map_cuda(e);
-  dim3 grid(key->m, (unsigned)((b_pad + BB - 1) / BB));
+  dim3 grid((key->m + JB - 1) / JB, (unsigned)((b_pad + BB - 1) / BB));
   const lc_ntt_plan* plan = key->plan;
   kern<<<grid, NT, smem, st>>>(w, dst, key->m, (uint32_t)batch, b_pad,
                                reinterpret_cast<const typename A::Tw*>(plan->d_tw_fwd), plan->q[0],
@@ -494,8 +545,18 @@ static int launch_witness_cfg(const lc_ajtai_key* key, const S* w, size_t batch,
   return map_cuda(cudaGetLastError());
 }
 
+// Polynomials per CTA of the small-batch tiles: as many slots as fit in
+// 96 KB, a multiple of the 128-thread CTA's polynomial groups, at most 128.
+template <class A, int LOG_N, int LOG_V>
+struct SmallWitnessTile {
+  static constexpr int groups = 128 / Geo<LOG_N, LOG_V>::T;
+  static constexpr int fit = (96 * 1024) / (WitnessSlotStride<A, LOG_N>::value * (int)sizeof(typename A::T));
+  static constexpr int polys = (fit > 128 ? 128 : fit) / groups * groups;
+};
+
 // 128 witnesses per CTA when the batch is tiled and 128 slots fit in 160 KB of
-// shared memory (64 otherwise), 32 for small batches.
+// shared memory (64 otherwise); small batches: 8, 4 or 1 witnesses by as many
+// ring elements as fill SmallWitnessTile, 32 witnesses when b_pad is neither.
 template <class A, int LOG_N, int LOG_V, class S>
 static int launch_witness_to(const lc_ajtai_key* key, const S* w, size_t batch, uint32_t b_pad,
                              typename A::T* dst, cudaStream_t st) {
@@ -507,6 +568,11 @@ static int launch_witness_to(const lc_ajtai_key* key, const S* w, size_t batch, 
     else
       return launch_witness_cfg<A, LOG_N, LOG_V, S, 256, 64>(key, w, batch, b_pad, dst, st);
   }
+  constexpr int PP = SmallWitnessTile<A, LOG_N, LOG_V>::polys;
+  static_assert(PP >= 8 && PP % 8 == 0, "small tile");
+  if (b_pad % 8 == 0) return launch_witness_cfg<A, LOG_N, LOG_V, S, 128, 8, PP / 8>(key, w, batch, b_pad, dst, st);
+  if (b_pad % 4 == 0) return launch_witness_cfg<A, LOG_N, LOG_V, S, 128, 4, PP / 4>(key, w, batch, b_pad, dst, st);
+  if (b_pad < 4) return launch_witness_cfg<A, LOG_N, LOG_V, S, 128, 1, PP>(key, w, batch, b_pad, dst, st);
   return launch_witness_cfg<A, LOG_N, LOG_V, S, 128, 32>(key, w, batch, b_pad, dst, st);
 }
 
@@ -564,12 +630,15 @@ static int commit_core(lc_ajtai_key* key, size_t batch, uint32_t b_pad, void* ou
   const uint32_t n = key->n, m = key->m, kappa = key->k;
   const uint32_t q = key->plan->q[0];
   const bool tiled = b_pad % kBTile == 0;
+  const bool quad = !tiled && b_pad % 4 == 0;
   const uint32_t btiles = tiled ? b_pad / kBTile : 1;
-  // small batches: about 2^18 threads, each summing a contiguous j-range
-  const size_t outs = (size_t)n * kappa * batch;
+  // small batches: about 2^18 threads (2^19 quad threads), each summing a
+  // contiguous j-range
+  const size_t outs = quad ? (size_t)n * ((kappa + 1) / 2) * (b_pad / 4) : (size_t)n * kappa * batch;
+  const size_t want = quad ? ((size_t)1 << 19) : ((size_t)1 << 18);
   const uint32_t splits =
       tiled ? choose_splits(n, btiles, m)
-            : (uint32_t)std::max<size_t>(1, std::min<size_t>(m, ((size_t)1 << 18) / std::max<size_t>(1, outs)));
+            : (uint32_t)std::max<size_t>(1, std::min<size_t>(m, want / std::max<size_t>(1, outs)));
   int rc = grow(&key->d_partial, &key->partial_bytes, (size_t)splits * n * kIPad * b_pad * sizeof(E));
   if (rc) return rc;
   rc = grow(&key->d_chat, &key->chat_bytes, (size_t)batch * kappa * n * sizeof(E));
@@ -589,6 +658,10 @@ static int commit_core(lc_ajtai_key* key, size_t batch, uint32_t b_pad, void* ou
     }
     kern<<<dim3(n, btiles, splits), MC::NT, MC::SMEM, st>>>(ahat, what, part, m, b_pad, n, splits, q,
                                                            key->d_err);
+  } else if (quad) {
+    const size_t total = (size_t)splits * n * ((kappa + 1) / 2) * (b_pad / 4);
+    const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, 65535);
+    mac_quad_kernel<E><<<blocks, 256, 0, st>>>(ahat, what, part, m, b_pad, n, splits, kappa, q);
   } else {
     const size_t total = (size_t)splits * n * kappa * batch;
     const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, 65535);
@@ -613,7 +686,10 @@ template <class S>
 static int commit_any(lc_ajtai_key* key, const S* w, size_t batch, void* out, cudaStream_t st) {
   if (batch == 0) return LC_OK;
   if (batch > (1u << 24)) return LC_ERR_INVALID_ARGUMENT;
-  const uint32_t b_pad = batch >= 64 ? (uint32_t)((batch + kBTile - 1) / kBTile * kBTile) : (uint32_t)batch;
+  // tiles of 128 witnesses from 64 on; from 4 on a multiple of 4 (zero
+  // columns) for the quad product
+  const uint32_t b_pad = batch >= 64 ? (uint32_t)((batch + kBTile - 1) / kBTile * kBTile)
+                                     : batch >= 4 ? (uint32_t)((batch + 3) / 4 * 4) : (uint32_t)batch;
   const size_t eb = key->wide ? 8 : 4;
   int rc = grow(&key->d_what_t, &key->what_bytes, (size_t)key->n * key->m * b_pad * eb);
   if (rc) return rc;
