@@ -155,6 +155,14 @@ LC_API int lc_ajtai_commit_u8_host(lc_ajtai_key *key, const uint8_t *s, size_t b
 /* Wait for `stream` and report device-side errors of this key's kernels. */
 LC_API int lc_ajtai_key_check(lc_ajtai_key *key, lc_stream stream);
 
+/* A view of the first k rows and m columns of `parent`'s A: commits through
+ * it equal commits with a key created from that sub-matrix (rows and columns
+ * of A enter the commitment independently), without copying the cached
+ * NTT(A).  No counterpart in the reference, where an AjtaiPublicKey is built
+ * per shape; it lets callers with many commitment shapes share one resident
+ * key.  The view owns its scratch; `parent` must outlive it; NTT engine only. */
+LC_API int lc_ajtai_key_view(const lc_ajtai_key *parent, uint32_t k, uint32_t m, lc_ajtai_key **out);
+
 /* Key creation flags. */
 #define LC_KEY_TENSOR_I8 1u /* also build the INT8 tensor-core commit tables */
 
@@ -257,6 +265,58 @@ LC_API int lc_fold_pipeline_run(lc_fold_pipeline *pipe, lc_stream stream);
 /* Wait for `stream` and report device-side errors of the pipeline's kernels. */
 LC_API int lc_fold_pipeline_check(lc_fold_pipeline *pipe, lc_stream stream);
 LC_API void lc_fold_pipeline_destroy(lc_fold_pipeline *pipe);
+
+/* ------------------------------------------------------------------------
+ * Batches of uneven commitment jobs in persistent launches.
+ * No single counterpart in the reference (which commits one witness per
+ * AjtaiPublicKey::commit call, ajtai.rs:118-153): every job's result equals
+ * that call on its key's first `kappa` rows and first `n` columns.
+ * ---------------------------------------------------------------------- */
+
+/* A class: one Goldilocks key, or 1..4 u32 keys (one per prime of a CRT set),
+ * all with the same log_n (6, 7 or 8).  A job of the class is committed under
+ * every key of the class. */
+typedef struct lc_commit_class {
+  const lc_ajtai_key *keys[4];
+  uint32_t num_keys;
+} lc_commit_class;
+
+/* A job: int8 digit witness w = [n][d] (device), committed with the first
+ * kappa rows and n columns of its class's keys; out (device) = [num_keys][kappa][d]
+ * residues (uint64 for Goldilocks, uint32 per prime). */
+typedef struct lc_commit_job {
+  uint32_t cls;
+  uint32_t kappa;
+  uint32_t n;
+  const int8_t *w;
+  void *out;
+} lc_commit_job;
+
+typedef struct lc_batch lc_batch;
+
+/* Plan a batch: jobs of one key are grouped into lanes of at most 128 jobs
+ * sorted by n, so the key's cached NTT(A) is read once per lane, not once
+ * per job.  Three persistent kernels, each fed by a device work counter, run
+ * it: the witness NTTs, the products (one work item per NTT slot and chunk
+ * of ring elements), and per job the sum over chunks plus the inverse NTT.
+ * flags: LC_BATCH_GRAPH captures the three launches into a CUDA graph on
+ * the second run and replays it afterwards.  The keys must outlive the batch;
+ * runs of one batch must not overlap on the GPU. */
+#define LC_BATCH_GRAPH 1u
+LC_API int lc_batch_create(const lc_commit_class *classes, uint32_t num_classes, const lc_commit_job *jobs,
+                           uint32_t num_jobs, uint32_t flags, lc_batch **out);
+/* Tuning: ring elements per product work item (chunk, a power of two in
+ * 1024..16384), CTAs per SM of the persistent launches (1..4) and work items
+ * claimed per counter increment (1..16).  Results do not depend on them. */
+LC_API int lc_batch_set_config(lc_batch *batch, uint32_t chunk, uint32_t ctas_per_sm, uint32_t claim);
+LC_API int lc_batch_get_config(const lc_batch *batch, uint32_t *chunk, uint32_t *ctas_per_sm, uint32_t *claim);
+/* Work items of the three launches, and the lanes of the plan. */
+LC_API int lc_batch_info(const lc_batch *batch, uint64_t *items_ntt, uint64_t *items_product,
+                         uint64_t *items_finish, uint32_t *lanes);
+LC_API int lc_batch_run(lc_batch *batch, lc_stream stream);
+/* Wait for `stream` and report device-side errors of the batch's kernels. */
+LC_API int lc_batch_check(lc_batch *batch, lc_stream stream);
+LC_API void lc_batch_destroy(lc_batch *batch);
 
 /* Benchmark/test utility, no counterpart in the reference: fill `count`
  * elements of `out` (device) with the seeded counter-based synthetic stream

@@ -31,6 +31,7 @@ LC_ERR_NO_DEVICE = 12
 LC_KEY_TENSOR_I8 = 1
 LC_ENGINE_NTT = 0
 LC_ENGINE_TENSOR_I8 = 1
+LC_BATCH_GRAPH = 1
 
 
 class LatticeCudaError(RuntimeError):
@@ -92,6 +93,14 @@ def _declare(L):
         "lc_fold_pipeline_run": (i32, [P, P]),
         "lc_fold_pipeline_check": (i32, [P, P]),
         "lc_fold_pipeline_destroy": (None, [P]),
+        "lc_ajtai_key_view": (i32, [P, u32, u32, C.POINTER(P)]),
+        "lc_batch_create": (i32, [P, u32, P, u32, u32, C.POINTER(P)]),
+        "lc_batch_set_config": (i32, [P, u32, u32, u32]),
+        "lc_batch_get_config": (i32, [P, U32P, U32P, U32P]),
+        "lc_batch_info": (i32, [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), U32P]),
+        "lc_batch_run": (i32, [P, P]),
+        "lc_batch_check": (i32, [P, P]),
+        "lc_batch_destroy": (None, [P]),
         "lc_synth_fill": (i32, [i32, C.c_uint64, C.c_uint64, u32, P, sz, sz, P]),
     }
     optional = {

@@ -1,0 +1,643 @@
+// batch.cu -- many Ajtai commitments of uneven ring degree, length, row count
+// and modulus in three persistent launches fed by device work counters.
+//
+// Every job is AjtaiPublicKey::commit (lattice-commitment/src/ajtai.rs:
+// 118-153) of one int8-digit witness with the first kappa rows and n columns
+// of its class's key(s).  Jobs that share a key form lanes of at most 128
+// jobs, sorted by n (longest first).  At ring element j only the jobs with
+// n_b > j take part, so a lane's transformed witnesses are stored as a
+// staircase: slot t, ring element j, job b at  what[t*S + R[j] + b],  where
+// R[j] = sum over j' < j of the number of jobs longer than j', S = sum n_b.
+//   1. witness NTT: an item is PB consecutive staircase polynomials; their
+//      (j, b) come from a per-item start table and a short walk over R;
+//   2. product: an item is (slot t, chunk of ring elements); each thread holds
+//      2 rows x 4 jobs (160-bit accumulators) and streams the key's rows
+//      Ahat[t][j][0..16) -- read once per lane, not once per job;
+//   3. finish: an item is one job: the sum over its chunks (mod q), then the
+//      inverse NTT of its kappa rows straight into the job's output.
+// A CTA claims `claim` items at a time from the phase's counter
+// (atomicAdd), so uneven items balance across the SMs.  The three launches
+// and the counter reset are captured into a CUDA graph when asked.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <new>
+#include <vector>
+
+#include "../../include/lattice_cuda.h"
+#include "arith.cuh"
+#include "common.cuh"
+#include "internal.h"
+#include "mac.cuh"
+#include "ntt_kernels.cuh"
+
+namespace lc {
+
+constexpr int kBatchThreads = 256;
+constexpr uint32_t kLaneJobs = 128;
+constexpr uint32_t kMinChunk = 1024;
+
+// Slot strides (odd, >= N + T) that keep the transposed reads of the
+// staircase store free of bank conflicts: the commit witness tiles' values.
+template <class A, int LOG_N>
+struct BatchSlotStride;
+template <class A>
+struct BatchSlotStride<A, 6> {
+  static constexpr int value = sizeof(typename A::T) == 8 ? 73 : 75;
+};
+template <class A>
+struct BatchSlotStride<A, 7> {
+  static constexpr int value = 137;
+};
+template <class A>
+struct BatchSlotStride<A, 8> {
+  static constexpr int value = 273;
+};
+
+struct LaneDesc {
+  uint32_t kind;   // PlanKind
+  uint32_t log_n;
+  uint32_t q, qinv;
+  const void* tw_fwd;
+  const void* tw_inv;
+  const void* ahat;  // [d][a_m][16]
+  uint32_t a_m;
+  uint32_t nb;      // jobs in the lane
+  uint32_t n_max;   // longest job
+  uint32_t nchunks;
+  uint64_t S;       // staircase polynomials
+  const uint64_t* R;       // [n_max + 1]
+  const uint32_t* item_j;  // witness items: ring element of the first polynomial
+  uint32_t sub0;           // first job of the lane in the sub-job table
+  uint32_t pb;             // polynomials per witness item
+  void* what;              // [d][S]
+  void* partial;           // [nchunks][d][16][nb]
+  uint64_t item0[3];       // first item of the lane in each launch
+};
+
+struct SubJob {
+  const int8_t* w;  // [n][d]
+  void* out;        // [kappa][d] of this lane's modulus
+  uint32_t n, kappa;
+};
+
+struct BatchParams {
+  const LaneDesc* lanes;
+  const SubJob* subs;
+  unsigned long long* counters;  // [3]
+  uint32_t* err;
+  uint64_t total[3];
+  uint32_t nlanes, chunk, claim;
+};
+
+template <class A, int LOG_N, int LOG_V>
+struct BCfg {
+  using G = Geo<LOG_N, LOG_V>;
+  using T = typename A::T;
+  using Tw = typename A::Tw;
+  static constexpr int N = G::N;
+  static constexpr int GROUPS = kBatchThreads / G::T;
+  static constexpr int PB = GROUPS;  // one polynomial per thread group
+  static constexpr int SS = BatchSlotStride<A, LOG_N>::value;
+  static constexpr int TWE = G::fwd_entries() > G::inv_entries() ? G::fwd_entries() : G::inv_entries();
+  static constexpr size_t TWB = ((size_t)TWE * sizeof(Tw) + 15) / 16 * 16;
+  static constexpr size_t SMEM1 = TWB + (size_t)PB * SS * sizeof(T) + (size_t)PB * 8;
+  static constexpr size_t SMEM3 = TWB + (size_t)16 * SS * sizeof(T);
+  static_assert(SS >= Slots<A, LOG_N, LOG_V>::S, "slot stride");
+};
+
+template <class T>
+LC_D T digit_residue(int8_t x, uint32_t q);
+template <>
+LC_D uint64_t digit_residue<uint64_t>(int8_t x, uint32_t) {
+  return x >= 0 ? (uint64_t)x : kGlP - (uint64_t)(-(int)x);
+}
+template <>
+LC_D uint32_t digit_residue<uint32_t>(int8_t x, uint32_t q) {
+  return x >= 0 ? (uint32_t)x : q - (uint32_t)(-(int)x);
+}
+
+LC_D uint64_t add_mod(uint64_t a, uint64_t b, uint32_t) { return gl_add(a, b); }
+LC_D uint32_t add_mod(uint32_t a, uint32_t b, uint32_t q) {
+  const uint64_t s = (uint64_t)a + b;  // canonical inputs; q may exceed 2^31
+  return (uint32_t)(s >= q ? s - q : s);
+}
+
+// ---- launch 1: witness NTT of PB staircase polynomials
+template <class A, int LOG_N, int LOG_V>
+LC_D void witness_item(const LaneDesc& L, const SubJob* __restrict__ subs, uint64_t k, unsigned char* smem) {
+  using C = BCfg<A, LOG_N, LOG_V>;
+  using T = typename A::T;
+  using Tw = typename A::Tw;
+  constexpr int N = C::N, PB = C::PB, SS = C::SS;
+  Tw* tw = reinterpret_cast<Tw*>(smem);
+  T* slots = reinterpret_cast<T*>(smem + C::TWB);
+  uint32_t* sj = reinterpret_cast<uint32_t*>(slots + PB * SS);
+  uint32_t* sb = sj + PB;
+  const int tid = threadIdx.x;
+  const uint64_t p0 = k * PB;
+  for (int i = tid; i < Geo<LOG_N, LOG_V>::fwd_entries(); i += kBatchThreads)
+    tw[i] = reinterpret_cast<const Tw*>(L.tw_fwd)[i];
+  if (tid < PB) {
+    const uint64_t p = p0 + tid;
+    uint32_t jr = 0xFFFFFFFFu, br = 0;
+    if (p < L.S) {
+      uint32_t j = L.item_j[k];
+      while (L.R[j + 1] <= p) ++j;
+      jr = j;
+      br = (uint32_t)(p - L.R[j]);
+    }
+    sj[tid] = jr;
+    sb[tid] = br;
+  }
+  __syncthreads();
+  constexpr int CH = N / 16;  // 16-digit chunks per polynomial
+  for (int e = tid; e < PB * CH; e += kBatchThreads) {
+    const int s = e / CH, c = e % CH;
+    T* dst = slots + s * SS + c * 16;
+    if (sj[s] != 0xFFFFFFFFu) {
+      const SubJob& J = subs[L.sub0 + sb[s]];
+      const uint4 v = *reinterpret_cast<const uint4*>(J.w + (size_t)sj[s] * N + c * 16);
+      const int8_t* x = reinterpret_cast<const int8_t*>(&v);
+#pragma unroll
+      for (int u = 0; u < 16; ++u) dst[u] = digit_residue<T>(x[u], L.q);
+    } else {
+#pragma unroll
+      for (int u = 0; u < 16; ++u) dst[u] = 0;
+    }
+  }
+  __syncthreads();
+  const A ar = make_arith_q<A>(L.q, L.qinv);
+  transform_slot<A, LOG_N, LOG_V, false>(slots + (tid / Geo<LOG_N, LOG_V>::T) * SS, tw, ar,
+                                         tid % Geo<LOG_N, LOG_V>::T);
+  __syncthreads();
+  T* what = reinterpret_cast<T*>(L.what);
+  for (int e = tid; e < PB * N; e += kBatchThreads) {
+    const int tt = e / PB, s = e % PB;
+    if (sj[s] != 0xFFFFFFFFu) what[(size_t)tt * L.S + p0 + s] = slots[s * SS + tt];
+  }
+  __syncthreads();
+}
+
+// ---- launch 2: products of one (slot, chunk)
+template <class E>
+LC_D void product_item(const LaneDesc& L, const SubJob* __restrict__ subs, uint32_t chunk, uint64_t k) {
+  const uint32_t d = 1u << L.log_n;
+  const uint32_t t = (uint32_t)(k % d), c = (uint32_t)(k / d);
+  const uint32_t j0 = c * chunk, j1 = min(L.n_max, j0 + chunk);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t ip = lane & 7, bq = warp * 4 + (lane >> 3);  // rows 2ip, 2ip+1; jobs 4bq..4bq+3
+  uint32_t nq[4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const uint32_t b = 4 * bq + u;
+    nq[u] = b < L.nb ? subs[L.sub0 + b].n : 0;  // sorted: nq[0] >= nq[1] >= ...
+  }
+  Acc160 acc[2][4];
+  const E* A = reinterpret_cast<const E*>(L.ahat) + ((size_t)t * L.a_m) * kIPad + 2 * ip;
+  const E* W = reinterpret_cast<const E*>(L.what) + (size_t)t * L.S + 4 * bq;
+  const uint32_t jend = min(j1, nq[0]);
+#pragma unroll 2
+  for (uint32_t j = j0; j < jend; ++j) {
+    const E a0 = A[(size_t)j * kIPad], a1 = A[(size_t)j * kIPad + 1];
+    const uint64_t r0 = L.R[j];
+    E wv[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) wv[u] = j < nq[u] ? W[r0 + u] : E(0);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      mac<E>(acc[0][u], a0, wv[u]);
+      mac<E>(acc[1][u], a1, wv[u]);
+    }
+  }
+  // jobs active at j0 own a partial of this chunk (the finish launch reads
+  // chunks c with c*chunk < n_b)
+  E* P = reinterpret_cast<E*>(L.partial) + ((size_t)c * d + t) * kIPad * L.nb;
+#pragma unroll
+  for (int ii = 0; ii < 2; ++ii)
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (j0 < nq[u]) P[(size_t)(2 * ip + ii) * L.nb + 4 * bq + u] = acc_reduce<E>(acc[ii][u], L.q);
+}
+
+// ---- launch 3: one job's chunk sums and inverse NTT
+template <class A, int LOG_N, int LOG_V>
+LC_D void finish_item(const LaneDesc& L, const SubJob* __restrict__ subs, uint32_t chunk, uint64_t b,
+                      unsigned char* smem) {
+  using C = BCfg<A, LOG_N, LOG_V>;
+  using T = typename A::T;
+  using Tw = typename A::Tw;
+  constexpr int N = C::N, SS = C::SS, GROUPS = C::GROUPS;
+  Tw* tw = reinterpret_cast<Tw*>(smem);
+  T* slots = reinterpret_cast<T*>(smem + C::TWB);
+  const int tid = threadIdx.x;
+  const SubJob J = subs[L.sub0 + b];
+  const uint32_t nch = (J.n + chunk - 1) / chunk;
+  for (int i = tid; i < Geo<LOG_N, LOG_V>::inv_entries(); i += kBatchThreads)
+    tw[i] = reinterpret_cast<const Tw*>(L.tw_inv)[i];
+  const T* P = reinterpret_cast<const T*>(L.partial);
+  for (uint32_t e = tid; e < J.kappa * N; e += kBatchThreads) {
+    const uint32_t i = e / N, tt = e % N;
+    T s = 0;
+    for (uint32_t c = 0; c < nch; ++c) s = add_mod(s, P[(((size_t)c * N + tt) * kIPad + i) * L.nb + b], L.q);
+    slots[i * SS + tt] = s;
+  }
+  __syncthreads();
+  const A ar = make_arith_q<A>(L.q, L.qinv);
+  const int grp = tid / Geo<LOG_N, LOG_V>::T;
+  const uint32_t lt = tid % Geo<LOG_N, LOG_V>::T;
+  for (uint32_t p0 = 0; p0 < J.kappa; p0 += GROUPS)
+    if (p0 + grp < J.kappa) transform_slot<A, LOG_N, LOG_V, true>(slots + (p0 + grp) * SS, tw, ar, lt);
+  __syncthreads();
+  T* out = reinterpret_cast<T*>(J.out);
+  for (uint32_t e = tid; e < J.kappa * N; e += kBatchThreads) out[e] = slots[(e / N) * SS + e % N];
+  __syncthreads();
+}
+
+template <int PHASE>
+LC_D void run_item(const BatchParams& p, const LaneDesc& L, uint64_t k, unsigned char* smem) {
+  const int key = (int)L.kind * 16 + (int)L.log_n;
+  constexpr int GL = (int)PlanKind::Goldilocks * 16, SL = (int)PlanKind::U32Lazy * 16, MC = (int)PlanKind::U32Mont * 16;
+  if (PHASE == 1) {
+    if (L.kind == (uint32_t)PlanKind::Goldilocks)
+      product_item<uint64_t>(L, p.subs, p.chunk, k);
+    else
+      product_item<uint32_t>(L, p.subs, p.chunk, k);
+    return;
+  }
+#define LC_BATCH_CASE(K, A, LN, LV)                       \
+  case K + LN:                                            \
+    if (PHASE == 0)                                       \
+      witness_item<A, LN, LV>(L, p.subs, k, smem);        \
+    else                                                  \
+      finish_item<A, LN, LV>(L, p.subs, p.chunk, k, smem); \
+    return;
+  switch (key) {
+    LC_BATCH_CASE(GL, Goldilocks, 6, 3)
+    LC_BATCH_CASE(GL, Goldilocks, 7, 4)
+    LC_BATCH_CASE(GL, Goldilocks, 8, 4)
+    LC_BATCH_CASE(SL, ShoupLazy, 6, 3)
+    LC_BATCH_CASE(SL, ShoupLazy, 7, 4)
+    LC_BATCH_CASE(SL, ShoupLazy, 8, 4)
+    LC_BATCH_CASE(MC, MontCanon, 6, 3)
+    LC_BATCH_CASE(MC, MontCanon, 7, 4)
+    LC_BATCH_CASE(MC, MontCanon, 8, 4)
+    default:
+      if (threadIdx.x == 0) record_error(p.err, 2);
+  }
+#undef LC_BATCH_CASE
+}
+
+template <int PHASE>
+__global__ void __launch_bounds__(kBatchThreads) batch_kernel(const __grid_constant__ BatchParams p) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ unsigned long long s_base;
+  const uint64_t total = p.total[PHASE];
+  uint32_t lane = 0;
+  for (;;) {
+    if (threadIdx.x == 0) s_base = atomicAdd(&p.counters[PHASE], (unsigned long long)p.claim);
+    __syncthreads();
+    const uint64_t base = s_base;
+    __syncthreads();
+    if (base >= total) break;
+    const uint64_t end = min(base + p.claim, total);
+    for (uint64_t it = base; it < end; ++it) {
+      // claims only grow, so the lane index only moves forward
+      while (lane + 1 < p.nlanes && p.lanes[lane + 1].item0[PHASE] <= it) ++lane;
+      run_item<PHASE>(p, p.lanes[lane], it - p.lanes[lane].item0[PHASE], smem);
+    }
+  }
+}
+
+template <class A, int LOG_N, int LOG_V>
+static void smem_need(size_t& s1, size_t& s3, uint32_t& pb) {
+  using C = BCfg<A, LOG_N, LOG_V>;
+  s1 = C::SMEM1;
+  s3 = C::SMEM3;
+  pb = C::PB;
+}
+
+static bool lane_geometry(PlanKind kind, uint32_t log_n, size_t& s1, size_t& s3, uint32_t& pb) {
+  switch ((int)kind * 16 + (int)log_n) {
+#define LC_GEO(K, A, LN, LV)            \
+  case (int)K * 16 + LN:                \
+    smem_need<A, LN, LV>(s1, s3, pb);   \
+    return true;
+    LC_GEO(PlanKind::Goldilocks, Goldilocks, 6, 3)
+    LC_GEO(PlanKind::Goldilocks, Goldilocks, 7, 4)
+    LC_GEO(PlanKind::Goldilocks, Goldilocks, 8, 4)
+    LC_GEO(PlanKind::U32Lazy, ShoupLazy, 6, 3)
+    LC_GEO(PlanKind::U32Lazy, ShoupLazy, 7, 4)
+    LC_GEO(PlanKind::U32Lazy, ShoupLazy, 8, 4)
+    LC_GEO(PlanKind::U32Mont, MontCanon, 6, 3)
+    LC_GEO(PlanKind::U32Mont, MontCanon, 7, 4)
+    LC_GEO(PlanKind::U32Mont, MontCanon, 8, 4)
+#undef LC_GEO
+    default:
+      return false;
+  }
+}
+
+}  // namespace lc
+
+struct lc_batch {
+  std::vector<lc::LaneDesc> lanes;     // host copies (device pointers inside)
+  std::vector<uint64_t> lane_elem;     // element bytes per lane
+  lc::LaneDesc* d_lanes = nullptr;
+  lc::SubJob* d_subs = nullptr;
+  uint64_t* d_R = nullptr;
+  uint32_t* d_itemj = nullptr;
+  unsigned char* d_what = nullptr;
+  unsigned char* d_partial = nullptr;
+  unsigned long long* d_counters = nullptr;
+  uint32_t* d_err = nullptr;
+  uint64_t total[3] = {0, 0, 0};
+  size_t smem[3] = {0, 0, 0};
+  uint32_t chunk = 4096, ctas = 2, claim = 1;
+  uint32_t flags = 0;
+  bool warmed = false, dirty = true;
+  cudaStream_t cap = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+namespace lc {
+
+static void batch_free(lc_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->cap) cudaStreamDestroy(b->cap);
+  for (void* p : {(void*)b->d_lanes, (void*)b->d_subs, (void*)b->d_R, (void*)b->d_itemj, (void*)b->d_what,
+                  (void*)b->d_partial, (void*)b->d_counters, (void*)b->d_err})
+    if (p) cudaFree(p);
+  delete b;
+}
+
+// chunk-dependent fields, item bases and the device copy of the lanes
+static int batch_layout(lc_batch* b) {
+  uint64_t base[3] = {0, 0, 0};
+  for (auto& L : b->lanes) {
+    L.nchunks = (L.n_max + b->chunk - 1) / b->chunk;
+    const uint64_t items[3] = {(L.S + L.pb - 1) / L.pb, (uint64_t)(1u << L.log_n) * L.nchunks, L.nb};
+    for (int ph = 0; ph < 3; ++ph) {
+      L.item0[ph] = base[ph];
+      base[ph] += items[ph];
+    }
+  }
+  for (int ph = 0; ph < 3; ++ph) b->total[ph] = base[ph];
+  if (cudaMemcpy(b->d_lanes, b->lanes.data(), b->lanes.size() * sizeof(LaneDesc), cudaMemcpyHostToDevice) !=
+      cudaSuccess)
+    return map_cuda(cudaGetLastError());
+  b->dirty = true;
+  return LC_OK;
+}
+
+static int batch_launch(lc_batch* b, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(b->d_counters, 0, 3 * sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return map_cuda(e);
+  BatchParams p{};
+  p.lanes = b->d_lanes;
+  p.subs = b->d_subs;
+  p.counters = b->d_counters;
+  p.err = b->d_err;
+  for (int ph = 0; ph < 3; ++ph) p.total[ph] = b->total[ph];
+  p.nlanes = (uint32_t)b->lanes.size();
+  p.chunk = b->chunk;
+  p.claim = b->claim;
+  const unsigned grid = (unsigned)std::max(1, device_sm_count()) * b->ctas;
+  batch_kernel<0><<<grid, kBatchThreads, b->smem[0], st>>>(p);
+  batch_kernel<1><<<grid, kBatchThreads, b->smem[1], st>>>(p);
+  batch_kernel<2><<<grid, kBatchThreads, b->smem[2], st>>>(p);
+  return map_cuda(cudaGetLastError());
+}
+
+}  // namespace lc
+
+extern "C" {
+
+LC_API int lc_batch_create(const lc_commit_class* classes, uint32_t num_classes, const lc_commit_job* jobs,
+                           uint32_t num_jobs, uint32_t flags, lc_batch** out) {
+  using namespace lc;
+  if (!out || (num_classes && !classes) || (num_jobs && !jobs) || (flags & ~LC_BATCH_GRAPH))
+    return LC_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  // ---- validate
+  for (uint32_t c = 0; c < num_classes; ++c) {
+    const lc_commit_class& C = classes[c];
+    if (C.num_keys < 1 || C.num_keys > 4) return LC_ERR_INVALID_ARGUMENT;
+    for (uint32_t k = 0; k < C.num_keys; ++k) {
+      const lc_ajtai_key* K = C.keys[k];
+      if (!K || K->log_n != C.keys[0]->log_n || K->wide != C.keys[0]->wide) return LC_ERR_INVALID_ARGUMENT;
+      if (K->log_n < 6 || K->log_n > 8) return LC_ERR_UNSUPPORTED;
+    }
+    if (C.keys[0]->wide && C.num_keys != 1) return LC_ERR_INVALID_ARGUMENT;
+  }
+  for (uint32_t i = 0; i < num_jobs; ++i) {
+    const lc_commit_job& J = jobs[i];
+    if (J.cls >= num_classes || !J.w || !J.out || J.n == 0 || J.kappa == 0) return LC_ERR_INVALID_ARGUMENT;
+    if (reinterpret_cast<uintptr_t>(J.w) & 15) return LC_ERR_INVALID_ARGUMENT;
+    for (uint32_t k = 0; k < classes[J.cls].num_keys; ++k) {
+      const lc_ajtai_key* K = classes[J.cls].keys[k];
+      if (J.kappa > K->k || J.n > K->m) return LC_ERR_DIMENSION_MISMATCH;
+    }
+  }
+  lc_batch* b = new (std::nothrow) lc_batch();
+  if (!b) return LC_ERR_OUT_OF_MEMORY;
+  b->flags = flags;
+  // ---- lanes: per class and key, jobs sorted by n (longest first), 128 at a time
+  std::vector<SubJob> subs;
+  std::vector<uint64_t> Rall;
+  std::vector<uint32_t> itemj_all;
+  std::vector<size_t> r_off, ij_off;
+  size_t what_bytes = 0, partial_bytes = 0;
+  std::vector<size_t> what_off, part_off;
+  for (uint32_t c = 0; c < num_classes; ++c) {
+    std::vector<uint32_t> idx;
+    for (uint32_t i = 0; i < num_jobs; ++i)
+      if (jobs[i].cls == c) idx.push_back(i);
+    std::stable_sort(idx.begin(), idx.end(), [&](uint32_t x, uint32_t y) { return jobs[x].n > jobs[y].n; });
+    for (uint32_t k = 0; k < classes[c].num_keys; ++k) {
+      const lc_ajtai_key* K = classes[c].keys[k];
+      const size_t eb = K->wide ? 8 : 4;
+      const uint32_t d = 1u << K->log_n;
+      for (size_t g0 = 0; g0 < idx.size(); g0 += kLaneJobs) {
+        const size_t g1 = std::min(idx.size(), g0 + (size_t)kLaneJobs);
+        LaneDesc L{};
+        L.kind = (uint32_t)K->plan->kind;
+        L.log_n = K->log_n;
+        L.q = K->plan->q[0];
+        L.qinv = K->plan->qinv[0];
+        L.tw_fwd = K->plan->d_tw_fwd;
+        L.tw_inv = K->plan->d_tw_inv;
+        L.ahat = K->d_ahat_t;
+        L.a_m = K->a_m;
+        L.nb = (uint32_t)(g1 - g0);
+        L.sub0 = (uint32_t)subs.size();
+        size_t s1, s3;
+        uint32_t pb;
+        if (!lane_geometry(K->plan->kind, K->log_n, s1, s3, pb)) {
+          batch_free(b);
+          return LC_ERR_UNSUPPORTED;
+        }
+        b->smem[0] = std::max(b->smem[0], s1);
+        b->smem[2] = std::max(b->smem[2], s3);
+        L.pb = pb;
+        for (size_t g = g0; g < g1; ++g) {
+          const lc_commit_job& J = jobs[idx[g]];
+          SubJob sj{J.w, static_cast<unsigned char*>(J.out) + (size_t)k * J.kappa * d * eb, J.n, J.kappa};
+          subs.push_back(sj);
+        }
+        L.n_max = jobs[idx[g0]].n;
+        // staircase offsets R[j] and the witness items' first ring elements
+        r_off.push_back(Rall.size());
+        std::vector<uint64_t> R(L.n_max + 1);
+        uint64_t acc = 0;
+        size_t active = g1 - g0;  // jobs longer than j
+        for (uint32_t j = 0; j < L.n_max; ++j) {
+          while (active > 0 && jobs[idx[g0 + active - 1]].n <= j) --active;
+          R[j] = acc;
+          acc += active;
+        }
+        R[L.n_max] = acc;
+        L.S = acc;
+        ij_off.push_back(itemj_all.size());
+        const uint64_t items = (L.S + pb - 1) / pb;
+        uint32_t j = 0;
+        for (uint64_t it = 0; it < items; ++it) {
+          const uint64_t p = it * pb;
+          while (R[j + 1] <= p) ++j;
+          itemj_all.push_back(j);
+        }
+        Rall.insert(Rall.end(), R.begin(), R.end());
+        what_off.push_back(what_bytes);
+        what_bytes += ((size_t)d * L.S * eb + 255) / 256 * 256;
+        part_off.push_back(partial_bytes);
+        partial_bytes += (((size_t)(L.n_max + kMinChunk - 1) / kMinChunk) * d * kIPad * L.nb * eb + 255) / 256 * 256;
+        b->lanes.push_back(L);
+      }
+    }
+  }
+  // ---- device buffers
+  const size_t nl = std::max<size_t>(1, b->lanes.size());
+  if (cudaMalloc(&b->d_lanes, nl * sizeof(LaneDesc)) != cudaSuccess ||
+      cudaMalloc(&b->d_subs, std::max<size_t>(1, subs.size()) * sizeof(SubJob)) != cudaSuccess ||
+      cudaMalloc(&b->d_R, std::max<size_t>(1, Rall.size()) * 8) != cudaSuccess ||
+      cudaMalloc(&b->d_itemj, std::max<size_t>(1, itemj_all.size()) * 4) != cudaSuccess ||
+      cudaMalloc(&b->d_what, std::max<size_t>(256, what_bytes)) != cudaSuccess ||
+      cudaMalloc(&b->d_partial, std::max<size_t>(256, partial_bytes)) != cudaSuccess ||
+      cudaMalloc(&b->d_counters, 3 * sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&b->d_err, 4) != cudaSuccess) {
+    cudaGetLastError();
+    batch_free(b);
+    return LC_ERR_OUT_OF_MEMORY;
+  }
+  cudaMemset(b->d_err, 0, 4);
+  if (!subs.empty()) cudaMemcpy(b->d_subs, subs.data(), subs.size() * sizeof(SubJob), cudaMemcpyHostToDevice);
+  if (!Rall.empty()) cudaMemcpy(b->d_R, Rall.data(), Rall.size() * 8, cudaMemcpyHostToDevice);
+  if (!itemj_all.empty())
+    cudaMemcpy(b->d_itemj, itemj_all.data(), itemj_all.size() * 4, cudaMemcpyHostToDevice);
+  for (size_t l = 0; l < b->lanes.size(); ++l) {
+    LaneDesc& L = b->lanes[l];
+    L.R = b->d_R + r_off[l];
+    L.item_j = b->d_itemj + ij_off[l];
+    L.what = b->d_what + what_off[l];
+    L.partial = b->d_partial + part_off[l];
+  }
+  const int rc = batch_layout(b);
+  if (rc) {
+    batch_free(b);
+    return rc;
+  }
+  *out = b;
+  return LC_OK;
+}
+
+LC_API int lc_batch_set_config(lc_batch* b, uint32_t chunk, uint32_t ctas_per_sm, uint32_t claim) {
+  using namespace lc;
+  if (!b || chunk < kMinChunk || chunk > 16384 || (chunk & (chunk - 1)) || ctas_per_sm < 1 || ctas_per_sm > 4 ||
+      claim < 1 || claim > 16)
+    return LC_ERR_INVALID_ARGUMENT;
+  b->chunk = chunk;
+  b->ctas = ctas_per_sm;
+  b->claim = claim;
+  return batch_layout(b);
+}
+
+LC_API int lc_batch_get_config(const lc_batch* b, uint32_t* chunk, uint32_t* ctas_per_sm, uint32_t* claim) {
+  if (!b) return LC_ERR_INVALID_ARGUMENT;
+  if (chunk) *chunk = b->chunk;
+  if (ctas_per_sm) *ctas_per_sm = b->ctas;
+  if (claim) *claim = b->claim;
+  return LC_OK;
+}
+
+LC_API int lc_batch_info(const lc_batch* b, uint64_t* items_ntt, uint64_t* items_product, uint64_t* items_finish,
+                         uint32_t* lanes) {
+  if (!b) return LC_ERR_INVALID_ARGUMENT;
+  if (items_ntt) *items_ntt = b->total[0];
+  if (items_product) *items_product = b->total[1];
+  if (items_finish) *items_finish = b->total[2];
+  if (lanes) *lanes = (uint32_t)b->lanes.size();
+  return LC_OK;
+}
+
+LC_API int lc_batch_run(lc_batch* b, lc_stream stream) {
+  using namespace lc;
+  if (!b) return LC_ERR_INVALID_ARGUMENT;
+  if (b->lanes.empty()) return LC_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!(b->flags & LC_BATCH_GRAPH) || !b->warmed) {
+    const int rc = batch_launch(b, st);
+    if (!rc) b->warmed = true;
+    return rc;
+  }
+  if (b->dirty && b->exec) {
+    cudaGraphExecDestroy(b->exec);
+    cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+  }
+  if (!b->exec) {
+    if (!b->cap && cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking) != cudaSuccess)
+      return map_cuda(cudaGetLastError());
+    cudaError_t e = cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return map_cuda(e);
+    const int rc = batch_launch(b, b->cap);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(b->cap, &g);
+    if (rc || e != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      return rc ? rc : map_cuda(e);
+    }
+    e = cudaGraphInstantiate(&b->exec, g, 0);
+    if (e != cudaSuccess) {
+      cudaGraphDestroy(g);
+      b->exec = nullptr;
+      return map_cuda(e);
+    }
+    b->graph = g;
+    b->dirty = false;
+  }
+  return map_cuda(cudaGraphLaunch(b->exec, st));
+}
+
+LC_API int lc_batch_check(lc_batch* b, lc_stream stream) {
+  using namespace lc;
+  if (!b) return LC_ERR_INVALID_ARGUMENT;
+  cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+  if (e != cudaSuccess) return map_cuda(e);
+  uint32_t flag = 0;
+  if (cudaMemcpy(&flag, b->d_err, 4, cudaMemcpyDeviceToHost) != cudaSuccess) return map_cuda(cudaGetLastError());
+  if (flag) {
+    cudaMemset(b->d_err, 0, 4);
+    return LC_ERR_UNSUPPORTED;
+  }
+  return LC_OK;
+}
+
+LC_API void lc_batch_destroy(lc_batch* b) {
+  if (b) lc::batch_free(b);
+}
+
+}  // extern "C"

@@ -23,107 +23,13 @@
 
 #include "../../include/lattice_cuda.h"
 #include "internal.h"
+#include "mac.cuh"
 #include "ntt_kernels.cuh"
 
 namespace lc {
 
-constexpr int kIPad = 16;    // rows of A per MAC tile (padded)
 constexpr int kBTile = 128;  // witnesses per MAC tile
 
-// ------------------------------------------------------------------ element traits
-
-template <class E>
-struct Field;
-
-template <>
-struct Field<uint64_t> {  // Goldilocks
-  LC_D static uint64_t reduce160(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3, uint32_t r4,
-                                 uint32_t) {
-    // x = (r3 r2)*2^64 + (r1 r0) + r4*2^128;  2^128 == -2^32 (mod p)
-    uint64_t lo = ((uint64_t)r1 << 32) | r0;
-    uint64_t hi = ((uint64_t)r3 << 32) | r2;
-    uint64_t y = gl_canon(gl_reduce128_lazy(hi, lo));
-    uint64_t z = gl_canon(((uint64_t)r4 << 32) % kGlP);  // r4 * 2^32 < 2^64
-    return gl_sub(y, z);
-  }
-  LC_D static uint64_t add(uint64_t a, uint64_t b, uint32_t) { return gl_add(a, b); }
-};
-
-template <>
-struct Field<uint32_t> {  // any odd u32 modulus q
-  LC_D static uint32_t reduce160(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3, uint32_t r4,
-                                 uint32_t q) {
-    // products are < 2^64 and at most 2^32 of them are summed: r3 = r4 = 0 is
-    // not assumed; fold limb by limb from the top with 64-bit remainders.
-    uint64_t acc = r4 % q;
-    acc = ((acc << 32) | r3) % q;
-    acc = ((acc << 32) | r2) % q;
-    acc = ((acc << 32) | r1) % q;
-    acc = ((acc << 32) | r0) % q;
-    return (uint32_t)acc;
-  }
-  LC_D static uint32_t add(uint32_t a, uint32_t b, uint32_t q) {
-    uint32_t s = a + b;
-    return (s < a || s >= q) ? s - q : s;
-  }
-};
-
-// 160-bit accumulator: outer products a0*b0 and a1*b1 into r0..r4, the two
-// middle products into m0..m2 (added at 2^32 when the sum is reduced).
-struct Acc160 {
-  uint32_t r0 = 0, r1 = 0, r2 = 0, r3 = 0, r4 = 0, m0 = 0, m1 = 0, m2 = 0;
-};
-
-LC_D void mac64(Acc160& c, uint64_t a, uint64_t b) {
-  const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32);
-  const uint32_t b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
-  asm("mad.lo.cc.u32 %0, %5, %7, %0;\n\t"
-      "madc.hi.cc.u32 %1, %5, %7, %1;\n\t"
-      "madc.lo.cc.u32 %2, %6, %8, %2;\n\t"
-      "madc.hi.cc.u32 %3, %6, %8, %3;\n\t"
-      "addc.u32 %4, %4, 0;"
-      : "+r"(c.r0), "+r"(c.r1), "+r"(c.r2), "+r"(c.r3), "+r"(c.r4)
-      : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
-  asm("mad.lo.cc.u32 %0, %3, %6, %0;\n\t"
-      "madc.hi.cc.u32 %1, %3, %6, %1;\n\t"
-      "addc.u32 %2, %2, 0;\n\t"
-      "mad.lo.cc.u32 %0, %4, %5, %0;\n\t"
-      "madc.hi.cc.u32 %1, %4, %5, %1;\n\t"
-      "addc.u32 %2, %2, 0;"
-      : "+r"(c.m0), "+r"(c.m1), "+r"(c.m2)
-      : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
-}
-
-LC_D void mac32(Acc160& c, uint32_t a, uint32_t b) {
-  asm("mad.lo.cc.u32 %0, %3, %4, %0;\n\t"
-      "madc.hi.cc.u32 %1, %3, %4, %1;\n\t"
-      "addc.u32 %2, %2, 0;"
-      : "+r"(c.r0), "+r"(c.r1), "+r"(c.r2)
-      : "r"(a), "r"(b));
-}
-
-template <class E>
-LC_D void mac(Acc160& c, E a, E b);
-template <>
-LC_D void mac<uint64_t>(Acc160& c, uint64_t a, uint64_t b) {
-  mac64(c, a, b);
-}
-template <>
-LC_D void mac<uint32_t>(Acc160& c, uint32_t a, uint32_t b) {
-  mac32(c, a, b);
-}
-
-template <class E>
-LC_D E acc_reduce(const Acc160& c, uint32_t q) {
-  uint32_t r1, r2, r3, r4;
-  asm("add.cc.u32 %0, %4, %7;\n\t"
-      "addc.cc.u32 %1, %5, %8;\n\t"
-      "addc.cc.u32 %2, %6, %9;\n\t"
-      "addc.u32 %3, %10, 0;"
-      : "=r"(r1), "=r"(r2), "=r"(r3), "=r"(r4)
-      : "r"(c.r1), "r"(c.r2), "r"(c.r3), "r"(c.m0), "r"(c.m1), "r"(c.m2), "r"(c.r4));
-  return Field<E>::reduce160(c.r0, r1, r2, r3, r4, q);
-}
 
 // ------------------------------------------------------------------ kernels
 
@@ -310,7 +216,7 @@ struct MacCfg {
 
 template <class E, int JB>
 __global__ void __launch_bounds__(256)
-    mac_tiled_kernel(const E* __restrict__ ahat_t, const E* __restrict__ what_t, E* __restrict__ partial,
+    mac_tiled_kernel(const E* __restrict__ ahat_t, uint32_t am, const E* __restrict__ what_t, E* __restrict__ partial,
                      uint32_t m, uint32_t b_pad, uint32_t n, uint32_t splits, uint32_t q,
                      uint32_t* err) {
   using C = MacCfg<E, JB>;
@@ -333,7 +239,7 @@ __global__ void __launch_bounds__(256)
     const uint32_t rows = min((uint32_t)JB, j1 - jb);
     const uint32_t a_bytes = rows * kIPad * sizeof(E);
     mbar_arrive_expect_tx(&bar[s], a_bytes + rows * kBTile * (uint32_t)sizeof(E));
-    bulk_g2s(stage_a(s), ahat_t + ((size_t)t * m + jb) * kIPad, a_bytes, &bar[s]);
+    bulk_g2s(stage_a(s), ahat_t + ((size_t)t * am + jb) * kIPad, a_bytes, &bar[s]);
     if (b_pad == kBTile) {
       bulk_g2s(stage_w(s), what_t + ((size_t)t * m + jb) * b_pad, rows * kBTile * sizeof(E), &bar[s]);
     } else {
@@ -398,7 +304,7 @@ __global__ void __launch_bounds__(256)
 // (one 128-byte A row per slot), then the witness quads (broadcast loads).
 template <class E>
 __global__ void __launch_bounds__(256)
-    mac_quad_kernel(const E* __restrict__ ahat_t, const E* __restrict__ what_t, E* __restrict__ partial,
+    mac_quad_kernel(const E* __restrict__ ahat_t, uint32_t am, const E* __restrict__ what_t, E* __restrict__ partial,
                     uint32_t m, uint32_t b_pad, uint32_t n, uint32_t splits, uint32_t kappa, uint32_t q) {
   const uint32_t npair = (kappa + 1) / 2, nquad = b_pad / 4;
   const size_t total = (size_t)splits * n * nquad * npair;
@@ -411,7 +317,7 @@ __global__ void __launch_bounds__(256)
     const uint32_t per = (m + splits - 1) / splits;
     const uint32_t j0 = split * per, j1 = min(m, j0 + per);
     Acc160 acc[2][4];
-    const E* ap = ahat_t + ((size_t)t * m + j0) * kIPad + 2 * ip;
+    const E* ap = ahat_t + ((size_t)t * am + j0) * kIPad + 2 * ip;
     const E* wp = what_t + ((size_t)t * m + j0) * b_pad + 4 * bq;
 #pragma unroll 2
     for (uint32_t j = j0; j < j1; ++j) {
@@ -436,7 +342,7 @@ __global__ void __launch_bounds__(256)
 
 // Small-batch product: one thread per (split, t, i, b).
 template <class E>
-__global__ void mac_small_kernel(const E* __restrict__ ahat_t, const E* __restrict__ what_t,
+__global__ void mac_small_kernel(const E* __restrict__ ahat_t, uint32_t am, const E* __restrict__ what_t,
                                  E* __restrict__ partial, uint32_t m, uint32_t b_pad, uint32_t n,
                                  uint32_t splits, uint32_t kappa, uint32_t batch, uint32_t q) {
   const size_t total = (size_t)splits * n * kappa * batch;
@@ -450,7 +356,7 @@ __global__ void mac_small_kernel(const E* __restrict__ ahat_t, const E* __restri
     const uint32_t j0 = split * per, j1 = min(m, j0 + per);
     Acc160 acc;
     for (uint32_t j = j0; j < j1; ++j)
-      mac<E>(acc, ahat_t[((size_t)t * m + j) * kIPad + i], what_t[((size_t)t * m + j) * b_pad + b]);
+      mac<E>(acc, ahat_t[((size_t)t * am + j) * kIPad + i], what_t[((size_t)t * m + j) * b_pad + b]);
     partial[(((size_t)split * n + t) * kIPad + i) * b_pad + b] = acc_reduce<E>(acc, q);
   }
 }
@@ -479,29 +385,8 @@ using namespace lc;
 
 // ------------------------------------------------------------------ key object
 
-struct lc_ajtai_key {
-  lc_ntt_plan* plan = nullptr;  // owned copy of the ring's plan
-  uint32_t k = 0, m = 0, n = 0, log_n = 0;
-  bool wide = false;           // Goldilocks (u64) or u32
-  void* d_ahat_t = nullptr;    // [n][m][16]
-  // scratch, grown on demand
-  void* d_what_t = nullptr;
-  size_t what_bytes = 0;
-  void* d_partial = nullptr;
-  size_t partial_bytes = 0;
-  void* d_chat = nullptr;
-  size_t chat_bytes = 0;
-  void* d_wtmp = nullptr;  // generic witness path: converted + transformed witnesses
-  size_t wtmp_bytes = 0;
-  void* d_in = nullptr;  // host-API staging
-  size_t in_bytes = 0;
-  void* d_out = nullptr;
-  size_t out_bytes = 0;
-  cudaStream_t host_stream = nullptr;
-  uint32_t* d_err = nullptr;
-  lc_tc_tables* tc = nullptr;  // tensor-core engine tables (LC_KEY_TENSOR_I8)
-  int engine = LC_ENGINE_NTT;
-};
+// struct lc_ajtai_key is defined in internal.h
+
 
 namespace lc {
 
@@ -656,16 +541,16 @@ static int commit_core(lc_ajtai_key* key, size_t batch, uint32_t b_pad, void* ou
         return map_cuda(cudaGetLastError());
       attr = true;
     }
-    kern<<<dim3(n, btiles, splits), MC::NT, MC::SMEM, st>>>(ahat, what, part, m, b_pad, n, splits, q,
+    kern<<<dim3(n, btiles, splits), MC::NT, MC::SMEM, st>>>(ahat, key->a_m, what, part, m, b_pad, n, splits, q,
                                                            key->d_err);
   } else if (quad) {
     const size_t total = (size_t)splits * n * ((kappa + 1) / 2) * (b_pad / 4);
     const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, 65535);
-    mac_quad_kernel<E><<<blocks, 256, 0, st>>>(ahat, what, part, m, b_pad, n, splits, kappa, q);
+    mac_quad_kernel<E><<<blocks, 256, 0, st>>>(ahat, key->a_m, what, part, m, b_pad, n, splits, kappa, q);
   } else {
     const size_t total = (size_t)splits * n * kappa * batch;
     const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, 65535);
-    mac_small_kernel<E><<<blocks, 256, 0, st>>>(ahat, what, part, m, b_pad, n, splits, kappa,
+    mac_small_kernel<E><<<blocks, 256, 0, st>>>(ahat, key->a_m, what, part, m, b_pad, n, splits, kappa,
                                                 (uint32_t)batch, q);
   }
   rc = map_cuda(cudaGetLastError());
@@ -795,11 +680,11 @@ static int noalloc_commit(const lc_ajtai_key* key, const E* s, size_t batch, voi
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MC::SMEM);
     if (e != cudaSuccess) return map_cuda(e);
     kern<<<dim3(n, btiles, splits), MC::NT, MC::SMEM, st>>>(
-        reinterpret_cast<const E*>(key->d_ahat_t), what, part, m, b_pad, n, splits, q, key->d_err);
+        reinterpret_cast<const E*>(key->d_ahat_t), key->a_m, what, part, m, b_pad, n, splits, q, key->d_err);
   } else {
     const size_t total = (size_t)splits * n * kappa * batch;
     const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, 65535);
-    mac_small_kernel<E><<<blocks, 256, 0, st>>>(reinterpret_cast<const E*>(key->d_ahat_t), what, part,
+    mac_small_kernel<E><<<blocks, 256, 0, st>>>(reinterpret_cast<const E*>(key->d_ahat_t), key->a_m, what, part,
                                                 m, b_pad, n, splits, kappa, (uint32_t)batch, q);
   }
   rc = map_cuda(cudaGetLastError());
@@ -836,6 +721,7 @@ LC_API int lc_ajtai_key_create_ex(const lc_ntt_plan* plan, uint32_t k, uint32_t 
   if (!key) return LC_ERR_OUT_OF_MEMORY;
   key->k = k;
   key->m = m;
+  key->a_m = m;
   key->log_n = plan->log_n;
   key->n = 1u << plan->log_n;
   key->wide = plan->kind == PlanKind::Goldilocks;
@@ -901,13 +787,43 @@ LC_API int lc_ajtai_key_create_ex(const lc_ntt_plan* plan, uint32_t k, uint32_t 
 
 LC_API void lc_ajtai_key_destroy(lc_ajtai_key* key) {
   if (!key) return;
-  for (void* p : {key->d_ahat_t, key->d_what_t, key->d_partial, key->d_chat, key->d_wtmp, key->d_in,
+  if (key->owns_ahat && key->d_ahat_t) cudaFree(key->d_ahat_t);
+  for (void* p : {key->d_what_t, key->d_partial, key->d_chat, key->d_wtmp, key->d_in,
                   key->d_out, (void*)key->d_err})
     if (p) cudaFree(p);
   if (key->host_stream) cudaStreamDestroy(key->host_stream);
   if (key->plan) lc_ntt_plan_destroy(key->plan);
   tc_tables_destroy(key->tc);
   delete key;
+}
+
+LC_API int lc_ajtai_key_view(const lc_ajtai_key* parent, uint32_t k, uint32_t m, lc_ajtai_key** out) {
+  if (!parent || !out || k == 0 || m == 0 || k > parent->k || m > parent->m) return LC_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  lc_ajtai_key* key = new (std::nothrow) lc_ajtai_key();
+  if (!key) return LC_ERR_OUT_OF_MEMORY;
+  key->k = k;
+  key->m = m;
+  key->a_m = parent->a_m;
+  key->log_n = parent->log_n;
+  key->n = parent->n;
+  key->wide = parent->wide;
+  key->d_ahat_t = parent->d_ahat_t;
+  key->owns_ahat = false;
+  const lc_ntt_plan* pp = parent->plan;
+  int rc = key->wide ? lc_ntt_plan_create_goldilocks(pp->log_n, &key->plan)
+                     : lc_ntt_plan_create_u32(pp->log_n, pp->q, pp->two_adicity, pp->generator, 1, &key->plan);
+  if (!rc && cudaMalloc(&key->d_err, 4) != cudaSuccess) {
+    cudaGetLastError();
+    rc = LC_ERR_OUT_OF_MEMORY;
+  }
+  if (!rc) rc = map_cuda(cudaMemset(key->d_err, 0, 4));
+  if (rc) {
+    lc_ajtai_key_destroy(key);
+    return rc;
+  }
+  *out = key;
+  return LC_OK;
 }
 
 LC_API int lc_ajtai_key_set_engine(lc_ajtai_key* key, int engine) {

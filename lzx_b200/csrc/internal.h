@@ -74,6 +74,34 @@ struct lc_ntt_plan {
 
 struct lc_tc_tables;  // INT8 tensor-core commit tables (tc_commit.cu)
 
+// Ajtai key: cached NTT(A) transposed to [slot t][ring element j][row i padded
+// to 16], plus the scratch a commit grows on demand (commit.cu).
+struct lc_ajtai_key {
+  lc_ntt_plan* plan = nullptr;  // owned copy of the ring's plan
+  uint32_t k = 0, m = 0, n = 0, log_n = 0;
+  bool wide = false;           // Goldilocks (u64) or u32
+  void* d_ahat_t = nullptr;    // [n][a_m][16]
+  uint32_t a_m = 0;            // ring elements per NTT slot of d_ahat_t (m, or the parent's m for a view)
+  bool owns_ahat = true;       // false for a view (lc_ajtai_key_view)
+  // scratch, grown on demand
+  void* d_what_t = nullptr;
+  size_t what_bytes = 0;
+  void* d_partial = nullptr;
+  size_t partial_bytes = 0;
+  void* d_chat = nullptr;
+  size_t chat_bytes = 0;
+  void* d_wtmp = nullptr;  // generic witness path: converted + transformed witnesses
+  size_t wtmp_bytes = 0;
+  void* d_in = nullptr;  // host-API staging
+  size_t in_bytes = 0;
+  void* d_out = nullptr;
+  size_t out_bytes = 0;
+  cudaStream_t host_stream = nullptr;
+  uint32_t* d_err = nullptr;
+  lc_tc_tables* tc = nullptr;  // tensor-core engine tables (LC_KEY_TENSOR_I8)
+  int engine = LC_ENGINE_NTT;
+};
+
 namespace lc {
 int device_sm_count();
 int map_cuda(cudaError_t e);
