@@ -61,11 +61,15 @@ def parse():
     ap.add_argument("--no-commit", action="store_true", help="skip the Ajtai commit measurement")
     ap.add_argument("--commit-only", action="store_true",
                     help="run only the commit measurement (1 GPU) and print its JSON object")
-    ap.add_argument("--only", choices=["commit", "fold", "single"], default=None,
+    ap.add_argument("--only", choices=["commit", "fold", "single", "uneven"], default=None,
                     help="run only one secondary measurement (1 GPU) and print its JSON object")
     ap.add_argument("--no-fold", action="store_true", help="skip the folding-step measurement")
     ap.add_argument("--fold-m", type=int, default=1 << 20, help="ring elements of the folding-step witness")
     ap.add_argument("--fold-steps", type=int, default=5)
+    ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch measurement")
+    ap.add_argument("--uneven-jobs", type=int, default=512)
+    ap.add_argument("--uneven-log-nmax", type=int, default=18, help="jobs' n is log-uniform in [2^10, 2^this]")
+    ap.add_argument("--uneven-steps", type=int, default=3)
     ap.add_argument("--commit-steps", type=int, default=5)
     ap.add_argument("--commit-m", type=int, default=1 << 16,
                     help="witness ring elements per commitment (profiling runs use fewer)")
@@ -395,6 +399,172 @@ def bench_fold(args, rank, max_over_ranks, barrier, world):
     return res
 
 
+# ------------------------------------------------------------------ uneven batch of commit jobs
+
+U_WORKLOAD = ("uneven commit jobs: d in {64,128,256}, n log-uniform in [2^10, 2^LOG], kappa in {8,16}, "
+              "Goldilocks or the 4-prime 30-bit CRT set, int8 witness digits; one batch (3 persistent "
+              "work-queue launches, CUDA graph, autotuned) vs the same jobs one commit call at a time")
+
+
+def bench_uneven(args, rank, max_over_ranks, barrier, world):
+    """Total committed ring elements/s (sum of n over the jobs)."""
+    import numpy as np
+    import torch
+
+    from lzx_b200 import CRT_SET_30BIT, GoldilocksAjtaiKey, synth, tune
+    from lzx_b200.batch import CommitBatch, CommitJob, U32AjtaiKey, key_view
+    rng = np.random.default_rng(2024 + rank)
+    nj, lmax = args.uneven_jobs, args.uneven_log_nmax
+    m = 1 << lmax
+    # classes: (log_d, Goldilocks?) with one kappa=16, m=2^lmax key (or one per CRT prime)
+    specs = [(ld, gl) for gl in (True, False) for ld in (6, 7, 8)]
+    classes = []
+    for ci, (ld, gl) in enumerate(specs):
+        d = 1 << ld
+        if gl:
+            A = torch.empty(16 * m * d, dtype=torch.int64, device="cuda")
+            synth.fill_device(A, "gl", 300 + ci, 0)
+            classes.append([GoldilocksAjtaiKey(ld, 16, m, A)])
+        else:
+            keys = []
+            A = torch.empty(16 * m * d, dtype=torch.int32, device="cuda")
+            for pi, mod in enumerate(CRT_SET_30BIT):
+                synth.fill_device(A, "mod32", 300 + ci, pi, q=mod.q)
+                keys.append(U32AjtaiKey(mod, ld, 16, m, A))
+            classes.append(keys)
+        del A
+    # jobs: witnesses in one device buffer, outputs in one buffer per element type
+    cls_of = rng.integers(len(specs), size=nj)
+    ns = np.floor(2.0 ** (10 + (lmax - 10) * rng.random(nj))).astype(np.int64)
+    kappas = rng.choice([8, 16], size=nj)
+    wofs, gofs, uofs, wtot, gtot, utot = [], [], [], 0, 0, 0
+    for c, n, k in zip(cls_of, ns, kappas):
+        ld, gl = specs[c]
+        wofs.append(wtot)
+        wtot += ((int(n) << ld) + 15) // 16 * 16  # 16-byte aligned witnesses
+        if gl:
+            gofs.append(gtot)
+            uofs.append(None)
+            gtot += int(k) << ld
+        else:
+            gofs.append(None)
+            uofs.append(utot)
+            utot += (4 * int(k)) << ld
+    W = torch.empty(wtot, dtype=torch.int8, device="cuda")
+    synth.fill_device(W, "i8", 400 + rank, 0)
+    OG = torch.empty(max(gtot, 1), dtype=torch.int64, device="cuda")
+    OU = torch.empty(max(utot, 1), dtype=torch.int32, device="cuda")
+    jobs = []
+    for i in range(nj):
+        ld, gl = specs[cls_of[i]]
+        d, n, k = 1 << ld, int(ns[i]), int(kappas[i])
+        w = W[wofs[i]:wofs[i] + n * d].view(n, d)
+        out = (OG[gofs[i]:gofs[i] + k * d].view(1, k, d) if gl
+               else OU[uofs[i]:uofs[i] + 4 * k * d].view(4, k, d))
+        jobs.append(CommitJob(int(cls_of[i]), k, n, w, out))
+    total_elems = int(ns.sum())
+    res = {"workload": U_WORKLOAD.replace("LOG", str(lmax)), "jobs": nj, "sum_n": total_elems,
+           "unit": "committed ring-elems/s"}
+
+    # ---- one by one: a key view per job and key, warmed (scratch allocated) before timing
+    ref_g, ref_u = torch.empty_like(OG), torch.empty_like(OU)
+    views = []
+    for i, j in enumerate(jobs):
+        size = j.out.numel()
+        ro = (ref_g[gofs[i]:gofs[i] + size] if gofs[i] is not None else ref_u[uofs[i]:uofs[i] + size])
+        views.append(([key_view(key, j.kappa, j.n) for key in classes[j.cls]], ro.view(j.out.shape)))
+
+    def one_by_one():
+        for j, (vs, ro) in zip(jobs, views):
+            for ki, v in enumerate(vs):
+                v.commit_i8(j.w, ro[ki])
+    one_by_one()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    a.record()
+    one_by_one()
+    b.record()
+    torch.cuda.synchronize()
+    obo_ms = max_over_ranks(a.elapsed_time(b))
+    calls = sum(len(vs) for vs, _ in views)
+    del views
+    res["one_by_one"] = {"ms": obo_ms, "value": world * total_elems / (obo_ms / 1e3), "commit_calls": calls}
+
+    # ---- the batch: autotuned, graph-captured
+    batch = CommitBatch(classes, jobs, graph=True)
+    best, timings = tune.tune_batch(batch)
+    K = max(1, args.uneven_steps)
+    batch.run()
+    torch.cuda.synchronize()
+    barrier()
+    a.record()
+    for _ in range(K):
+        batch.run()
+    b.record()
+    torch.cuda.synchronize()
+    batch.check()
+    ms = max_over_ranks(a.elapsed_time(b) / K)
+    exact = bool(torch.equal(OG, ref_g) and torch.equal(OU, ref_u))
+    res["batch"] = {"ms": ms, "value": world * total_elems / (ms / 1e3), "steps": K,
+                    "config": {"chunk": best[0], "ctas_per_sm": best[1], "claim": best[2]},
+                    "tuning_ms": timings, "items": batch.info, "bit_exact_vs_one_by_one": exact}
+    res["speedup_batch_vs_one_by_one"] = obo_ms / ms
+    # ---- end to end: witnesses in from pinned host memory, commitments out
+    hw = torch.empty(wtot, dtype=torch.int8).pin_memory()
+    hw.copy_(W.cpu())
+    hg = torch.empty_like(OG, device="cpu").pin_memory()
+    hu = torch.empty_like(OU, device="cpu").pin_memory()
+    KE = 2
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(KE):
+        W.copy_(hw, non_blocking=True)
+        batch.run()
+        hg.copy_(OG, non_blocking=True)
+        hu.copy_(OU, non_blocking=True)
+        torch.cuda.synchronize()
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / KE)
+    res["batch"]["e2e"] = {"value": world * total_elems / e2e_s, "unit": "committed ring-elems/s",
+                           "h2d_bytes_per_step": wtot, "d2h_bytes_per_step": OG.numel() * 8 + OU.numel() * 4}
+    if not exact:
+        raise RuntimeError("batch outputs differ from the one-by-one commits")
+    del batch
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracle
+        oracle.prefer_native(True)
+        nt = host_threads()
+        sample = [i for i in range(nj) if ns[i] <= 8192][:12]
+        t_cpu, elems = 0.0, 0
+        for i in sample:
+            ld, gl = specs[cls_of[i]]
+            d, n, k = 1 << ld, int(ns[i]), int(kappas[i])
+            wv = jobs[i].w.cpu().numpy()
+            if gl:
+                a_h = synth.synth_gl(7, i, k * n * d)
+                t = oracle.NttTablesGl(ld)
+                a_ntt = t.forward_batch(a_h, nthreads=nt)
+                t0 = time.perf_counter()
+                oracle.ajtaigl_commit_batch(t, a_ntt, k, n, wv.reshape(1, n, d), nthreads=nt, simd=True,
+                                            native=True)
+                t_cpu += time.perf_counter() - t0
+            else:
+                for pi, mod in enumerate(oracle.CRT_PRIMES):
+                    t = oracle.NttTables32(oracle.Modulus32(*mod), ld)
+                    a_h = synth.synth_mod32(7, i * 4 + pi, mod[0], k * n * d)
+                    a_ntt = t.forward_batch(a_h.reshape(-1, d), nthreads=nt)
+                    s_res = np.where(wv < 0, mod[0] - np.abs(wv.astype(np.int64)), wv).astype(np.uint32)
+                    t0 = time.perf_counter()
+                    oracle.ajtai32_commit(t, a_ntt, k, n, s_res)
+                    t_cpu += time.perf_counter() - t0
+            elems += n
+        res["cpu_baseline"] = {"value": elems / t_cpu, "unit": "committed ring-elems/s", "cores": nt,
+                               "kind": "port",
+                               "sample": f"{len(sample)} of the jobs with n <= 8192 (oracle cached-NTT commit "
+                                         f"per job; Goldilocks MAC on {nt} threads, u32 commits 1 thread)"}
+    return res
+
+
 # ------------------------------------------------------------------ single commitment latency
 
 S_KAPPA, S_M = 8, 256
@@ -569,6 +739,7 @@ def run_ours(args):
 
     commit = None if args.no_commit else bench_commit(args, rank, max_over_ranks, barrier, world)
     fold = None if args.no_fold else bench_fold(args, rank, max_over_ranks, barrier, world)
+    uneven = None if args.no_uneven else bench_uneven(args, rank, max_over_ranks, barrier, world)
     single = bench_single(args, rank, max_over_ranks, barrier, world)
 
     if dist is not None:
@@ -626,6 +797,7 @@ def run_ours(args):
         "clocks": clocks,
         "commit": commit,
         "fold": fold,
+        "uneven_batch": uneven,
         "single_commit": single,
     }
     print(json.dumps(line), flush=True)
@@ -635,7 +807,7 @@ def run_ours(args):
 def run_only(args, which):
     import torch
     torch.cuda.set_device(0)
-    fn = {"commit": bench_commit, "fold": bench_fold, "single": bench_single}[which]
+    fn = {"commit": bench_commit, "fold": bench_fold, "single": bench_single, "uneven": bench_uneven}[which]
     res = fn(args, 0, lambda x: x, lambda: None, 1)
     print(json.dumps(res), flush=True)
     return 0

@@ -10,9 +10,11 @@
 // R[j] = sum over j' < j of the number of jobs longer than j', S = sum n_b.
 //   1. witness NTT: an item is PB consecutive staircase polynomials; their
 //      (j, b) come from a per-item start table and a short walk over R;
-//   2. product: an item is (slot t, chunk of ring elements); each thread holds
-//      2 rows x 4 jobs (160-bit accumulators) and streams the key's rows
-//      Ahat[t][j][0..16) -- read once per lane, not once per job;
+//   2. product: an item is (chunk of ring elements, 1..8 slots t sized to the
+//      jobs active in the chunk); TMA bulk copies stream the key's rows
+//      Ahat[t][j][0..16) -- read once per lane, not once per job -- and the
+//      staircase rows through shared memory; each thread holds 2 rows x 4 jobs
+//      (160-bit accumulators);
 //   3. finish: an item is one job: the sum over its chunks (mod q), then the
 //      inverse NTT of its kappa rows straight into the job's output.
 // A CTA claims `claim` items at a time from the phase's counter
@@ -72,6 +74,8 @@ struct LaneDesc {
   uint32_t pb;             // polynomials per witness item
   void* what;              // [d][S]
   void* partial;           // [nchunks][d][16][nb]
+  const uint64_t* citem;   // [nchunks + 1]: first product item of each chunk (lane-relative)
+  const uint8_t* ctg;      // [nchunks]: slots per product item of each chunk
   uint64_t item0[3];       // first item of the lane in each launch
 };
 
@@ -101,7 +105,7 @@ struct BCfg {
   static constexpr int SS = BatchSlotStride<A, LOG_N>::value;
   static constexpr int TWE = G::fwd_entries() > G::inv_entries() ? G::fwd_entries() : G::inv_entries();
   static constexpr size_t TWB = ((size_t)TWE * sizeof(Tw) + 15) / 16 * 16;
-  static constexpr size_t SMEM1 = TWB + (size_t)PB * SS * sizeof(T) + (size_t)PB * 8;
+  static constexpr size_t SMEM1 = TWB + (size_t)PB * SS * sizeof(T) + (size_t)PB * 8 + (size_t)(PB + 2) * 8;
   static constexpr size_t SMEM3 = TWB + (size_t)16 * SS * sizeof(T);
   static_assert(SS >= Slots<A, LOG_N, LOG_V>::S, "slot stride");
 };
@@ -134,18 +138,27 @@ LC_D void witness_item(const LaneDesc& L, const SubJob* __restrict__ subs, uint6
   T* slots = reinterpret_cast<T*>(smem + C::TWB);
   uint32_t* sj = reinterpret_cast<uint32_t*>(slots + PB * SS);
   uint32_t* sb = sj + PB;
+  uint64_t* sR = reinterpret_cast<uint64_t*>(sb + PB);  // R[j_lo .. j_lo + PB + 1]
+  __shared__ uint32_t s_jlo;
   const int tid = threadIdx.x;
   const uint64_t p0 = k * PB;
   for (int i = tid; i < Geo<LOG_N, LOG_V>::fwd_entries(); i += kBatchThreads)
     tw[i] = reinterpret_cast<const Tw*>(L.tw_fwd)[i];
+  if (tid == 0) s_jlo = L.item_j[k];
+  __syncthreads();
+  // consecutive staircase polynomials advance the ring element by at most one,
+  // so the item's PB polynomials lie in ring elements j_lo .. j_lo + PB - 1
+  const uint32_t jlo = s_jlo;
+  if (tid < PB + 2) sR[tid] = jlo + tid <= L.n_max ? L.R[jlo + tid] : L.S;
+  __syncthreads();
   if (tid < PB) {
     const uint64_t p = p0 + tid;
     uint32_t jr = 0xFFFFFFFFu, br = 0;
     if (p < L.S) {
-      uint32_t j = L.item_j[k];
-      while (L.R[j + 1] <= p) ++j;
-      jr = j;
-      br = (uint32_t)(p - L.R[j]);
+      uint32_t x = 0;
+      while (sR[x + 1] <= p) ++x;
+      jr = jlo + x;
+      br = (uint32_t)(p - sR[x]);
     }
     sj[tid] = jr;
     sb[tid] = br;
@@ -179,36 +192,158 @@ LC_D void witness_item(const LaneDesc& L, const SubJob* __restrict__ subs, uint6
   __syncthreads();
 }
 
-// ---- launch 2: products of one (slot, chunk)
+// ---- launch 2: products of one item = (chunk c of ring elements, tg slots t)
+//
+// The planner sizes items to the staircase: with cnt jobs active at the
+// chunk's first ring element, a 16-job block per warp needs ceil(cnt/16)
+// warps per slot, rounded up to 1, 2, 4 or 8; the CTA's 8 warps then take
+// tg = 8 / that many slots at once, so sparse chunks (few long jobs) still
+// keep every warp busy.  Blocks of kPJB/tg ring elements stream through a
+// kPStages-deep shared-memory ring by TMA bulk copies issued by thread 0:
+// per slot the key rows Ahat[t][jb..je) and the witness values
+// what[t*S + R[jb] .. t*S + R[je]) (both contiguous; the witness range and
+// the shared staircase slice R[jb..je] start at the 16-byte boundary below
+// them, `head` elements early).  Threads multiply out of shared memory,
+// 2 rows x 4 jobs each.
+constexpr int kPJB = 32;
+constexpr int kPStages = 3;
+constexpr int kPMaxT = 8;
+
 template <class E>
-LC_D void product_item(const LaneDesc& L, const SubJob* __restrict__ subs, uint32_t chunk, uint64_t k) {
+struct PStage {
+  static constexpr size_t A_BYTES = (size_t)kPJB * kIPad * sizeof(E);
+  static constexpr size_t R_BYTES = ((size_t)(kPJB + 1) * 8 + 16 + 15) / 16 * 16;
+  // one slot's witness values: (kPJB/tg) rows of at most 128/tg jobs, plus the head
+  LC_HD static constexpr size_t w_slot(uint32_t tg) {
+    return (((size_t)(kPJB / tg) * (kLaneJobs / tg)) * sizeof(E) + 16 + 15) / 16 * 16;
+  }
+  static constexpr size_t W_BYTES = w_slot(1);  // tg * w_slot(tg) is largest at tg = 1
+  static constexpr size_t BYTES = A_BYTES + R_BYTES + W_BYTES;
+};
+constexpr size_t kPStageBytes = PStage<uint64_t>::BYTES;  // the larger element type sizes the ring
+constexpr size_t kProductSmem = kPStages * kPStageBytes;
+static_assert(PStage<uint64_t>::w_slot(2) * 2 <= PStage<uint64_t>::W_BYTES &&
+                  PStage<uint64_t>::w_slot(4) * 4 <= PStage<uint64_t>::W_BYTES &&
+                  PStage<uint64_t>::w_slot(8) * 8 <= PStage<uint64_t>::W_BYTES,
+              "witness slots fit");
+
+struct ProductPipe {
+  uint64_t* bar;    // [kPStages]
+  uint32_t* head;   // [kPStages][1 + kPMaxT]: R head, then each slot's witness head
+  uint32_t issued;  // blocks issued (thread 0) / consumed (all threads) by this CTA so far
+  uint32_t consumed;
+};
+
+template <class E>
+LC_D void product_issue(const LaneDesc& L, uint32_t t0, uint32_t tg, uint32_t jb, uint32_t je,
+                        unsigned char* smem, ProductPipe& pp) {
+  const int st = pp.issued % kPStages;
+  unsigned char* base = smem + st * kPStageBytes;
+  const uint32_t rows_cap = kPJB / tg;
+  const size_t a_bytes = (size_t)(je - jb) * kIPad * sizeof(E);
+  const uintptr_t raddr = reinterpret_cast<uintptr_t>(L.R + jb);
+  const uint32_t rhead = (uint32_t)((raddr & 15) / 8);
+  const size_t r_bytes = (((size_t)(je + 1 - jb) + rhead) * 8 + 15) / 16 * 16;
+  const uint64_t w_lo = L.R[jb], w_hi = L.R[je];
+  const size_t wslot = PStage<E>::w_slot(tg);
+  uint32_t* head = pp.head + st * (1 + kPMaxT);
+  head[0] = rhead;
+  size_t total = r_bytes;
+  for (uint32_t ts = 0; ts < tg; ++ts) {
+    const E* wsrc = reinterpret_cast<const E*>(L.what) + (size_t)(t0 + ts) * L.S + w_lo;
+    const uint32_t whead = (uint32_t)((reinterpret_cast<uintptr_t>(wsrc) & 15) / sizeof(E));
+    head[1 + ts] = whead;
+    total += a_bytes + (((size_t)(w_hi - w_lo) + whead) * sizeof(E) + 15) / 16 * 16;
+  }
+  mbar_arrive_expect_tx(&pp.bar[st], (uint32_t)total);
+  bulk_g2s(base + PStage<E>::A_BYTES, reinterpret_cast<const void*>(raddr - rhead * 8), (uint32_t)r_bytes,
+           &pp.bar[st]);
+  for (uint32_t ts = 0; ts < tg; ++ts) {
+    const uint32_t t = t0 + ts;
+    const E* asrc = reinterpret_cast<const E*>(L.ahat) + ((size_t)t * L.a_m + jb) * kIPad;
+    bulk_g2s(base + (size_t)ts * rows_cap * kIPad * sizeof(E), asrc, (uint32_t)a_bytes, &pp.bar[st]);
+    const uint32_t whead = head[1 + ts];
+    const E* wsrc = reinterpret_cast<const E*>(L.what) + (size_t)t * L.S + w_lo;
+    const size_t w_bytes = (((size_t)(w_hi - w_lo) + whead) * sizeof(E) + 15) / 16 * 16;
+    bulk_g2s(base + PStage<E>::A_BYTES + PStage<E>::R_BYTES + ts * wslot, wsrc - whead, (uint32_t)w_bytes,
+             &pp.bar[st]);
+  }
+  ++pp.issued;
+}
+
+// false when a wait timed out (the error is recorded; copies in flight were waited for)
+template <class E>
+LC_D bool product_item(const LaneDesc& L, const SubJob* __restrict__ subs, uint32_t chunk, uint64_t k,
+                       unsigned char* smem, ProductPipe& pp, uint32_t* err) {
   const uint32_t d = 1u << L.log_n;
-  const uint32_t t = (uint32_t)(k % d), c = (uint32_t)(k / d);
+  // chunk of the item: citem[c] <= k < citem[c + 1]
+  uint32_t lo = 0, hi = L.nchunks;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) / 2;
+    if (L.citem[mid] <= k)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  const uint32_t c = lo, tg = L.ctg[c];
+  const uint32_t t0 = (uint32_t)(k - L.citem[c]) * tg;
   const uint32_t j0 = c * chunk, j1 = min(L.n_max, j0 + chunk);
+  const uint32_t rows_cap = kPJB / tg, wpt = kPMaxT / tg;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint32_t ip = lane & 7, bq = warp * 4 + (lane >> 3);  // rows 2ip, 2ip+1; jobs 4bq..4bq+3
+  const uint32_t ts = warp / wpt, jblk = warp % wpt;
+  const uint32_t t = t0 + ts;
+  const uint32_t ip = lane & 7, bq = jblk * 4 + (lane >> 3);  // rows 2ip, 2ip+1; jobs 4bq..4bq+3
   uint32_t nq[4];
 #pragma unroll
   for (int u = 0; u < 4; ++u) {
     const uint32_t b = 4 * bq + u;
     nq[u] = b < L.nb ? subs[L.sub0 + b].n : 0;  // sorted: nq[0] >= nq[1] >= ...
   }
+  const uint32_t nblk = j1 > j0 ? (j1 - j0 + rows_cap - 1) / rows_cap : 0;
+  if (threadIdx.x == 0)
+    for (uint32_t kb = 0; kb < min(nblk, (uint32_t)kPStages); ++kb)
+      product_issue<E>(L, t0, tg, j0 + kb * rows_cap, min(j1, j0 + (kb + 1) * rows_cap), smem, pp);
   Acc160 acc[2][4];
-  const E* A = reinterpret_cast<const E*>(L.ahat) + ((size_t)t * L.a_m) * kIPad + 2 * ip;
-  const E* W = reinterpret_cast<const E*>(L.what) + (size_t)t * L.S + 4 * bq;
-  const uint32_t jend = min(j1, nq[0]);
-#pragma unroll 2
-  for (uint32_t j = j0; j < jend; ++j) {
-    const E a0 = A[(size_t)j * kIPad], a1 = A[(size_t)j * kIPad + 1];
-    const uint64_t r0 = L.R[j];
-    E wv[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) wv[u] = j < nq[u] ? W[r0 + u] : E(0);
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      mac<E>(acc[0][u], a0, wv[u]);
-      mac<E>(acc[1][u], a1, wv[u]);
+  const size_t wslot = PStage<E>::w_slot(tg);
+  for (uint32_t kb = 0; kb < nblk; ++kb) {
+    const int st = pp.consumed % kPStages;
+    const bool ok = mbar_wait(&pp.bar[st], (pp.consumed / kPStages) & 1);
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) {
+        record_error(err, LC_DEVERR_TIMEOUT);
+        for (uint32_t q = pp.consumed + 1; q < pp.issued; ++q)  // later blocks may still be landing
+          mbar_wait(&pp.bar[q % kPStages], (q / kPStages) & 1);
+      }
+      return false;
     }
+    ++pp.consumed;
+    const unsigned char* base = smem + st * kPStageBytes;
+    const uint32_t* head = pp.head + st * (1 + kPMaxT);
+    const E* sA = reinterpret_cast<const E*>(base) + (size_t)ts * rows_cap * kIPad;
+    const uint64_t* sR = reinterpret_cast<const uint64_t*>(base + PStage<E>::A_BYTES) + head[0];
+    const E* sW = reinterpret_cast<const E*>(base + PStage<E>::A_BYTES + PStage<E>::R_BYTES + ts * wslot) +
+                  head[1 + ts];
+    const uint32_t jb = j0 + kb * rows_cap;
+    const uint32_t rows = min(rows_cap, j1 - jb);
+    const uint64_t w0 = sR[0];
+    const uint32_t jq = nq[0] > jb ? min(rows, nq[0] - jb) : 0;  // rows where this quad has work
+    for (uint32_t jj = 0; jj < jq; ++jj) {
+      const uint32_t j = jb + jj;
+      const uint32_t r = (uint32_t)(sR[jj] - w0);
+      const E a0 = sA[jj * kIPad + 2 * ip], a1 = sA[jj * kIPad + 2 * ip + 1];
+      E wv[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) wv[u] = j < nq[u] ? sW[r + 4 * bq + u] : E(0);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        mac<E>(acc[0][u], a0, wv[u]);
+        mac<E>(acc[1][u], a1, wv[u]);
+      }
+    }
+    __syncthreads();  // the stage is free again
+    if (threadIdx.x == 0 && kb + kPStages < nblk)
+      product_issue<E>(L, t0, tg, j0 + (kb + kPStages) * rows_cap, min(j1, j0 + (kb + kPStages + 1) * rows_cap),
+                       smem, pp);
   }
   // jobs active at j0 own a partial of this chunk (the finish launch reads
   // chunks c with c*chunk < n_b)
@@ -218,6 +353,7 @@ LC_D void product_item(const LaneDesc& L, const SubJob* __restrict__ subs, uint3
 #pragma unroll
     for (int u = 0; u < 4; ++u)
       if (j0 < nq[u]) P[(size_t)(2 * ip + ii) * L.nb + 4 * bq + u] = acc_reduce<E>(acc[ii][u], L.q);
+  return true;
 }
 
 // ---- launch 3: one job's chunk sums and inverse NTT
@@ -258,13 +394,6 @@ template <int PHASE>
 LC_D void run_item(const BatchParams& p, const LaneDesc& L, uint64_t k, unsigned char* smem) {
   const int key = (int)L.kind * 16 + (int)L.log_n;
   constexpr int GL = (int)PlanKind::Goldilocks * 16, SL = (int)PlanKind::U32Lazy * 16, MC = (int)PlanKind::U32Mont * 16;
-  if (PHASE == 1) {
-    if (L.kind == (uint32_t)PlanKind::Goldilocks)
-      product_item<uint64_t>(L, p.subs, p.chunk, k);
-    else
-      product_item<uint32_t>(L, p.subs, p.chunk, k);
-    return;
-  }
 #define LC_BATCH_CASE(K, A, LN, LV)                       \
   case K + LN:                                            \
     if (PHASE == 0)                                       \
@@ -290,7 +419,7 @@ LC_D void run_item(const BatchParams& p, const LaneDesc& L, uint64_t k, unsigned
 
 template <int PHASE>
 __global__ void __launch_bounds__(kBatchThreads) batch_kernel(const __grid_constant__ BatchParams p) {
-  extern __shared__ __align__(16) unsigned char smem[];
+  extern __shared__ __align__(128) unsigned char smem[];
   __shared__ unsigned long long s_base;
   const uint64_t total = p.total[PHASE];
   uint32_t lane = 0;
@@ -305,6 +434,38 @@ __global__ void __launch_bounds__(kBatchThreads) batch_kernel(const __grid_const
       // claims only grow, so the lane index only moves forward
       while (lane + 1 < p.nlanes && p.lanes[lane + 1].item0[PHASE] <= it) ++lane;
       run_item<PHASE>(p, p.lanes[lane], it - p.lanes[lane].item0[PHASE], smem);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kBatchThreads) product_kernel(const __grid_constant__ BatchParams p) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ unsigned long long s_base;
+  __shared__ __align__(8) uint64_t bars[kPStages];
+  __shared__ uint32_t heads[kPStages * (1 + kPMaxT)];
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kPStages; ++i) mbar_init(&bars[i], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  ProductPipe pp{bars, heads, 0, 0};
+  const uint64_t total = p.total[1];
+  uint32_t lane = 0;
+  for (;;) {
+    if (threadIdx.x == 0) s_base = atomicAdd(&p.counters[1], (unsigned long long)p.claim);
+    __syncthreads();
+    const uint64_t base = s_base;
+    __syncthreads();
+    if (base >= total) return;
+    const uint64_t end = min(base + p.claim, total);
+    for (uint64_t it = base; it < end; ++it) {
+      while (lane + 1 < p.nlanes && p.lanes[lane + 1].item0[1] <= it) ++lane;
+      const LaneDesc& L = p.lanes[lane];
+      const uint64_t k = it - L.item0[1];
+      const bool ok = L.kind == (uint32_t)PlanKind::Goldilocks
+                          ? product_item<uint64_t>(L, p.subs, p.chunk, k, smem, pp, p.err)
+                          : product_item<uint32_t>(L, p.subs, p.chunk, k, smem, pp, p.err);
+      if (!ok) return;  // every thread saw the same failure
     }
   }
 }
@@ -342,6 +503,9 @@ static bool lane_geometry(PlanKind kind, uint32_t log_n, size_t& s1, size_t& s3,
 
 struct lc_batch {
   std::vector<lc::LaneDesc> lanes;     // host copies (device pointers inside)
+  std::vector<std::vector<uint64_t>> R;  // staircase offsets per lane (host)
+  uint64_t* d_citem = nullptr;
+  uint8_t* d_ctg = nullptr;
   std::vector<uint64_t> lane_elem;     // element bytes per lane
   lc::LaneDesc* d_lanes = nullptr;
   lc::SubJob* d_subs = nullptr;
@@ -368,17 +532,57 @@ static void batch_free(lc_batch* b) {
   if (b->graph) cudaGraphDestroy(b->graph);
   if (b->cap) cudaStreamDestroy(b->cap);
   for (void* p : {(void*)b->d_lanes, (void*)b->d_subs, (void*)b->d_R, (void*)b->d_itemj, (void*)b->d_what,
-                  (void*)b->d_partial, (void*)b->d_counters, (void*)b->d_err})
+                  (void*)b->d_partial, (void*)b->d_counters, (void*)b->d_err, (void*)b->d_citem,
+                  (void*)b->d_ctg})
     if (p) cudaFree(p);
   delete b;
 }
 
 // chunk-dependent fields, item bases and the device copy of the lanes
 static int batch_layout(lc_batch* b) {
-  uint64_t base[3] = {0, 0, 0};
-  for (auto& L : b->lanes) {
+  // product items per chunk: slots per item from the jobs active at the chunk's start
+  std::vector<uint64_t> citem;
+  std::vector<uint8_t> ctg;
+  std::vector<size_t> coff;
+  for (size_t l = 0; l < b->lanes.size(); ++l) {
+    LaneDesc& L = b->lanes[l];
+    const std::vector<uint64_t>& R = b->R[l];
     L.nchunks = (L.n_max + b->chunk - 1) / b->chunk;
-    const uint64_t items[3] = {(L.S + L.pb - 1) / L.pb, (uint64_t)(1u << L.log_n) * L.nchunks, L.nb};
+    coff.push_back(citem.size());
+    const uint32_t d = 1u << L.log_n;
+    uint64_t acc = 0;
+    for (uint32_t c = 0; c < L.nchunks; ++c) {
+      const uint64_t j0 = (uint64_t)c * b->chunk;
+      const uint64_t cnt = R[j0 + 1] - R[j0];
+      uint32_t wpt = 1;
+      while (wpt * 16 < cnt) wpt *= 2;
+      const uint32_t tg = kPMaxT / wpt;
+      citem.push_back(acc);
+      ctg.push_back((uint8_t)tg);
+      acc += d / tg;
+    }
+    citem.push_back(acc);
+    ctg.push_back(0);
+  }
+  if (b->d_citem) cudaFree(b->d_citem);
+  if (b->d_ctg) cudaFree(b->d_ctg);
+  b->d_citem = nullptr;
+  b->d_ctg = nullptr;
+  if (cudaMalloc(&b->d_citem, std::max<size_t>(1, citem.size()) * 8) != cudaSuccess ||
+      cudaMalloc(&b->d_ctg, std::max<size_t>(1, ctg.size())) != cudaSuccess) {
+    cudaGetLastError();
+    return LC_ERR_OUT_OF_MEMORY;
+  }
+  if (!citem.empty()) {
+    cudaMemcpy(b->d_citem, citem.data(), citem.size() * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(b->d_ctg, ctg.data(), ctg.size(), cudaMemcpyHostToDevice);
+  }
+  uint64_t base[3] = {0, 0, 0};
+  for (size_t l = 0; l < b->lanes.size(); ++l) {
+    LaneDesc& L = b->lanes[l];
+    L.citem = b->d_citem + coff[l];
+    L.ctg = b->d_ctg + coff[l];
+    const uint64_t items[3] = {(L.S + L.pb - 1) / L.pb, citem[coff[l] + L.nchunks], L.nb};
     for (int ph = 0; ph < 3; ++ph) {
       L.item0[ph] = base[ph];
       base[ph] += items[ph];
@@ -393,7 +597,11 @@ static int batch_layout(lc_batch* b) {
 }
 
 static int batch_launch(lc_batch* b, cudaStream_t st) {
-  cudaError_t e = cudaMemsetAsync(b->d_counters, 0, 3 * sizeof(unsigned long long), st);
+  static_assert(kProductSmem <= 227 * 1024, "product ring");
+  cudaError_t e = cudaFuncSetAttribute(product_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kProductSmem);
+  if (e != cudaSuccess) return map_cuda(e);
+  e = cudaMemsetAsync(b->d_counters, 0, 3 * sizeof(unsigned long long), st);
   if (e != cudaSuccess) return map_cuda(e);
   BatchParams p{};
   p.lanes = b->d_lanes;
@@ -406,7 +614,7 @@ static int batch_launch(lc_batch* b, cudaStream_t st) {
   p.claim = b->claim;
   const unsigned grid = (unsigned)std::max(1, device_sm_count()) * b->ctas;
   batch_kernel<0><<<grid, kBatchThreads, b->smem[0], st>>>(p);
-  batch_kernel<1><<<grid, kBatchThreads, b->smem[1], st>>>(p);
+  product_kernel<<<grid, kBatchThreads, kProductSmem, st>>>(p);
   batch_kernel<2><<<grid, kBatchThreads, b->smem[2], st>>>(p);
   return map_cuda(cudaGetLastError());
 }
@@ -509,6 +717,7 @@ LC_API int lc_batch_create(const lc_commit_class* classes, uint32_t num_classes,
           itemj_all.push_back(j);
         }
         Rall.insert(Rall.end(), R.begin(), R.end());
+        b->R.push_back(std::move(R));
         what_off.push_back(what_bytes);
         what_bytes += ((size_t)d * L.S * eb + 255) / 256 * 256;
         part_off.push_back(partial_bytes);
@@ -521,9 +730,9 @@ LC_API int lc_batch_create(const lc_commit_class* classes, uint32_t num_classes,
   const size_t nl = std::max<size_t>(1, b->lanes.size());
   if (cudaMalloc(&b->d_lanes, nl * sizeof(LaneDesc)) != cudaSuccess ||
       cudaMalloc(&b->d_subs, std::max<size_t>(1, subs.size()) * sizeof(SubJob)) != cudaSuccess ||
-      cudaMalloc(&b->d_R, std::max<size_t>(1, Rall.size()) * 8) != cudaSuccess ||
+      cudaMalloc(&b->d_R, (Rall.size() + 2) * 8) != cudaSuccess ||  // + slack for 16-byte copy rounding
       cudaMalloc(&b->d_itemj, std::max<size_t>(1, itemj_all.size()) * 4) != cudaSuccess ||
-      cudaMalloc(&b->d_what, std::max<size_t>(256, what_bytes)) != cudaSuccess ||
+      cudaMalloc(&b->d_what, what_bytes + 256) != cudaSuccess ||  // + slack for 16-byte copy rounding
       cudaMalloc(&b->d_partial, std::max<size_t>(256, partial_bytes)) != cudaSuccess ||
       cudaMalloc(&b->d_counters, 3 * sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&b->d_err, 4) != cudaSuccess) {
@@ -631,7 +840,7 @@ LC_API int lc_batch_check(lc_batch* b, lc_stream stream) {
   if (cudaMemcpy(&flag, b->d_err, 4, cudaMemcpyDeviceToHost) != cudaSuccess) return map_cuda(cudaGetLastError());
   if (flag) {
     cudaMemset(b->d_err, 0, 4);
-    return LC_ERR_UNSUPPORTED;
+    return flag == LC_DEVERR_TIMEOUT ? LC_ERR_TIMEOUT : LC_ERR_UNSUPPORTED;
   }
   return LC_OK;
 }

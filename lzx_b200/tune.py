@@ -65,3 +65,43 @@ def tune_ntt(plan, count: int, reps: int = 10) -> int:
 def last_results(plan, count: int):
     key = (plan.n, plan.num_moduli, plan.elem_dtype.__name__, count)
     return _cache.get(key)
+
+
+# ------------------------------------------------------------------ commit batches
+
+BATCH_CHUNKS = (1024, 2048, 4096, 8192, 16384)
+BATCH_CTAS = (1, 2, 3, 4)
+BATCH_CLAIMS = (1, 4)
+
+
+def _time_batch(batch, reps: int) -> float:
+    import torch
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    batch.run()  # warm-up (and graph capture for a new configuration)
+    a.record()
+    for _ in range(reps):
+        batch.run()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def tune_batch(batch, reps: int = 2):
+    """Pick the product chunk, the CTAs per SM of the persistent launches and
+    the work items per claim for this batch: a coordinate search (chunk at
+    2 CTAs/SM, then CTAs/SM, then the claim size) timed with CUDA events.
+    Leaves the best configuration on ``batch``; returns (config, timings)."""
+    timings = {}
+
+    def t(cfg):
+        if cfg not in timings:
+            batch.set_config(*cfg)
+            timings[cfg] = _time_batch(batch, reps)
+        return timings[cfg]
+
+    best = min(((c, 2, 1) for c in BATCH_CHUNKS), key=t)
+    best = min(((best[0], n, 1) for n in BATCH_CTAS), key=t)
+    best = min(((best[0], best[1], k) for k in BATCH_CLAIMS), key=t)
+    batch.set_config(*best)
+    batch.check()
+    return best, {f"{c[0]}/{c[1]}/{c[2]}": ms for c, ms in timings.items()}
