@@ -737,9 +737,16 @@ def run_ours(args):
     assert torch.equal(hout, hin)
     e2e_value = world * TRANSFORMS_PER_STEP * COEFFS * KE / e2e_s
 
+    # secondary workloads; torch's cached blocks go back to the driver between them,
+    # since the library allocates its keys and scratch with cudaMalloc
+    del x, y, z
+    torch.cuda.empty_cache()
     commit = None if args.no_commit else bench_commit(args, rank, max_over_ranks, barrier, world)
+    torch.cuda.empty_cache()
     fold = None if args.no_fold else bench_fold(args, rank, max_over_ranks, barrier, world)
+    torch.cuda.empty_cache()
     uneven = None if args.no_uneven else bench_uneven(args, rank, max_over_ranks, barrier, world)
+    torch.cuda.empty_cache()
     single = bench_single(args, rank, max_over_ranks, barrier, world)
 
     if dist is not None:
