@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--uneven-jobs", type=int, default=512)
     ap.add_argument("--uneven-log-nmax", type=int, default=18, help="jobs' n is log-uniform in [2^10, 2^this]")
     ap.add_argument("--uneven-steps", type=int, default=3)
+    ap.add_argument("--uneven-profile", action="store_true",
+                    help="run only the batch, untuned and without the one-by-one arm (for profilers)")
     ap.add_argument("--commit-steps", type=int, default=5)
     ap.add_argument("--commit-m", type=int, default=1 << 16,
                     help="witness ring elements per commitment (profiling runs use fewer)")
@@ -465,6 +467,13 @@ def bench_uneven(args, rank, max_over_ranks, barrier, world):
     total_elems = int(ns.sum())
     res = {"workload": U_WORKLOAD.replace("LOG", str(lmax)), "jobs": nj, "sum_n": total_elems,
            "unit": "committed ring-elems/s"}
+    if args.uneven_profile:
+        batch = CommitBatch(classes, jobs, graph=False)
+        for _ in range(max(1, args.uneven_steps)):
+            batch.run()
+        batch.check()
+        res["profile_run"] = {"items": batch.info, "config": batch.config}
+        return res
 
     # ---- one by one: a key view per job and key, warmed (scratch allocated) before timing
     ref_g, ref_u = torch.empty_like(OG), torch.empty_like(OU)
