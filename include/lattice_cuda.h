@@ -126,7 +126,8 @@ typedef struct lc_ajtai_key lc_ajtai_key;
  * (entry (i,j) at (i*m + j)*n), residues of the plan's element type; host
  * memory, or device memory when matrix_on_device != 0.  Replaces the
  * cached-NTT part of AjtaiPublicKey::from_seed (ajtai.rs:91-96); the seed
- * expansion itself (uniform_from_seed, ring.rs:102-180) stays on the host. */
+ * expansion (uniform_from_seed, ring.rs:102-180) runs on the device in
+ * lc_ajtai_key_from_seed, or on the host before this call. */
 LC_API int lc_ajtai_key_create(const lc_ntt_plan *plan, uint32_t k, uint32_t m, const void *matrix,
                                int matrix_on_device, lc_ajtai_key **out);
 LC_API void lc_ajtai_key_destroy(lc_ajtai_key *key);
@@ -162,6 +163,23 @@ LC_API int lc_ajtai_key_check(lc_ajtai_key *key, lc_stream stream);
  * per shape; it lets callers with many commitment shapes share one resident
  * key.  The view owns its scratch; `parent` must outlive it; NTT engine only. */
 LC_API int lc_ajtai_key_view(const lc_ajtai_key *parent, uint32_t k, uint32_t m, lc_ajtai_key **out);
+
+/* RingConfig::uniform_from_seed (lattice-ring/src/ring.rs:102-180) on the
+ * device for `count` consecutive indices index0, index0+1, ...: out (device)
+ * = [count][n] residues of the plan's single u32 modulus, byte-identical to
+ * the reference (SHAKE256 via Transcript::xof, transcript.rs:229-237;
+ * rejection of windows >= 2^32 - 2^32 mod q).  The framed message
+ * (domain and seed plus 27 bytes) must fit 4 SHAKE blocks: domain_len +
+ * seed_len <= 516, else LC_ERR_INVALID_ARGUMENT. */
+LC_API int lc_uniform_from_seed(const lc_ntt_plan *plan, const uint8_t *domain, size_t domain_len,
+                                const uint8_t *seed, size_t seed_len, uint64_t index0, size_t count,
+                                uint32_t *out, lc_stream stream);
+
+/* AjtaiPublicKey::from_seed (lattice-commitment/src/ajtai.rs:87-103) on the
+ * device: A[i][j] = uniform_from_seed(b"ajtai-A", seed, i*m + j), then the
+ * cached NTT as lc_ajtai_key_create.  Synchronous. */
+LC_API int lc_ajtai_key_from_seed(const lc_ntt_plan *plan, uint32_t k, uint32_t m, const uint8_t seed[32],
+                                  lc_ajtai_key **out);
 
 /* Key creation flags. */
 #define LC_KEY_TENSOR_I8 1u /* also build the INT8 tensor-core commit tables */

@@ -94,6 +94,8 @@ def _declare(L):
         "lc_fold_pipeline_check": (i32, [P, P]),
         "lc_fold_pipeline_destroy": (None, [P]),
         "lc_ajtai_key_view": (i32, [P, u32, u32, C.POINTER(P)]),
+        "lc_uniform_from_seed": (i32, [P, P, sz, P, sz, C.c_uint64, sz, P, P]),
+        "lc_ajtai_key_from_seed": (i32, [P, u32, u32, P, C.POINTER(P)]),
         "lc_batch_create": (i32, [P, u32, P, u32, u32, C.POINTER(P)]),
         "lc_batch_set_config": (i32, [P, u32, u32, u32]),
         "lc_batch_get_config": (i32, [P, U32P, U32P, U32P]),

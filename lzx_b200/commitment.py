@@ -157,7 +157,22 @@ class AjtaiPublicKey:
 
     @classmethod
     def from_seed(cls, params: AjtaiParams, seed: bytes) -> "AjtaiPublicKey":
-        """Expand A[i][j] = uniform_from_seed(b"ajtai-A", seed, i*m + j) (ajtai.rs:87-103)."""
+        """Expand A[i][j] = uniform_from_seed(b"ajtai-A", seed, i*m + j) (ajtai.rs:87-103)
+        on the GPU (``lc_uniform_from_seed``); NTT(A) is cached from the device copy."""
+        if len(seed) != 32:
+            raise ValueError("seed must be 32 bytes")
+        import torch
+        dev = params.ring.uniform_from_seed_batch(b"ajtai-A", seed, 0, params.k * params.m)
+        key = cls.__new__(cls)
+        key.params, key.seed = params, bytes(seed)
+        key._dev = _DeviceKey(params.ring.tables, params.k, params.m, dev)
+        torch.cuda.synchronize()
+        key._matrix = dev.cpu().numpy().view(np.uint32)
+        return key
+
+    @classmethod
+    def from_seed_host(cls, params: AjtaiParams, seed: bytes) -> "AjtaiPublicKey":
+        """The same expansion element by element on the host (ring.rs:102-180)."""
         if len(seed) != 32:
             raise ValueError("seed must be 32 bytes")
         ring = params.ring

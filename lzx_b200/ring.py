@@ -287,6 +287,18 @@ class RingConfig:
             counter += 1
         return RingElement(self, np.array(coeffs, dtype=np.uint32))
 
+    def uniform_from_seed_batch(self, domain: bytes, seed: bytes, index0: int, count: int, out=None):
+        """``uniform_from_seed`` for indices index0 .. index0+count-1 on the GPU
+        (``lc_uniform_from_seed``): a CUDA int32 tensor [count][n] of the residues."""
+        import torch
+        n = self.n()
+        if out is None:
+            out = torch.empty((count, n), dtype=torch.int32, device="cuda")
+        st = _lib.lib().lc_uniform_from_seed(self.tables.handle, domain, len(domain), seed, len(seed), index0, count,
+                                             C.c_void_p(out.data_ptr()), _current_stream())
+        _raise_for(st, "lc_uniform_from_seed")
+        return out
+
 
 class RingElement:
     """``RingElement`` (ring.rs:183-447)."""
