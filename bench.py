@@ -61,7 +61,7 @@ def parse():
     ap.add_argument("--no-commit", action="store_true", help="skip the Ajtai commit measurement")
     ap.add_argument("--commit-only", action="store_true",
                     help="run only the commit measurement (1 GPU) and print its JSON object")
-    ap.add_argument("--only", choices=["commit", "fold", "single", "uneven"], default=None,
+    ap.add_argument("--only", choices=["commit", "fold", "single", "uneven", "keygen"], default=None,
                     help="run only one secondary measurement (1 GPU) and print its JSON object")
     ap.add_argument("--no-fold", action="store_true", help="skip the folding-step measurement")
     ap.add_argument("--fold-m", type=int, default=1 << 20, help="ring elements of the folding-step witness")
@@ -574,6 +574,58 @@ def bench_uneven(args, rank, max_over_ranks, barrier, world):
     return res
 
 
+# ------------------------------------------------------------------ seeded key derivation
+
+def bench_keygen(args, rank, max_over_ranks, barrier, world):
+    """AjtaiPublicKey::from_seed at the verifier's shape (Q_32, d=64, k=2,
+    m=500/2000/8000, seed [7; 32]): microseconds per matrix element, and the
+    device SHAKE256 expansion alone at 2^20 elements."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from lzx_b200 import Modulus32, RingConfig, _lib
+    L = _lib.lib()
+    ring = RingConfig(Modulus32.Q_32, 6)
+    seed = bytes([7]) * 32
+    res = {"workload": "AjtaiPublicKey::from_seed, Q_32, d=64, k=2 (verifier key regeneration)",
+           "unit": "us/element"}
+    for m in (500, 2000, 8000):
+        h = C.c_void_p()
+        _lib.check(L.lc_ajtai_key_from_seed(ring.tables.handle, 2, m, seed, C.byref(h)), "from_seed")
+        L.lc_ajtai_key_destroy(h)
+        t0 = time.perf_counter()
+        reps = 5
+        for _ in range(reps):
+            _lib.check(L.lc_ajtai_key_from_seed(ring.tables.handle, 2, m, seed, C.byref(h)), "from_seed")
+            L.lc_ajtai_key_destroy(h)
+        res[f"m{m}"] = {"us_per_element": (time.perf_counter() - t0) / reps * 1e6 / (2 * m),
+                        "api": "lc_ajtai_key_from_seed (synchronous: derivation, cached NTT, key set-up)"}
+    count = 1 << 20
+    out = torch.empty((count, 64), dtype=torch.int32, device="cuda")
+    ring.uniform_from_seed_batch(b"ajtai-A", seed, 0, count, out)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(3):
+        ring.uniform_from_seed_batch(b"ajtai-A", seed, 0, count, out)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / 3
+    res["device_expansion"] = {"elements": count, "ms": ms, "elements_per_s": count / (ms / 1e3)}
+    del out
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracle
+        t = oracle.NttTables32(oracle.Modulus32(*oracle.Q_32), 6)
+        t0 = time.perf_counter()
+        oracle.ajtai32_from_seed(t, 2, 2000, seed)
+        dt = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": dt * 1e6 / 4000, "unit": "us/element", "cores": 1, "kind": "port",
+                               "sample": "k=2, m=2000 (oracle restatement of from_seed: SHAKE256 expansion + "
+                                         "NTT per element), 1 thread"}
+    return res
+
+
 # ------------------------------------------------------------------ single commitment latency
 
 S_KAPPA, S_M = 8, 256
@@ -757,6 +809,7 @@ def run_ours(args):
     uneven = None if args.no_uneven else bench_uneven(args, rank, max_over_ranks, barrier, world)
     torch.cuda.empty_cache()
     single = bench_single(args, rank, max_over_ranks, barrier, world)
+    keygen = bench_keygen(args, rank, max_over_ranks, barrier, world)
 
     if dist is not None:
         dist.destroy_process_group()
@@ -814,6 +867,7 @@ def run_ours(args):
         "commit": commit,
         "fold": fold,
         "uneven_batch": uneven,
+        "key_from_seed": keygen,
         "single_commit": single,
     }
     print(json.dumps(line), flush=True)
@@ -823,7 +877,8 @@ def run_ours(args):
 def run_only(args, which):
     import torch
     torch.cuda.set_device(0)
-    fn = {"commit": bench_commit, "fold": bench_fold, "single": bench_single, "uneven": bench_uneven}[which]
+    fn = {"commit": bench_commit, "fold": bench_fold, "single": bench_single, "uneven": bench_uneven,
+          "keygen": bench_keygen}[which]
     res = fn(args, 0, lambda x: x, lambda: None, 1)
     print(json.dumps(res), flush=True)
     return 0

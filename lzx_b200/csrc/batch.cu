@@ -10,11 +10,10 @@
 // R[j] = sum over j' < j of the number of jobs longer than j', S = sum n_b.
 //   1. witness NTT: an item is PB consecutive staircase polynomials; their
 //      (j, b) come from a per-item start table and a short walk over R;
-//   2. product: an item is (chunk of ring elements, 1..8 slots t sized to the
-//      jobs active in the chunk); TMA bulk copies stream the key's rows
-//      Ahat[t][j][0..16) -- read once per lane, not once per job -- and the
-//      staircase rows through shared memory; each thread holds 2 rows x 4 jobs
-//      (160-bit accumulators);
+//   2. product: a warp's item is (chunk of ring elements, slot t, block of 16
+//      jobs active at the chunk's start); each thread holds 2 rows x 4 jobs
+//      (160-bit accumulators) and streams the key's rows Ahat[t][j][..] --
+//      read once per lane of jobs, not once per job -- and the staircase;
 //   3. finish: an item is one job: the sum over its chunks (mod q), then the
 //      inverse NTT of its kappa rows straight into the job's output.
 // A CTA claims `claim` items at a time from the phase's counter
@@ -75,7 +74,7 @@ struct LaneDesc {
   void* what;              // [d][S]
   void* partial;           // [nchunks][d][16][nb]
   const uint64_t* citem;   // [nchunks + 1]: first product item of each chunk (lane-relative)
-  const uint8_t* ctg;      // [nchunks]: slots per product item of each chunk
+  const uint8_t* cblk;     // [nchunks]: 16-job blocks with jobs active at the chunk's start
   uint64_t item0[3];       // first item of the lane in each launch
 };
 
@@ -192,90 +191,34 @@ LC_D void witness_item(const LaneDesc& L, const SubJob* __restrict__ subs, uint6
   __syncthreads();
 }
 
-// ---- launch 2: products of one item = (chunk c of ring elements, tg slots t)
+// ---- launch 2: products, one warp per item = (chunk c, slot t, block of 16 jobs)
 //
-// The planner sizes items to the staircase: with cnt jobs active at the
-// chunk's first ring element, a 16-job block per warp needs ceil(cnt/16)
-// warps per slot, rounded up to 1, 2, 4 or 8; the CTA's 8 warps then take
-// tg = 8 / that many slots at once, so sparse chunks (few long jobs) still
-// keep every warp busy.  Blocks of kPJB/tg ring elements stream through a
-// kPStages-deep shared-memory ring by TMA bulk copies issued by thread 0:
-// per slot the key rows Ahat[t][jb..je) and the witness values
-// what[t*S + R[jb] .. t*S + R[je]) (both contiguous; the witness range and
-// the shared staircase slice R[jb..je] start at the 16-byte boundary below
-// them, `head` elements early).  Threads multiply out of shared memory,
-// 2 rows x 4 jobs each.
-constexpr int kPJB = 32;
-constexpr int kPStages = 3;
-constexpr int kPMaxT = 8;
-
+// The planner lists, for every chunk of ring elements, the 16-job blocks with
+// jobs active at the chunk's first element (jobs are sorted longest first, so
+// the active jobs are a prefix) and one item per (slot t, block).  A warp
+// claims items from the launch's counter on its own -- no CTA-wide barrier,
+// so a warp whose jobs end early simply takes the next item.  Lane
+// (ip, g) holds rows 2ip, 2ip+1 of jobs 4(4*blk + g) .. +3 in 160-bit
+// accumulators and streams, two ring elements at a time (loads before the
+// multiply-adds), the key pair Ahat[t][j][2ip..2ip+1] and the witness values
+// what[t*S + R[j] + b] from L2.
 template <class E>
-struct PStage {
-  static constexpr size_t A_BYTES = (size_t)kPJB * kIPad * sizeof(E);
-  static constexpr size_t R_BYTES = ((size_t)(kPJB + 1) * 8 + 16 + 15) / 16 * 16;
-  // one slot's witness values: (kPJB/tg) rows of at most 128/tg jobs, plus the head
-  LC_HD static constexpr size_t w_slot(uint32_t tg) {
-    return (((size_t)(kPJB / tg) * (kLaneJobs / tg)) * sizeof(E) + 16 + 15) / 16 * 16;
-  }
-  static constexpr size_t W_BYTES = w_slot(1);  // tg * w_slot(tg) is largest at tg = 1
-  static constexpr size_t BYTES = A_BYTES + R_BYTES + W_BYTES;
-};
-constexpr size_t kPStageBytes = PStage<uint64_t>::BYTES;  // the larger element type sizes the ring
-constexpr size_t kProductSmem = kPStages * kPStageBytes;
-static_assert(PStage<uint64_t>::w_slot(2) * 2 <= PStage<uint64_t>::W_BYTES &&
-                  PStage<uint64_t>::w_slot(4) * 4 <= PStage<uint64_t>::W_BYTES &&
-                  PStage<uint64_t>::w_slot(8) * 8 <= PStage<uint64_t>::W_BYTES,
-              "witness slots fit");
-
-struct ProductPipe {
-  uint64_t* bar;    // [kPStages]
-  uint32_t* head;   // [kPStages][1 + kPMaxT]: R head, then each slot's witness head
-  uint32_t issued;  // blocks issued (thread 0) / consumed (all threads) by this CTA so far
-  uint32_t consumed;
-};
-
-template <class E>
-LC_D void product_issue(const LaneDesc& L, uint32_t t0, uint32_t tg, uint32_t jb, uint32_t je,
-                        unsigned char* smem, ProductPipe& pp) {
-  const int st = pp.issued % kPStages;
-  unsigned char* base = smem + st * kPStageBytes;
-  const uint32_t rows_cap = kPJB / tg;
-  const size_t a_bytes = (size_t)(je - jb) * kIPad * sizeof(E);
-  const uintptr_t raddr = reinterpret_cast<uintptr_t>(L.R + jb);
-  const uint32_t rhead = (uint32_t)((raddr & 15) / 8);
-  const size_t r_bytes = (((size_t)(je + 1 - jb) + rhead) * 8 + 15) / 16 * 16;
-  const uint64_t w_lo = L.R[jb], w_hi = L.R[je];
-  const size_t wslot = PStage<E>::w_slot(tg);
-  uint32_t* head = pp.head + st * (1 + kPMaxT);
-  head[0] = rhead;
-  size_t total = r_bytes;
-  for (uint32_t ts = 0; ts < tg; ++ts) {
-    const E* wsrc = reinterpret_cast<const E*>(L.what) + (size_t)(t0 + ts) * L.S + w_lo;
-    const uint32_t whead = (uint32_t)((reinterpret_cast<uintptr_t>(wsrc) & 15) / sizeof(E));
-    head[1 + ts] = whead;
-    total += a_bytes + (((size_t)(w_hi - w_lo) + whead) * sizeof(E) + 15) / 16 * 16;
-  }
-  mbar_arrive_expect_tx(&pp.bar[st], (uint32_t)total);
-  bulk_g2s(base + PStage<E>::A_BYTES, reinterpret_cast<const void*>(raddr - rhead * 8), (uint32_t)r_bytes,
-           &pp.bar[st]);
-  for (uint32_t ts = 0; ts < tg; ++ts) {
-    const uint32_t t = t0 + ts;
-    const E* asrc = reinterpret_cast<const E*>(L.ahat) + ((size_t)t * L.a_m + jb) * kIPad;
-    bulk_g2s(base + (size_t)ts * rows_cap * kIPad * sizeof(E), asrc, (uint32_t)a_bytes, &pp.bar[st]);
-    const uint32_t whead = head[1 + ts];
-    const E* wsrc = reinterpret_cast<const E*>(L.what) + (size_t)t * L.S + w_lo;
-    const size_t w_bytes = (((size_t)(w_hi - w_lo) + whead) * sizeof(E) + 15) / 16 * 16;
-    bulk_g2s(base + PStage<E>::A_BYTES + PStage<E>::R_BYTES + ts * wslot, wsrc - whead, (uint32_t)w_bytes,
-             &pp.bar[st]);
-  }
-  ++pp.issued;
+LC_D void load_pair(const E* p, E& a0, E& a1);
+template <>
+LC_D void load_pair<uint64_t>(const uint64_t* p, uint64_t& a0, uint64_t& a1) {
+  const uint4 v = __ldg(reinterpret_cast<const uint4*>(p));
+  a0 = ((uint64_t)v.y << 32) | v.x;
+  a1 = ((uint64_t)v.w << 32) | v.z;
+}
+template <>
+LC_D void load_pair<uint32_t>(const uint32_t* p, uint32_t& a0, uint32_t& a1) {
+  const uint2 v = __ldg(reinterpret_cast<const uint2*>(p));
+  a0 = v.x;
+  a1 = v.y;
 }
 
-// false when a wait timed out (the error is recorded; copies in flight were waited for)
 template <class E>
-LC_D bool product_item(const LaneDesc& L, const SubJob* __restrict__ subs, uint32_t chunk, uint64_t k,
-                       unsigned char* smem, ProductPipe& pp, uint32_t* err) {
-  const uint32_t d = 1u << L.log_n;
+LC_D void product_warp_item(const LaneDesc& L, const SubJob* __restrict__ subs, uint32_t chunk, uint64_t k) {
   // chunk of the item: citem[c] <= k < citem[c + 1]
   uint32_t lo = 0, hi = L.nchunks;
   while (hi - lo > 1) {
@@ -285,65 +228,53 @@ LC_D bool product_item(const LaneDesc& L, const SubJob* __restrict__ subs, uint3
     else
       hi = mid;
   }
-  const uint32_t c = lo, tg = L.ctg[c];
-  const uint32_t t0 = (uint32_t)(k - L.citem[c]) * tg;
+  const uint32_t c = lo, nblk = L.cblk[c];
+  const uint32_t r = (uint32_t)(k - L.citem[c]);
+  const uint32_t t = r / nblk, blk = r % nblk;
+  const uint32_t d = 1u << L.log_n;
   const uint32_t j0 = c * chunk, j1 = min(L.n_max, j0 + chunk);
-  const uint32_t rows_cap = kPJB / tg, wpt = kPMaxT / tg;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint32_t ts = warp / wpt, jblk = warp % wpt;
-  const uint32_t t = t0 + ts;
-  const uint32_t ip = lane & 7, bq = jblk * 4 + (lane >> 3);  // rows 2ip, 2ip+1; jobs 4bq..4bq+3
+  const int lane = threadIdx.x & 31;
+  const uint32_t ip = lane & 7, bq = blk * 4 + (lane >> 3);  // rows 2ip, 2ip+1; jobs 4bq..4bq+3
   uint32_t nq[4];
 #pragma unroll
   for (int u = 0; u < 4; ++u) {
     const uint32_t b = 4 * bq + u;
     nq[u] = b < L.nb ? subs[L.sub0 + b].n : 0;  // sorted: nq[0] >= nq[1] >= ...
   }
-  const uint32_t nblk = j1 > j0 ? (j1 - j0 + rows_cap - 1) / rows_cap : 0;
-  if (threadIdx.x == 0)
-    for (uint32_t kb = 0; kb < min(nblk, (uint32_t)kPStages); ++kb)
-      product_issue<E>(L, t0, tg, j0 + kb * rows_cap, min(j1, j0 + (kb + 1) * rows_cap), smem, pp);
+  const uint32_t jend = min(j1, nq[0]);
+  const E* A = reinterpret_cast<const E*>(L.ahat) + (size_t)t * L.a_m * kIPad + 2 * ip;
+  const E* W = reinterpret_cast<const E*>(L.what) + (size_t)t * L.S + 4 * bq;
+  const uint64_t* R = L.R;
   Acc160 acc[2][4];
-  const size_t wslot = PStage<E>::w_slot(tg);
-  for (uint32_t kb = 0; kb < nblk; ++kb) {
-    const int st = pp.consumed % kPStages;
-    const bool ok = mbar_wait(&pp.bar[st], (pp.consumed / kPStages) & 1);
-    if (__syncthreads_or(!ok)) {
-      if (threadIdx.x == 0) {
-        record_error(err, LC_DEVERR_TIMEOUT);
-        for (uint32_t q = pp.consumed + 1; q < pp.issued; ++q)  // later blocks may still be landing
-          mbar_wait(&pp.bar[q % kPStages], (q / kPStages) & 1);
-      }
-      return false;
-    }
-    ++pp.consumed;
-    const unsigned char* base = smem + st * kPStageBytes;
-    const uint32_t* head = pp.head + st * (1 + kPMaxT);
-    const E* sA = reinterpret_cast<const E*>(base) + (size_t)ts * rows_cap * kIPad;
-    const uint64_t* sR = reinterpret_cast<const uint64_t*>(base + PStage<E>::A_BYTES) + head[0];
-    const E* sW = reinterpret_cast<const E*>(base + PStage<E>::A_BYTES + PStage<E>::R_BYTES + ts * wslot) +
-                  head[1 + ts];
-    const uint32_t jb = j0 + kb * rows_cap;
-    const uint32_t rows = min(rows_cap, j1 - jb);
-    const uint64_t w0 = sR[0];
-    const uint32_t jq = nq[0] > jb ? min(rows, nq[0] - jb) : 0;  // rows where this quad has work
-    for (uint32_t jj = 0; jj < jq; ++jj) {
-      const uint32_t j = jb + jj;
-      const uint32_t r = (uint32_t)(sR[jj] - w0);
-      const E a0 = sA[jj * kIPad + 2 * ip], a1 = sA[jj * kIPad + 2 * ip + 1];
-      E wv[4];
+  uint32_t j = j0;
+  for (; j + 2 <= jend; j += 2) {
+    const uint64_t r0 = __ldg(R + j), r1 = __ldg(R + j + 1);
+    E a[2][2], w[2][4];
+    load_pair<E>(A + (size_t)j * kIPad, a[0][0], a[0][1]);
+    load_pair<E>(A + (size_t)(j + 1) * kIPad, a[1][0], a[1][1]);
 #pragma unroll
-      for (int u = 0; u < 4; ++u) wv[u] = j < nq[u] ? sW[r + 4 * bq + u] : E(0);
+    for (int u = 0; u < 4; ++u) {
+      w[0][u] = j < nq[u] ? __ldg(W + r0 + u) : E(0);
+      w[1][u] = j + 1 < nq[u] ? __ldg(W + r1 + u) : E(0);
+    }
+#pragma unroll
+    for (int q = 0; q < 2; ++q)
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
-        mac<E>(acc[0][u], a0, wv[u]);
-        mac<E>(acc[1][u], a1, wv[u]);
+        mac<E>(acc[0][u], a[q][0], w[q][u]);
+        mac<E>(acc[1][u], a[q][1], w[q][u]);
       }
+  }
+  if (j < jend) {
+    const uint64_t r0 = __ldg(R + j);
+    E a0, a1;
+    load_pair<E>(A + (size_t)j * kIPad, a0, a1);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const E wv = j < nq[u] ? __ldg(W + r0 + u) : E(0);
+      mac<E>(acc[0][u], a0, wv);
+      mac<E>(acc[1][u], a1, wv);
     }
-    __syncthreads();  // the stage is free again
-    if (threadIdx.x == 0 && kb + kPStages < nblk)
-      product_issue<E>(L, t0, tg, j0 + (kb + kPStages) * rows_cap, min(j1, j0 + (kb + kPStages + 1) * rows_cap),
-                       smem, pp);
   }
   // jobs active at j0 own a partial of this chunk (the finish launch reads
   // chunks c with c*chunk < n_b)
@@ -353,7 +284,6 @@ LC_D bool product_item(const LaneDesc& L, const SubJob* __restrict__ subs, uint3
 #pragma unroll
     for (int u = 0; u < 4; ++u)
       if (j0 < nq[u]) P[(size_t)(2 * ip + ii) * L.nb + 4 * bq + u] = acc_reduce<E>(acc[ii][u], L.q);
-  return true;
 }
 
 // ---- launch 3: one job's chunk sums and inverse NTT
@@ -439,33 +369,24 @@ __global__ void __launch_bounds__(kBatchThreads) batch_kernel(const __grid_const
 }
 
 __global__ void __launch_bounds__(kBatchThreads) product_kernel(const __grid_constant__ BatchParams p) {
-  extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ unsigned long long s_base;
-  __shared__ __align__(8) uint64_t bars[kPStages];
-  __shared__ uint32_t heads[kPStages * (1 + kPMaxT)];
-  if (threadIdx.x == 0) {
-    for (int i = 0; i < kPStages; ++i) mbar_init(&bars[i], 1);
-    fence_mbar_init();
-  }
-  __syncthreads();
-  ProductPipe pp{bars, heads, 0, 0};
+  const int lane = threadIdx.x & 31;
   const uint64_t total = p.total[1];
-  uint32_t lane = 0;
+  uint32_t li = 0;
   for (;;) {
-    if (threadIdx.x == 0) s_base = atomicAdd(&p.counters[1], (unsigned long long)p.claim);
-    __syncthreads();
-    const uint64_t base = s_base;
-    __syncthreads();
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(&p.counters[1], (unsigned long long)p.claim);
+    base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= total) return;
-    const uint64_t end = min(base + p.claim, total);
+    const uint64_t end = min((uint64_t)base + p.claim, total);
     for (uint64_t it = base; it < end; ++it) {
-      while (lane + 1 < p.nlanes && p.lanes[lane + 1].item0[1] <= it) ++lane;
-      const LaneDesc& L = p.lanes[lane];
+      // a warp's claims only grow, so its lane index only moves forward
+      while (li + 1 < p.nlanes && p.lanes[li + 1].item0[1] <= it) ++li;
+      const LaneDesc& L = p.lanes[li];
       const uint64_t k = it - L.item0[1];
-      const bool ok = L.kind == (uint32_t)PlanKind::Goldilocks
-                          ? product_item<uint64_t>(L, p.subs, p.chunk, k, smem, pp, p.err)
-                          : product_item<uint32_t>(L, p.subs, p.chunk, k, smem, pp, p.err);
-      if (!ok) return;  // every thread saw the same failure
+      if (L.kind == (uint32_t)PlanKind::Goldilocks)
+        product_warp_item<uint64_t>(L, p.subs, p.chunk, k);
+      else
+        product_warp_item<uint32_t>(L, p.subs, p.chunk, k);
     }
   }
 }
@@ -505,7 +426,7 @@ struct lc_batch {
   std::vector<lc::LaneDesc> lanes;     // host copies (device pointers inside)
   std::vector<std::vector<uint64_t>> R;  // staircase offsets per lane (host)
   uint64_t* d_citem = nullptr;
-  uint8_t* d_ctg = nullptr;
+  uint8_t* d_cblk = nullptr;
   std::vector<uint64_t> lane_elem;     // element bytes per lane
   lc::LaneDesc* d_lanes = nullptr;
   lc::SubJob* d_subs = nullptr;
@@ -533,16 +454,16 @@ static void batch_free(lc_batch* b) {
   if (b->cap) cudaStreamDestroy(b->cap);
   for (void* p : {(void*)b->d_lanes, (void*)b->d_subs, (void*)b->d_R, (void*)b->d_itemj, (void*)b->d_what,
                   (void*)b->d_partial, (void*)b->d_counters, (void*)b->d_err, (void*)b->d_citem,
-                  (void*)b->d_ctg})
+                  (void*)b->d_cblk})
     if (p) cudaFree(p);
   delete b;
 }
 
 // chunk-dependent fields, item bases and the device copy of the lanes
 static int batch_layout(lc_batch* b) {
-  // product items per chunk: slots per item from the jobs active at the chunk's start
+  // product items per chunk: one per slot and 16-job block active at the chunk's start
   std::vector<uint64_t> citem;
-  std::vector<uint8_t> ctg;
+  std::vector<uint8_t> cblk;
   std::vector<size_t> coff;
   for (size_t l = 0; l < b->lanes.size(); ++l) {
     LaneDesc& L = b->lanes[l];
@@ -554,34 +475,32 @@ static int batch_layout(lc_batch* b) {
     for (uint32_t c = 0; c < L.nchunks; ++c) {
       const uint64_t j0 = (uint64_t)c * b->chunk;
       const uint64_t cnt = R[j0 + 1] - R[j0];
-      uint32_t wpt = 1;
-      while (wpt * 16 < cnt) wpt *= 2;
-      const uint32_t tg = kPMaxT / wpt;
+      const uint32_t nblk = (uint32_t)((cnt + 15) / 16);
       citem.push_back(acc);
-      ctg.push_back((uint8_t)tg);
-      acc += d / tg;
+      cblk.push_back((uint8_t)nblk);
+      acc += (uint64_t)d * nblk;
     }
     citem.push_back(acc);
-    ctg.push_back(0);
+    cblk.push_back(0);
   }
   if (b->d_citem) cudaFree(b->d_citem);
-  if (b->d_ctg) cudaFree(b->d_ctg);
+  if (b->d_cblk) cudaFree(b->d_cblk);
   b->d_citem = nullptr;
-  b->d_ctg = nullptr;
+  b->d_cblk = nullptr;
   if (cudaMalloc(&b->d_citem, std::max<size_t>(1, citem.size()) * 8) != cudaSuccess ||
-      cudaMalloc(&b->d_ctg, std::max<size_t>(1, ctg.size())) != cudaSuccess) {
+      cudaMalloc(&b->d_cblk, std::max<size_t>(1, cblk.size())) != cudaSuccess) {
     cudaGetLastError();
     return LC_ERR_OUT_OF_MEMORY;
   }
   if (!citem.empty()) {
     cudaMemcpy(b->d_citem, citem.data(), citem.size() * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(b->d_ctg, ctg.data(), ctg.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(b->d_cblk, cblk.data(), cblk.size(), cudaMemcpyHostToDevice);
   }
   uint64_t base[3] = {0, 0, 0};
   for (size_t l = 0; l < b->lanes.size(); ++l) {
     LaneDesc& L = b->lanes[l];
     L.citem = b->d_citem + coff[l];
-    L.ctg = b->d_ctg + coff[l];
+    L.cblk = b->d_cblk + coff[l];
     const uint64_t items[3] = {(L.S + L.pb - 1) / L.pb, citem[coff[l] + L.nchunks], L.nb};
     for (int ph = 0; ph < 3; ++ph) {
       L.item0[ph] = base[ph];
@@ -597,11 +516,7 @@ static int batch_layout(lc_batch* b) {
 }
 
 static int batch_launch(lc_batch* b, cudaStream_t st) {
-  static_assert(kProductSmem <= 227 * 1024, "product ring");
-  cudaError_t e = cudaFuncSetAttribute(product_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)kProductSmem);
-  if (e != cudaSuccess) return map_cuda(e);
-  e = cudaMemsetAsync(b->d_counters, 0, 3 * sizeof(unsigned long long), st);
+  cudaError_t e = cudaMemsetAsync(b->d_counters, 0, 3 * sizeof(unsigned long long), st);
   if (e != cudaSuccess) return map_cuda(e);
   BatchParams p{};
   p.lanes = b->d_lanes;
@@ -614,7 +529,7 @@ static int batch_launch(lc_batch* b, cudaStream_t st) {
   p.claim = b->claim;
   const unsigned grid = (unsigned)std::max(1, device_sm_count()) * b->ctas;
   batch_kernel<0><<<grid, kBatchThreads, b->smem[0], st>>>(p);
-  product_kernel<<<grid, kBatchThreads, kProductSmem, st>>>(p);
+  product_kernel<<<grid, kBatchThreads, 0, st>>>(p);
   batch_kernel<2><<<grid, kBatchThreads, b->smem[2], st>>>(p);
   return map_cuda(cudaGetLastError());
 }
