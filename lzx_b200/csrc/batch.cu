@@ -100,8 +100,15 @@ struct BCfg {
   using Tw = typename A::Tw;
   static constexpr int N = G::N;
   static constexpr int GROUPS = kBatchThreads / G::T;
-  static constexpr int PB = GROUPS;  // one polynomial per thread group
   static constexpr int SS = BatchSlotStride<A, LOG_N>::value;
+  // polynomials per thread group in a witness item: as many as keep the
+  // item's slots within 80 KB (a few per group amortise the item's fixed
+  // costs: counter claim, twiddles, four barriers)
+  static constexpr size_t POLY_BYTES = (size_t)SS * sizeof(T);
+  static constexpr int IT = (size_t)GROUPS * 4 * POLY_BYTES <= 80 * 1024   ? 4
+                            : (size_t)GROUPS * 2 * POLY_BYTES <= 80 * 1024 ? 2
+                                                                           : 1;
+  static constexpr int PB = GROUPS * IT;  // polynomials per witness item
   static constexpr int TWE = G::fwd_entries() > G::inv_entries() ? G::fwd_entries() : G::inv_entries();
   static constexpr size_t TWB = ((size_t)TWE * sizeof(Tw) + 15) / 16 * 16;
   static constexpr size_t SMEM1 = TWB + (size_t)PB * SS * sizeof(T) + (size_t)PB * 8 + (size_t)(PB + 2) * 8;
@@ -180,8 +187,10 @@ LC_D void witness_item(const LaneDesc& L, const SubJob* __restrict__ subs, uint6
   }
   __syncthreads();
   const A ar = make_arith_q<A>(L.q, L.qinv);
-  transform_slot<A, LOG_N, LOG_V, false>(slots + (tid / Geo<LOG_N, LOG_V>::T) * SS, tw, ar,
-                                         tid % Geo<LOG_N, LOG_V>::T);
+#pragma unroll 1
+  for (int it = 0; it < C::IT; ++it)
+    transform_slot<A, LOG_N, LOG_V, false>(slots + (it * C::GROUPS + tid / Geo<LOG_N, LOG_V>::T) * SS, tw, ar,
+                                           tid % Geo<LOG_N, LOG_V>::T);
   __syncthreads();
   T* what = reinterpret_cast<T*>(L.what);
   for (int e = tid; e < PB * N; e += kBatchThreads) {
@@ -348,7 +357,7 @@ LC_D void run_item(const BatchParams& p, const LaneDesc& L, uint64_t k, unsigned
 }
 
 template <int PHASE>
-__global__ void __launch_bounds__(kBatchThreads) batch_kernel(const __grid_constant__ BatchParams p) {
+__global__ void __launch_bounds__(kBatchThreads, 2) batch_kernel(const __grid_constant__ BatchParams p) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ unsigned long long s_base;
   const uint64_t total = p.total[PHASE];
@@ -528,6 +537,10 @@ static int batch_launch(lc_batch* b, cudaStream_t st) {
   p.chunk = b->chunk;
   p.claim = b->claim;
   const unsigned grid = (unsigned)std::max(1, device_sm_count()) * b->ctas;
+  if (b->smem[0] > 48 * 1024) {
+    e = cudaFuncSetAttribute(batch_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem[0]);
+    if (e != cudaSuccess) return map_cuda(e);
+  }
   batch_kernel<0><<<grid, kBatchThreads, b->smem[0], st>>>(p);
   product_kernel<<<grid, kBatchThreads, 0, st>>>(p);
   batch_kernel<2><<<grid, kBatchThreads, b->smem[2], st>>>(p);
