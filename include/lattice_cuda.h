@@ -100,6 +100,19 @@ LC_API int lc_ntt_forward(const lc_ntt_plan *plan, const void *in, void *out, si
 LC_API int lc_ntt_inverse(const lc_ntt_plan *plan, const void *in, void *out, size_t count,
                           lc_stream stream);
 
+/* Incomplete transform, device pointers: NttTables::forward_partial
+ * (ntt.rs:252-286) -- psi^i pre-scale, bit reversal, then only the first
+ * `levels` Cooley-Tukey levels -- and NttTables::complete_partial
+ * (ntt.rs:288-316), which applies the levels after `already`; the output is
+ * the reference's own intermediate order, and complete_partial(
+ * forward_partial(a, L), L) equals lc_ntt_forward(a).  u32 plans only
+ * (LC_ERR_UNSUPPORTED for Goldilocks); levels/already > log_n gives
+ * LC_ERR_LENGTH_MISMATCH as in the reference.  in == out is allowed. */
+LC_API int lc_ntt_forward_partial(lc_ntt_plan *plan, const void *in, void *out, size_t count, uint32_t levels,
+                                  lc_stream stream);
+LC_API int lc_ntt_complete_partial(lc_ntt_plan *plan, const void *in, void *out, size_t count, uint32_t already,
+                                   lc_stream stream);
+
 /* Host-buffer variants: synchronous; copy in, transform, copy out (pipelined
  * in chunks over two streams).  in == out is allowed.  Pinned host memory
  * gives the full PCIe rate; pageable memory works at a lower rate. */
@@ -335,6 +348,17 @@ LC_API int lc_batch_run(lc_batch *batch, lc_stream stream);
 /* Wait for `stream` and report device-side errors of the batch's kernels. */
 LC_API int lc_batch_check(lc_batch *batch, lc_stream stream);
 LC_API void lc_batch_destroy(lc_batch *batch);
+
+/* pack_field_elements (lattice-ring/src/packing.rs:30-52): each of the
+ * `count` Goldilocks values (device, reduced to canonical first) becomes the
+ * three 22-bit limbs raw & (2^22-1), (raw >> 22) & (2^22-1), raw >> 44 in
+ * consecutive coefficients of out = [out_elems][n] u32 (device), zero beyond;
+ * out_elems must be at least max(1, ceil(3*count/n)) (else
+ * LC_ERR_DIMENSION_MISMATCH), so passing the key's m gives pad_to_m
+ * (ajtai.rs:245-257) and the result is the witness AkitaPcs::commit
+ * (lattice-akita/src/pcs.rs:66-76) commits with lc_ajtai_commit. */
+LC_API int lc_pack_field_elements(const uint64_t *values, size_t count, uint32_t log_n, size_t out_elems,
+                                  uint32_t *out, lc_stream stream);
 
 /* Benchmark/test utility, no counterpart in the reference: fill `count`
  * elements of `out` (device) with the seeded counter-based synthetic stream

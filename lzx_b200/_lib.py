@@ -95,6 +95,9 @@ def _declare(L):
         "lc_fold_pipeline_destroy": (None, [P]),
         "lc_ajtai_key_view": (i32, [P, u32, u32, C.POINTER(P)]),
         "lc_uniform_from_seed": (i32, [P, P, sz, P, sz, C.c_uint64, sz, P, P]),
+        "lc_ntt_forward_partial": (i32, [P, P, P, sz, u32, P]),
+        "lc_pack_field_elements": (i32, [P, sz, u32, sz, P, P]),
+        "lc_ntt_complete_partial": (i32, [P, P, P, sz, u32, P]),
         "lc_ajtai_key_from_seed": (i32, [P, u32, u32, P, C.POINTER(P)]),
         "lc_batch_create": (i32, [P, u32, P, u32, u32, C.POINTER(P)]),
         "lc_batch_set_config": (i32, [P, u32, u32, u32]),

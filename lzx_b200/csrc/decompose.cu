@@ -68,6 +68,24 @@ __global__ void gadget_kernel(const uint64_t* __restrict__ z, size_t count, uint
   if (too_large && fails) atomicAdd(too_large, fails);
 }
 
+// pack_field_elements (lattice-ring/src/packing.rs:30-52): value e -> limbs
+// raw & (2^22-1), (raw >> 22) & (2^22-1), raw >> 44 at coefficients 3e..3e+2
+// of the flattened [elems][n] output; the rest zero.
+__global__ void pack_kernel(const uint64_t* __restrict__ v, size_t count, uint32_t* __restrict__ out,
+                            size_t total) {
+  constexpr uint64_t mask = (1ull << 22) - 1;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t e = i / 3;
+    uint32_t c = 0;
+    if (e < count) {
+      const uint64_t raw = gl_canon(__ldg(v + e));
+      const uint32_t part = (uint32_t)(i - 3 * e);
+      c = (uint32_t)(part == 0 ? raw & mask : part == 1 ? (raw >> 22) & mask : raw >> 44);
+    }
+    out[i] = c;
+  }
+}
+
 static unsigned grid_for(size_t items) {
   const int sms = std::max(device_sm_count(), 1);
   return (unsigned)std::max<size_t>(1, std::min<size_t>((items + 255) / 256, (size_t)sms * 16));
@@ -96,6 +114,19 @@ LC_API int lc_gadget_decompose(const uint64_t* z, size_t count, uint32_t log_bas
   if (device_sm_count() <= 0) return LC_ERR_NO_DEVICE;
   gadget_kernel<<<grid_for(count), 256, 0, (cudaStream_t)stream>>>(z, count, log_base, num_digits, out,
                                                                     too_large);
+  return map_cuda(cudaGetLastError());
+}
+
+LC_API int lc_pack_field_elements(const uint64_t* values, size_t count, uint32_t log_n, size_t out_elems,
+                                  uint32_t* out, lc_stream stream) {
+  using namespace lc;
+  if (log_n < 1 || log_n > 11 || !out || (count && !values)) return LC_ERR_INVALID_ARGUMENT;
+  const size_t n = (size_t)1 << log_n;
+  const size_t need = std::max<size_t>(1, (3 * count + n - 1) / n);
+  if (out_elems < need) return LC_ERR_DIMENSION_MISMATCH;
+  if (device_sm_count() <= 0) return LC_ERR_NO_DEVICE;
+  const size_t total = out_elems * n;
+  pack_kernel<<<grid_for(total), 256, 0, (cudaStream_t)stream>>>(values, count, out, total);
   return map_cuda(cudaGetLastError());
 }
 

@@ -70,6 +70,7 @@ struct lc_ntt_plan {
   uint32_t* d_err = nullptr;
   int variant = 0;
   lc::HostPipeline staging;
+  uint32_t* d_pow = nullptr;  // partial transforms: per modulus psi^i (n) then omega^k (n/2), built on first use
 };
 
 struct lc_tc_tables;  // INT8 tensor-core commit tables (tc_commit.cu)

@@ -429,6 +429,7 @@ LC_API void lc_ntt_plan_destroy(lc_ntt_plan* plan) {
   if (plan->d_tw_fwd) cudaFree(plan->d_tw_fwd);
   if (plan->d_tw_inv) cudaFree(plan->d_tw_inv);
   if (plan->d_err) cudaFree(plan->d_err);
+  if (plan->d_pow) cudaFree(plan->d_pow);
   plan->staging.release();
   delete plan;
 }

@@ -194,6 +194,30 @@ class NttTables(_Plan):
     forward = forward_fast
     inverse = inverse_fast
 
+    def forward_partial(self, a, levels: int):
+        """``forward_partial`` (ntt.rs:252-286) in place on the GPU."""
+        return self._run_partial(a, levels, _lib.lib().lc_ntt_forward_partial, "lc_ntt_forward_partial")
+
+    def complete_partial(self, a, already: int):
+        """``complete_partial`` (ntt.rs:288-316) in place on the GPU."""
+        return self._run_partial(a, already, _lib.lib().lc_ntt_complete_partial, "lc_ntt_complete_partial")
+
+    def _run_partial(self, a, lv, fn, name):
+        import torch
+        on_dev = _is_torch_cuda(a)
+        t = a if on_dev else torch.from_numpy(np.ascontiguousarray(a, dtype=np.uint32).view(np.int32)).cuda()
+        count = self._count(t.numel())
+        _raise_for(fn(self._h, C.c_void_p(t.data_ptr()), C.c_void_p(t.data_ptr()), count, lv, _current_stream()),
+                   name)
+        if on_dev:
+            return t
+        torch.cuda.synchronize()
+        out = t.cpu().numpy().view(np.uint32)
+        if isinstance(a, np.ndarray) and a.dtype == np.uint32 and a.flags.writeable:
+            a[...] = out.reshape(a.shape)
+            return a
+        return out
+
 
 class GoldilocksNttTables(_Plan):
     """The ``ntt.rs`` transform over Goldilocks (field.rs), generator 7."""

@@ -113,6 +113,7 @@ def _declare(lib):
         "orc_neo_commit_naive": (i32, [sz, sz, sz, P, P, sz, P]),
         "orc_neo_commit_pay_per_bit": (i32, [sz, sz, sz, P, P, sz, P, P]),
         "orc_decomp_b": (None, [P, sz, u32, P]),
+        "orc_pack_field_elements": (sz, [u32, u32, P, sz, P]),
         "orc_gadget_decompose": (i32, [u64, sz, u64, P]),
         "orc_keccak_f1600": (None, [P]),
         "orc_sha3_256": (None, [P, sz, P]),
@@ -399,6 +400,16 @@ def decomp_b(z, b_bits):
     rows = -(-64 // b_bits)
     out = np.empty((rows, z.size), dtype=np.uint64)
     lib().orc_decomp_b(ptr(z), z.size, b_bits, ptr(out))
+    return out
+
+
+def pack_field_elements(q, log_n, values):
+    """pack_field_elements (packing.rs:30-52): [elems][n] residues."""
+    values = np.ascontiguousarray(values, dtype=np.uint64)
+    n = 1 << log_n
+    elems = max(1, -(-3 * values.size // n))
+    out = np.empty((elems, n), dtype=np.uint32)
+    lib().orc_pack_field_elements(q, log_n, ptr(values), values.size, ptr(out))
     return out
 
 

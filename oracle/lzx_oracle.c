@@ -841,6 +841,28 @@ void orc_decomp_b(const uint64_t *z, size_t len, uint32_t b_bits, uint64_t *out)
   }
 }
 
+/* pack_field_elements, packing.rs:30-52: three 22-bit limbs per canonical
+ * value (the top one < 2^20), chunked into ring elements of n coefficients
+ * with zero padding, at least one element; RingElement::from_signed maps the
+ * (non-negative) limbs to residues.  Returns the number of elements. */
+size_t orc_pack_field_elements(uint32_t q, uint32_t log_n, const uint64_t *values, size_t count, uint32_t *out) {
+  size_t n = (size_t)1 << log_n;
+  size_t nl = 3 * count;
+  size_t elems = (nl + n - 1) / n;
+  if (elems == 0) elems = 1;
+  uint64_t mask = ((uint64_t)1 << 22) - 1;
+  for (size_t i = 0; i < elems * n; i++) {
+    int64_t limb = 0;
+    if (i < nl) {
+      uint64_t raw = orc_gl_from_u64(values[i / 3]);
+      size_t part = i % 3;
+      limb = (int64_t)(part == 0 ? raw & mask : part == 1 ? (raw >> 22) & mask : raw >> 44);
+    }
+    out[i] = (uint32_t)(((limb % (int64_t)q) + (int64_t)q) % (int64_t)q);
+  }
+  return elems;
+}
+
 /* GadgetDecomposition::decompose, decomposition.rs:48-70 */
 int orc_gadget_decompose(uint64_t base, size_t num_digits, uint64_t x, int64_t *out) {
   u128 rem = x;

@@ -153,6 +153,8 @@ int orc_neo_commit_pay_per_bit(size_t d, size_t kappa, size_t m, const uint64_t 
                                uint64_t *column_adds);
 /* decomp_b, neo.rs:253-266: rows = ceil(64/b_bits); out[row*len + j] */
 void orc_decomp_b(const uint64_t *z, size_t len, uint32_t b_bits, uint64_t *out);
+/* pack_field_elements, lattice-ring/src/packing.rs:30-52: out = [elems][n] residues mod q */
+size_t orc_pack_field_elements(uint32_t q, uint32_t log_n, const uint64_t *values, size_t count, uint32_t *out);
 /* GadgetDecomposition::decompose, lattice-core/src/decomposition.rs:48-70;
  * returns 0 ok, 1 ValueTooLarge */
 int orc_gadget_decompose(uint64_t base, size_t num_digits, uint64_t x, int64_t *out);

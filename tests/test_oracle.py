@@ -368,3 +368,21 @@ def test_synthetic_generator_golden(golden):
     assert oracle.synth_mod32(3, 9, oracle.CRT_PRIMES[0][0], 64).tolist() == s["mod32_q0_seed3_stream9"]
     assert [str(x) for x in oracle.synth_gl(3, 9, 64).tolist()] == s["gl_seed3_stream9"]
     assert oracle.synth_i8(3, 9, 64).tolist() == s["i8_seed3_stream9"]
+
+
+def test_pack_field_elements_restatement():
+    """packing.rs:30-52 restated in Python big integers against the oracle."""
+    p = oracle.GL_P
+    q = oracle.Q_32[0]
+    vals = [0, 1, (1 << 22) - 1, 1 << 22, (1 << 44) + 5, p - 1, p + 3, (1 << 64) - 1] + list(range(7, 70, 9))
+    for log_n in (1, 2, 6):
+        n = 1 << log_n
+        limbs = []
+        for v in vals:
+            raw = v % p
+            limbs += [raw & ((1 << 22) - 1), (raw >> 22) & ((1 << 22) - 1), raw >> 44]
+        elems = max(1, -(-len(limbs) // n))
+        want = (limbs + [0] * (elems * n - len(limbs)))
+        got = oracle.pack_field_elements(q, log_n, np.array(vals, dtype=np.uint64))
+        assert got.reshape(-1).tolist() == [x % q for x in want]
+    assert oracle.pack_field_elements(q, 6, np.zeros(0, dtype=np.uint64)).shape == (1, 64)
