@@ -130,6 +130,54 @@ def host_threads() -> int:
         return os.cpu_count() or 1
 
 
+class RankContext:
+    """One process per GPU, launched by torchrun: rank and world size from the
+    environment, a process group when world > 1 (nccl on the GPUs; gloo serves
+    the CPU tests), a barrier, and the maximum over ranks -- every timed
+    figure is the slowest rank's.  The path shards without a data-path
+    collective: each rank commits / transforms its own seeded inputs
+    (weak scaling), and only these scalars cross ranks."""
+
+    def __init__(self, backend: str = "nccl", device: str = "cuda", timeout_s: int = 120):
+        import torch
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.device = device
+        self.dist = None
+        if device == "cuda":
+            torch.cuda.set_device(self.local)
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+            kw = {"device_id": torch.device("cuda", self.local)} if backend == "nccl" else {}
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s), **kw)
+            self.dist = dist
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def max_over_ranks(self, x: float) -> float:
+        if self.dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.dist is not None:
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
+def rank_seed(base: int, rank: int) -> int:
+    """Seed of a rank's synthetic inputs: every rank gets its own batch."""
+    return base + rank
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -696,32 +744,13 @@ def run_ours(args):
 
     from lzx_b200 import CRT_SET_30BIT, NttTables, _lib, synth
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ctx = RankContext("nccl", "cuda")
+    world, rank, dist = ctx.world, ctx.rank, ctx.dist
+    barrier, max_over_ranks = ctx.barrier, ctx.max_over_ranks
 
     L = _lib.lib()
     plan = NttTables(CRT_SET_30BIT, LOG_N)
-    host = synth.crt_batch(1234 + rank, CRT_SET_30BIT, COUNT, 1 << LOG_N)
+    host = synth.crt_batch(rank_seed(1234, rank), CRT_SET_30BIT, COUNT, 1 << LOG_N)
     x = torch.from_numpy(host.view(np.int32)).cuda()
     y = torch.empty_like(x)
     z = torch.empty_like(x)
@@ -811,8 +840,7 @@ def run_ours(args):
     single = bench_single(args, rank, max_over_ranks, barrier, world)
     keygen = bench_keygen(args, rank, max_over_ranks, barrier, world)
 
-    if dist is not None:
-        dist.destroy_process_group()
+    ctx.close()
     if rank != 0:
         return 0
 
