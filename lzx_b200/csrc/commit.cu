@@ -454,10 +454,20 @@ static int launch_witness_to(const lc_ajtai_key* key, const S* w, size_t batch, 
       return launch_witness_cfg<A, LOG_N, LOG_V, S, 256, 64>(key, w, batch, b_pad, dst, st);
   }
   constexpr int PP = SmallWitnessTile<A, LOG_N, LOG_V>::polys;
-  static_assert(PP >= 8 && PP % 8 == 0, "small tile");
-  if (b_pad % 8 == 0) return launch_witness_cfg<A, LOG_N, LOG_V, S, 128, 8, PP / 8>(key, w, batch, b_pad, dst, st);
-  if (b_pad % 4 == 0) return launch_witness_cfg<A, LOG_N, LOG_V, S, 128, 4, PP / 4>(key, w, batch, b_pad, dst, st);
-  if (b_pad < 4) return launch_witness_cfg<A, LOG_N, LOG_V, S, 128, 1, PP>(key, w, batch, b_pad, dst, st);
+  constexpr int G = SmallWitnessTile<A, LOG_N, LOG_V>::groups;
+  static_assert(PP >= 8 && PP % 8 == 0 && G % 8 == 0, "small tile");
+  // tiny problems (fewer polynomials than full tiles for every SM): one
+  // polynomial per thread group, so the grid still spreads over the SMs
+  const bool tiny = (size_t)key->m * b_pad < (size_t)std::max(1, device_sm_count()) * PP;
+  if (b_pad % 8 == 0)
+    return tiny ? launch_witness_cfg<A, LOG_N, LOG_V, S, 128, 8, G / 8>(key, w, batch, b_pad, dst, st)
+                : launch_witness_cfg<A, LOG_N, LOG_V, S, 128, 8, PP / 8>(key, w, batch, b_pad, dst, st);
+  if (b_pad % 4 == 0)
+    return tiny ? launch_witness_cfg<A, LOG_N, LOG_V, S, 128, 4, G / 4>(key, w, batch, b_pad, dst, st)
+                : launch_witness_cfg<A, LOG_N, LOG_V, S, 128, 4, PP / 4>(key, w, batch, b_pad, dst, st);
+  if (b_pad < 4)
+    return tiny ? launch_witness_cfg<A, LOG_N, LOG_V, S, 128, 1, G>(key, w, batch, b_pad, dst, st)
+                : launch_witness_cfg<A, LOG_N, LOG_V, S, 128, 1, PP>(key, w, batch, b_pad, dst, st);
   return launch_witness_cfg<A, LOG_N, LOG_V, S, 128, 32>(key, w, batch, b_pad, dst, st);
 }
 
@@ -521,9 +531,12 @@ static int commit_core(lc_ajtai_key* key, size_t batch, uint32_t b_pad, void* ou
   // contiguous j-range
   const size_t outs = quad ? (size_t)n * ((kappa + 1) / 2) * (b_pad / 4) : (size_t)n * kappa * batch;
   const size_t want = quad ? ((size_t)1 << 19) : ((size_t)1 << 18);
+  // (each product thread sums at least 32 ring elements, so small commits keep
+  // few partial sums to add up afterwards)
   const uint32_t splits =
       tiled ? choose_splits(n, btiles, m)
-            : (uint32_t)std::max<size_t>(1, std::min<size_t>(m, want / std::max<size_t>(1, outs)));
+            : (uint32_t)std::max<size_t>(
+                  1, std::min<size_t>(std::max<size_t>(1, m / 32), want / std::max<size_t>(1, outs)));
   int rc = grow(&key->d_partial, &key->partial_bytes, (size_t)splits * n * kIPad * b_pad * sizeof(E));
   if (rc) return rc;
   rc = grow(&key->d_chat, &key->chat_bytes, (size_t)batch * kappa * n * sizeof(E));
