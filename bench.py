@@ -61,7 +61,7 @@ def parse():
     ap.add_argument("--no-commit", action="store_true", help="skip the Ajtai commit measurement")
     ap.add_argument("--commit-only", action="store_true",
                     help="run only the commit measurement (1 GPU) and print its JSON object")
-    ap.add_argument("--only", choices=["commit", "fold", "single", "uneven", "keygen"], default=None,
+    ap.add_argument("--only", choices=["commit", "fold", "single", "uneven", "keygen", "quad50"], default=None,
                     help="run only one secondary measurement (1 GPU) and print its JSON object")
     ap.add_argument("--no-fold", action="store_true", help="skip the folding-step measurement")
     ap.add_argument("--fold-m", type=int, default=1 << 20, help="ring elements of the folding-step witness")
@@ -72,6 +72,8 @@ def parse():
     ap.add_argument("--uneven-steps", type=int, default=3)
     ap.add_argument("--uneven-profile", action="store_true",
                     help="run only the batch, untuned and without the one-by-one arm (for profilers)")
+    ap.add_argument("--quad50-count", type=int, default=1 << 20, help="ring products per quadratic-slot step")
+    ap.add_argument("--quad50-steps", type=int, default=10)
     ap.add_argument("--commit-steps", type=int, default=5)
     ap.add_argument("--commit-m", type=int, default=1 << 16,
                     help="witness ring elements per commitment (profiling runs use fewer)")
@@ -674,6 +676,85 @@ def bench_keygen(args, rank, max_over_ranks, barrier, world):
     return res
 
 
+# ------------------------------------------------------------------ Modulus50 quadratic-slot products
+
+def bench_quad50(args, rank, max_over_ranks, barrier, world):
+    """RingConfig50::mul at n = 128 (the 64 quadratic slots), q = 2^50 - 2687:
+    a batch of independent ring products per step (two forwards, slotwise
+    Karatsuba, inverse in one launch).  Algorithmic bytes 3 x 128 x 8 per product."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from lzx_b200 import _lib
+    from lzx_b200.ring50 import Modulus50, QuadSlotTables
+    L = _lib.lib()
+    log_n, n = 7, 128
+    count = args.quad50_count
+    t = QuadSlotTables(Modulus50.Q_50, log_n)
+    q = Modulus50.Q_50.q
+    gen = torch.Generator(device="cuda").manual_seed(rank_seed(50, rank))
+    a = torch.randint(0, q, (count, n), dtype=torch.int64, device="cuda", generator=gen)
+    b = torch.randint(0, q, (count, n), dtype=torch.int64, device="cuda", generator=gen)
+    out = torch.empty_like(a)
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    h, pa, pb, po = t.handle, C.c_void_p(a.data_ptr()), C.c_void_p(b.data_ptr()), C.c_void_p(out.data_ptr())
+    for _ in range(3):
+        _lib.check(L.lc_quad50_mul(h, pa, pb, po, count, st), "lc_quad50_mul")
+    K = args.quad50_steps
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    ev0.record()
+    for _ in range(K):
+        L.lc_quad50_mul(h, pa, pb, po, count, st)
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(ev0.elapsed_time(ev1) / K)
+    alg = 3 * n * 8 * count
+    peak, peak_kind = peaks()
+    achieved = alg / (ms / 1e3) / 1e9
+    res = {"workload": f"RingConfig50::mul, q = 2^50 - 2687, n = 128 (64 quadratic slots), {count} products "
+                       f"per GPU ({3 * count * n * 8 >> 20} MiB per step > L2)",
+           "value": world * count / (ms / 1e3), "unit": "ring products/s", "ms_per_step": ms,
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak, "algorithmic_bytes_per_launch": alg,
+                        "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
+           "gpu_launches": K}
+    # end to end: pinned host operands through the host-buffer entry point
+    ca = a[: count // 4].cpu().pin_memory()
+    cb = b[: count // 4].cpu().pin_memory()
+    co = torch.empty_like(ca).pin_memory()
+    ne = ca.shape[0]
+    hp = [C.c_void_p(x.data_ptr()) for x in (ca, cb, co)]
+    _lib.check(L.lc_quad50_mul_host(h, *hp, ne), "lc_quad50_mul_host")
+    assert torch.equal(co[:8], out[:8].cpu())
+    t0 = time.perf_counter()
+    for _ in range(3):
+        L.lc_quad50_mul_host(h, *hp, ne)
+    e2e_s = (time.perf_counter() - t0) / 3
+    res["e2e"] = {"value": world * ne / e2e_s, "unit": "ring products/s", "h2d_bytes_per_step": 2 * ne * n * 8,
+                  "d2h_bytes_per_step": ne * n * 8, "api": "lc_quad50_mul_host, pinned host buffers"}
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracle
+        oracle.prefer_native(True)
+        ot = oracle.QuadSlotTables50(oracle.Modulus50(*oracle.Q_50), log_n)
+        sample = 1 << 16
+        ha = a[:sample].cpu().numpy().view(np.uint64)
+        hb = b[:sample].cpu().numpy().view(np.uint64)
+        nt = host_threads()
+        t0 = time.perf_counter()
+        got = ot.mul_batch(ha, hb, nthreads=nt)
+        dt = time.perf_counter() - t0
+        assert np.array_equal(got[:64], out[:64].cpu().numpy().view(np.uint64))
+        res["cpu_baseline"] = {"value": sample / dt, "unit": "ring products/s", "cores": nt, "kind": "port",
+                               "sample": f"{sample} products, oracle restatement of QuadSlotTables::mul, "
+                                         f"{nt} threads"}
+    del a, b, out
+    return res
+
+
 # ------------------------------------------------------------------ single commitment latency
 
 S_KAPPA, S_M = 8, 256
@@ -839,6 +920,9 @@ def run_ours(args):
     torch.cuda.empty_cache()
     single = bench_single(args, rank, max_over_ranks, barrier, world)
     keygen = bench_keygen(args, rank, max_over_ranks, barrier, world)
+    torch.cuda.empty_cache()
+    quad50 = bench_quad50(args, rank, max_over_ranks, barrier, world)
+    torch.cuda.empty_cache()
 
     ctx.close()
     if rank != 0:
@@ -897,6 +981,7 @@ def run_ours(args):
         "uneven_batch": uneven,
         "key_from_seed": keygen,
         "single_commit": single,
+        "quad_slot_mul": quad50,
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -906,7 +991,7 @@ def run_only(args, which):
     import torch
     torch.cuda.set_device(0)
     fn = {"commit": bench_commit, "fold": bench_fold, "single": bench_single, "uneven": bench_uneven,
-          "keygen": bench_keygen}[which]
+          "keygen": bench_keygen, "quad50": bench_quad50}[which]
     res = fn(args, 0, lambda x: x, lambda: None, 1)
     print(json.dumps(res), flush=True)
     return 0

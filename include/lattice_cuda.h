@@ -48,7 +48,9 @@ typedef enum lc_status {
   LC_ERR_CUDA = 9,                /* a CUDA runtime call failed */
   LC_ERR_OUT_OF_MEMORY = 10,
   LC_ERR_TIMEOUT = 11,            /* a bounded device-side wait expired */
-  LC_ERR_NO_DEVICE = 12           /* no sm_100 device available */
+  LC_ERR_NO_DEVICE = 12,          /* no sm_100 device available */
+  LC_ERR_LOG_N_OUT_OF_RANGE = 13, /* Mod50Error::LogNOutOfRange (lattice-ring/src/modulus50.rs:418) */
+  LC_ERR_GENERATOR_INVALID = 14   /* Mod50Error::GeneratorInvalid (modulus50.rs:420) */
 } lc_status;
 
 typedef void *lc_stream; /* cudaStream_t */
@@ -359,6 +361,41 @@ LC_API void lc_batch_destroy(lc_batch *batch);
  * (lattice-akita/src/pcs.rs:66-76) commits with lc_ajtai_commit. */
 LC_API int lc_pack_field_elements(const uint64_t *values, size_t count, uint32_t log_n, size_t out_elems,
                                   uint32_t *out, lc_stream stream);
+
+/* ---------------------------------------------------------------------------
+ * Modulus50 quadratic-slot ring (lattice-ring/src/modulus50.rs).
+ *
+ * A plan is QuadSlotTables::new(Modulus50::new(q, two_adicity, generator),
+ * log_n) (modulus50.rs:250-301): q an odd prime in (2^49, 2^50) -- the
+ * "~2^50" class, e.g. Q_50 = 2^50 - 2687 with generator 3 (:44-51); other q give
+ * LC_ERR_INVALID_ARGUMENT -- and log_n in [1, 7].  Errors in the reference's
+ * order: LC_ERR_LOG_N_OUT_OF_RANGE, LC_ERR_ADICITY_TOO_SMALL (two_adicity < 7),
+ * LC_ERR_GENERATOR_INVALID (zeta = g^((q-1)/128) not of order 128).
+ * Polynomials are contiguous [count][n] canonical u64 residues on the device;
+ * out may alias an input. */
+typedef struct lc_quad50_plan lc_quad50_plan;
+LC_API int lc_quad50_plan_create(uint64_t q, uint32_t two_adicity, uint64_t generator, uint32_t log_n,
+                                 lc_quad50_plan **out);
+LC_API void lc_quad50_plan_destroy(lc_quad50_plan *plan);
+/* zeta (QuadSlotTables::zeta) and, if non-null, the n/2 leaf constants
+ * gamma_p (RingConfig50::slot_constants, :446-448) into host memory. */
+LC_API int lc_quad50_plan_info(const lc_quad50_plan *plan, uint64_t *zeta, uint64_t *slot_constants);
+/* QuadSlotTables::forward (:313-334) / inverse (:338-364) of count polynomials */
+LC_API int lc_quad50_forward(const lc_quad50_plan *plan, const uint64_t *in, uint64_t *out, size_t count,
+                             lc_stream stream);
+LC_API int lc_quad50_inverse(const lc_quad50_plan *plan, const uint64_t *in, uint64_t *out, size_t count,
+                             lc_stream stream);
+/* QuadSlotTables::slotwise_mul (:368-392) of slot-form operands */
+LC_API int lc_quad50_slotwise_mul(const lc_quad50_plan *plan, const uint64_t *a, const uint64_t *b,
+                                  uint64_t *out, size_t count, lc_stream stream);
+/* QuadSlotTables::mul / RingConfig50::mul (:395-411, :450-453): count
+ * products in Z_q[X]/(X^n + 1), both forwards, the slot products and the
+ * inverse in one launch. */
+LC_API int lc_quad50_mul(const lc_quad50_plan *plan, const uint64_t *a, const uint64_t *b, uint64_t *out,
+                         size_t count, lc_stream stream);
+/* The same product over host buffers (synchronous; copies overlap kernels). */
+LC_API int lc_quad50_mul_host(lc_quad50_plan *plan, const uint64_t *a, const uint64_t *b, uint64_t *out,
+                              size_t count);
 
 /* Benchmark/test utility, no counterpart in the reference: fill `count`
  * elements of `out` (device) with the seeded counter-based synthetic stream

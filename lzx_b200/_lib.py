@@ -27,6 +27,8 @@ LC_ERR_CUDA = 9
 LC_ERR_OUT_OF_MEMORY = 10
 LC_ERR_TIMEOUT = 11
 LC_ERR_NO_DEVICE = 12
+LC_ERR_LOG_N_OUT_OF_RANGE = 13
+LC_ERR_GENERATOR_INVALID = 14
 
 LC_KEY_TENSOR_I8 = 1
 LC_ENGINE_NTT = 0
@@ -107,6 +109,14 @@ def _declare(L):
         "lc_batch_check": (i32, [P, P]),
         "lc_batch_destroy": (None, [P]),
         "lc_synth_fill": (i32, [i32, C.c_uint64, C.c_uint64, u32, P, sz, sz, P]),
+        "lc_quad50_plan_create": (i32, [C.c_uint64, u32, C.c_uint64, u32, C.POINTER(P)]),
+        "lc_quad50_plan_destroy": (None, [P]),
+        "lc_quad50_plan_info": (i32, [P, P, P]),
+        "lc_quad50_forward": (i32, [P, P, P, sz, P]),
+        "lc_quad50_inverse": (i32, [P, P, P, sz, P]),
+        "lc_quad50_slotwise_mul": (i32, [P, P, P, P, sz, P]),
+        "lc_quad50_mul": (i32, [P, P, P, P, sz, P]),
+        "lc_quad50_mul_host": (i32, [P, P, P, P, sz]),
     }
     optional = {
     }

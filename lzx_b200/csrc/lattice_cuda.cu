@@ -299,6 +299,8 @@ LC_API const char* lc_status_string(int s) {
     case LC_ERR_OUT_OF_MEMORY: return "out of memory";
     case LC_ERR_TIMEOUT: return "device wait timed out";
     case LC_ERR_NO_DEVICE: return "no sm_100 device";
+    case LC_ERR_LOG_N_OUT_OF_RANGE: return "log_n out of range";
+    case LC_ERR_GENERATOR_INVALID: return "generator invalid";
     default: return "unknown status";
   }
 }

@@ -56,6 +56,16 @@ class Ntt32(C.Structure):
                 ("level_tw_inv", C.c_void_p)]
 
 
+class Mod50(C.Structure):
+    _fields_ = [("q", C.c_uint64), ("recip", C.c_uint64), ("two_adicity", C.c_uint32),
+                ("generator", C.c_uint64)]
+
+
+class Quad50(C.Structure):
+    _fields_ = [("modulus", Mod50), ("log_n", C.c_uint32), ("zeta", C.c_uint64), ("level_tw", C.c_void_p),
+                ("level_tw_inv", C.c_void_p), ("leaf_gamma", C.c_void_p)]
+
+
 class NttGl(C.Structure):
     _fields_ = [("log_n", C.c_uint32), ("n_inv", C.c_uint64), ("pow_psi", C.c_void_p),
                 ("pow_psi_inv", C.c_void_p), ("level_tw", C.c_void_p), ("level_tw_inv", C.c_void_p)]
@@ -115,6 +125,19 @@ def _declare(lib):
         "orc_decomp_b": (None, [P, sz, u32, P]),
         "orc_pack_field_elements": (sz, [u32, u32, P, sz, P]),
         "orc_gadget_decompose": (i32, [u64, sz, u64, P]),
+        "orc_mod50_new": (Mod50, [u64, u32, u64]),
+        "orc_mod50_reduce_u128": (u64, [P, u64, u64]),
+        "orc_mod50_mul": (u64, [P, u64, u64]),
+        "orc_mod50_add": (u64, [P, u64, u64]),
+        "orc_mod50_sub": (u64, [P, u64, u64]),
+        "orc_mod50_pow": (u64, [P, u64, u64]),
+        "orc_quad50_new": (i32, [Mod50, u32, P]),
+        "orc_quad50_free": (None, [P]),
+        "orc_quad50_forward": (i32, [P, P, sz]),
+        "orc_quad50_inverse": (i32, [P, P, sz]),
+        "orc_quad50_slotwise_mul": (i32, [P, P, P, P, sz]),
+        "orc_quad50_mul": (i32, [P, P, P, P, sz]),
+        "orc_quad50_mul_batch": (i32, [P, P, P, P, sz, i32]),
         "orc_keccak_f1600": (None, [P]),
         "orc_sha3_256": (None, [P, sz, P]),
         "orc_shake256": (None, [P, sz, P, sz]),
@@ -419,6 +442,91 @@ def gadget_decompose(base, num_digits, x):
     if rc:
         raise ValueError("ValueTooLarge")
     return out
+
+
+# ----------------------------------------------------------------- Modulus50
+
+# Q_50 = 2^50 - 2687, two-adicity 7, generator 3 (lattice-ring/src/modulus50.rs:44-51)
+Q_50 = (1125899906839937, 7, 3)
+
+
+class Modulus50:
+    """Modulus50 (modulus50.rs:53-198) through the C restatement."""
+
+    def __init__(self, q: int, two_adicity: int, generator: int):
+        self.q, self.two_adicity, self.generator = q, two_adicity, generator
+        self.s = lib().orc_mod50_new(q, two_adicity, generator)
+
+    def _p(self):
+        return C.byref(self.s)
+
+    def reduce_u128(self, x: int) -> int:
+        return lib().orc_mod50_reduce_u128(self._p(), x >> 64, x & (2**64 - 1))
+
+    def mul(self, a, b):
+        return lib().orc_mod50_mul(self._p(), a, b)
+
+    def add(self, a, b):
+        return lib().orc_mod50_add(self._p(), a, b)
+
+    def sub(self, a, b):
+        return lib().orc_mod50_sub(self._p(), a, b)
+
+    def pow(self, a, e):
+        return lib().orc_mod50_pow(self._p(), a, e)
+
+
+class QuadSlotTables50:
+    """QuadSlotTables (modulus50.rs:206-411); raises NttError(code) like new()."""
+
+    def __init__(self, modulus: Modulus50, log_n: int):
+        self.modulus, self.log_n, self.n = modulus, log_n, 1 << log_n
+        self.t = Quad50()
+        _check(lib().orc_quad50_new(modulus.s, log_n, C.byref(self.t)))
+
+    def __del__(self):
+        if getattr(self, "t", None) is not None and self.t.level_tw and _lib is not None:
+            _lib.orc_quad50_free(C.byref(self.t))
+
+    @property
+    def zeta(self) -> int:
+        return self.t.zeta
+
+    @property
+    def leaf_gamma(self) -> np.ndarray:
+        return np.ctypeslib.as_array(C.cast(self.t.leaf_gamma, C.POINTER(C.c_uint64)), (self.n // 2,)).copy()
+
+    def _one(self, fn, a):
+        a = np.array(a, dtype=np.uint64)
+        _check(fn(C.byref(self.t), ptr(a), a.size))
+        return a
+
+    def forward(self, a):
+        return self._one(lib().orc_quad50_forward, a)
+
+    def inverse(self, a):
+        return self._one(lib().orc_quad50_inverse, a)
+
+    def slotwise_mul(self, a, b):
+        a = np.ascontiguousarray(a, dtype=np.uint64)
+        b = np.ascontiguousarray(b, dtype=np.uint64)
+        out = np.empty_like(a)
+        _check(lib().orc_quad50_slotwise_mul(C.byref(self.t), ptr(a), ptr(b), ptr(out), a.size))
+        return out
+
+    def mul(self, a, b):
+        a = np.ascontiguousarray(a, dtype=np.uint64)
+        b = np.ascontiguousarray(b, dtype=np.uint64)
+        out = np.empty_like(a)
+        _check(lib().orc_quad50_mul(C.byref(self.t), ptr(a), ptr(b), ptr(out), a.size))
+        return out
+
+    def mul_batch(self, a, b, nthreads: int = 0):
+        a = np.ascontiguousarray(a, dtype=np.uint64)
+        b = np.ascontiguousarray(b, dtype=np.uint64)
+        out = np.empty_like(a)
+        lib().orc_quad50_mul_batch(C.byref(self.t), ptr(a), ptr(b), ptr(out), a.size // self.n, nthreads)
+        return out
 
 
 # ----------------------------------------------------------------- hashing

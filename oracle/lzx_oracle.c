@@ -863,6 +863,190 @@ size_t orc_pack_field_elements(uint32_t q, uint32_t log_n, const uint64_t *value
   return elems;
 }
 
+/* ============== Modulus50 + QuadSlotTables (modulus50.rs) ================= */
+
+/* Modulus50::new, modulus50.rs:75-83 */
+orc_mod50 orc_mod50_new(uint64_t q, uint32_t two_adicity, uint64_t generator) {
+  orc_mod50 m;
+  m.q = q;
+  m.recip = UINT64_MAX / q;
+  m.two_adicity = two_adicity;
+  m.generator = generator;
+  return m;
+}
+
+/* Modulus50::reduce_u128, modulus50.rs:90-118: fold 2^50 == 2^50 mod q (once
+ * more if the result reaches 2^62), then one Barrett pass, <= 2 corrections. */
+uint64_t orc_mod50_reduce_u128(const orc_mod50 *m, uint64_t xhi, uint64_t xlo) {
+  u128 x = ((u128)xhi << 64) | xlo;
+  u128 q = m->q;
+  if (x < q) return (uint64_t)x;
+  u128 fold = ((u128)1 << 50) % q;
+  u128 mask = ((u128)1 << 50) - 1;
+  u128 y = (x >> 50) * fold + (x & mask);
+  if ((y >> 62) != 0) y = (y >> 50) * fold + (y & mask);
+  u128 qhat = (y * (u128)m->recip) >> 64;
+  u128 r = y - qhat * q;
+  if (r >= q) r -= q;
+  if (r >= q) r -= q;
+  return (uint64_t)r;
+}
+
+/* mul :126-128, add :131-139, sub :142-149, pow :168-180 */
+uint64_t orc_mod50_mul(const orc_mod50 *m, uint64_t a, uint64_t b) {
+  u128 x = (u128)a * b;
+  return orc_mod50_reduce_u128(m, (uint64_t)(x >> 64), (uint64_t)x);
+}
+
+uint64_t orc_mod50_add(const orc_mod50 *m, uint64_t a, uint64_t b) {
+  uint64_t s = a + b;
+  return s >= m->q ? s - m->q : s;
+}
+
+uint64_t orc_mod50_sub(const orc_mod50 *m, uint64_t a, uint64_t b) {
+  return a >= b ? a - b : a + (m->q - b);
+}
+
+uint64_t orc_mod50_pow(const orc_mod50 *m, uint64_t base, uint64_t exp) {
+  uint64_t acc = 1, b = base % m->q;
+  while (exp > 0) {
+    if (exp & 1) acc = orc_mod50_mul(m, acc, b);
+    b = orc_mod50_mul(m, b, b);
+    exp >>= 1;
+  }
+  return acc;
+}
+
+static size_t rev_bits50(size_t x, uint32_t bits) {
+  size_t r = 0;
+  for (uint32_t b = 0; b < bits; b++) r |= ((x >> b) & 1) << (bits - 1 - b);
+  return r;
+}
+
+/* QuadSlotTables::new, modulus50.rs:250-301 */
+int orc_quad50_new(orc_mod50 m, uint32_t log_n, orc_quad50 *out) {
+  memset(out, 0, sizeof(*out));
+  if (log_n == 0 || log_n > 7) return ORC_ERR_LOG_N_OUT_OF_RANGE;
+  if (m.two_adicity < 7) return ORC_ERR_ADICITY_TOO_SMALL;
+  uint64_t zeta = orc_mod50_pow(&m, m.generator, (m.q - 1) >> 7); /* root_of_unity(7), :191-197 */
+  if (orc_mod50_pow(&m, zeta, 64) != m.q - 1) return ORC_ERR_GENERATOR_INVALID;
+  size_t slots = (size_t)1 << (log_n - 1);
+  out->modulus = m;
+  out->log_n = log_n;
+  out->zeta = zeta;
+  out->level_tw = (uint64_t *)calloc(slots, sizeof(uint64_t));
+  out->level_tw_inv = (uint64_t *)calloc(slots, sizeof(uint64_t));
+  out->leaf_gamma = (uint64_t *)calloc(slots, sizeof(uint64_t));
+  for (uint32_t d = 0; d + 1 < log_n; d++) {
+    uint32_t shift = 5 - d;
+    for (size_t i = 0; i < ((size_t)1 << d); i++) {
+      uint64_t e = ((2 * (uint64_t)rev_bits50(i, d) + 1) << shift) % 128;
+      uint64_t w = orc_mod50_pow(&m, zeta, e);
+      out->level_tw[((size_t)1 << d) - 1 + i] = w;
+      out->level_tw_inv[((size_t)1 << d) - 1 + i] = orc_mod50_pow(&m, w, m.q - 2); /* inv, :183-189 */
+    }
+  }
+  uint32_t leaf_shift = 7 - log_n;
+  for (size_t p = 0; p < slots; p++) {
+    uint64_t e = ((2 * (uint64_t)rev_bits50(p, log_n - 1) + 1) << leaf_shift) % 128;
+    out->leaf_gamma[p] = orc_mod50_pow(&m, zeta, e);
+  }
+  return ORC_OK;
+}
+
+void orc_quad50_free(orc_quad50 *t) {
+  free(t->level_tw);
+  free(t->level_tw_inv);
+  free(t->leaf_gamma);
+  memset(t, 0, sizeof(*t));
+}
+
+/* forward, modulus50.rs:313-334 */
+int orc_quad50_forward(const orc_quad50 *t, uint64_t *a, size_t len) {
+  size_t n = (size_t)1 << t->log_n;
+  if (len != n) return ORC_ERR_LENGTH_MISMATCH;
+  const orc_mod50 *q = &t->modulus;
+  for (uint32_t d = 0; d + 1 < t->log_n; d++) {
+    size_t span = n >> d, half = span / 2;
+    for (size_t i = 0; i < ((size_t)1 << d); i++) {
+      uint64_t w = t->level_tw[((size_t)1 << d) - 1 + i];
+      size_t start = i * span;
+      for (size_t j = 0; j < half; j++) {
+        uint64_t lo = a[start + j], hi = a[start + j + half];
+        a[start + j] = orc_mod50_add(q, lo, orc_mod50_mul(q, w, hi));
+        a[start + j + half] = orc_mod50_sub(q, lo, orc_mod50_mul(q, w, hi));
+      }
+    }
+  }
+  return ORC_OK;
+}
+
+/* inverse, modulus50.rs:338-364 */
+int orc_quad50_inverse(const orc_quad50 *t, uint64_t *a, size_t len) {
+  size_t n = (size_t)1 << t->log_n;
+  if (len != n) return ORC_ERR_LENGTH_MISMATCH;
+  const orc_mod50 *q = &t->modulus;
+  uint64_t inv2 = orc_mod50_pow(q, 2, q->q - 2);
+  for (int d = (int)t->log_n - 2; d >= 0; d--) {
+    size_t span = n >> d, half = span / 2;
+    for (size_t i = 0; i < ((size_t)1 << d); i++) {
+      uint64_t w_inv = t->level_tw_inv[((size_t)1 << d) - 1 + i];
+      size_t start = i * span;
+      for (size_t j = 0; j < half; j++) {
+        uint64_t lo = a[start + j], hi = a[start + j + half];
+        uint64_t sum = orc_mod50_add(q, lo, hi);
+        uint64_t diff = orc_mod50_sub(q, lo, hi);
+        uint64_t half_diff = orc_mod50_mul(q, diff, inv2);
+        a[start + j] = orc_mod50_mul(q, sum, inv2);
+        a[start + j + half] = orc_mod50_mul(q, half_diff, w_inv);
+      }
+    }
+  }
+  return ORC_OK;
+}
+
+/* slotwise_mul, modulus50.rs:368-392 (Karatsuba per quadratic slot) */
+int orc_quad50_slotwise_mul(const orc_quad50 *t, const uint64_t *a, const uint64_t *b, uint64_t *out,
+                            size_t len) {
+  size_t n = (size_t)1 << t->log_n;
+  if (len != n) return ORC_ERR_LENGTH_MISMATCH;
+  const orc_mod50 *q = &t->modulus;
+  for (size_t p = 0; p < n / 2; p++) {
+    uint64_t u0 = a[2 * p], u1 = a[2 * p + 1], v0 = b[2 * p], v1 = b[2 * p + 1];
+    uint64_t g = t->leaf_gamma[p];
+    uint64_t p0 = orc_mod50_mul(q, u0, v0);
+    uint64_t p1 = orc_mod50_mul(q, u1, v1);
+    uint64_t cross = orc_mod50_mul(q, orc_mod50_add(q, u0, u1), orc_mod50_add(q, v0, v1));
+    out[2 * p] = orc_mod50_add(q, p0, orc_mod50_mul(q, g, p1));
+    out[2 * p + 1] = orc_mod50_sub(q, cross, orc_mod50_add(q, p0, p1));
+  }
+  return ORC_OK;
+}
+
+/* mul, modulus50.rs:395-411 */
+int orc_quad50_mul(const orc_quad50 *t, const uint64_t *a, const uint64_t *b, uint64_t *out, size_t len) {
+  size_t n = (size_t)1 << t->log_n;
+  if (len != n) return ORC_ERR_LENGTH_MISMATCH;
+  uint64_t ta[128], tb[128];
+  memcpy(ta, a, n * 8);
+  memcpy(tb, b, n * 8);
+  orc_quad50_forward(t, ta, n);
+  orc_quad50_forward(t, tb, n);
+  orc_quad50_slotwise_mul(t, ta, tb, out, n);
+  return orc_quad50_inverse(t, out, n);
+}
+
+int orc_quad50_mul_batch(const orc_quad50 *t, const uint64_t *a, const uint64_t *b, uint64_t *out,
+                         size_t count, int nthreads) {
+  size_t n = (size_t)1 << t->log_n;
+  int nt = resolve_threads(nthreads);
+  (void)nt;
+#pragma omp parallel for schedule(static) num_threads(nt)
+  for (long long i = 0; i < (long long)count; i++)
+    orc_quad50_mul(t, a + (size_t)i * n, b + (size_t)i * n, out + (size_t)i * n, n);
+  return ORC_OK;
+}
+
 /* GadgetDecomposition::decompose, decomposition.rs:48-70 */
 int orc_gadget_decompose(uint64_t base, size_t num_digits, uint64_t x, int64_t *out) {
   u128 rem = x;

@@ -159,6 +159,48 @@ size_t orc_pack_field_elements(uint32_t q, uint32_t log_n, const uint64_t *value
  * returns 0 ok, 1 ValueTooLarge */
 int orc_gadget_decompose(uint64_t base, size_t num_digits, uint64_t x, int64_t *out);
 
+/* ---------------- Modulus50 + quadratic-slot incomplete NTT --------------
+ * (crates/lattice-ring/src/modulus50.rs) */
+
+#define ORC_ERR_LOG_N_OUT_OF_RANGE 13 /* Mod50Error::LogNOutOfRange (modulus50.rs:418) */
+#define ORC_ERR_GENERATOR_INVALID 14  /* Mod50Error::GeneratorInvalid (modulus50.rs:420) */
+
+typedef struct {
+  uint64_t q;
+  uint64_t recip; /* floor((2^64-1) / q), modulus50.rs:69 */
+  uint32_t two_adicity;
+  uint64_t generator;
+} orc_mod50;
+
+orc_mod50 orc_mod50_new(uint64_t q, uint32_t two_adicity, uint64_t generator);
+uint64_t orc_mod50_reduce_u128(const orc_mod50 *m, uint64_t hi, uint64_t lo);
+uint64_t orc_mod50_mul(const orc_mod50 *m, uint64_t a, uint64_t b);
+uint64_t orc_mod50_add(const orc_mod50 *m, uint64_t a, uint64_t b);
+uint64_t orc_mod50_sub(const orc_mod50 *m, uint64_t a, uint64_t b);
+uint64_t orc_mod50_pow(const orc_mod50 *m, uint64_t base, uint64_t exp);
+
+/* QuadSlotTables (modulus50.rs:206-301): level d (blocks 2^d) at offset 2^d - 1 */
+typedef struct {
+  orc_mod50 modulus;
+  uint32_t log_n;
+  uint64_t zeta;
+  uint64_t *level_tw;     /* [n/2 - 1] */
+  uint64_t *level_tw_inv; /* [n/2 - 1] */
+  uint64_t *leaf_gamma;   /* [n/2] */
+} orc_quad50;
+
+/* ORC_ERR_LOG_N_OUT_OF_RANGE, ORC_ERR_ADICITY_TOO_SMALL, ORC_ERR_GENERATOR_INVALID */
+int orc_quad50_new(orc_mod50 m, uint32_t log_n, orc_quad50 *out);
+void orc_quad50_free(orc_quad50 *t);
+int orc_quad50_forward(const orc_quad50 *t, uint64_t *a, size_t len);
+int orc_quad50_inverse(const orc_quad50 *t, uint64_t *a, size_t len);
+int orc_quad50_slotwise_mul(const orc_quad50 *t, const uint64_t *a, const uint64_t *b, uint64_t *out,
+                            size_t len);
+int orc_quad50_mul(const orc_quad50 *t, const uint64_t *a, const uint64_t *b, uint64_t *out, size_t len);
+/* count independent ring products (CPU baseline); nthreads <= 0: all cores */
+int orc_quad50_mul_batch(const orc_quad50 *t, const uint64_t *a, const uint64_t *b, uint64_t *out,
+                         size_t count, int nthreads);
+
 /* ---------------- Keccak / transcript (keccak.rs, transcript.rs) ---------- */
 
 void orc_keccak_f1600(uint64_t st[25]);
