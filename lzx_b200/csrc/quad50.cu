@@ -11,10 +11,15 @@
 // GPU layout: polynomials are contiguous [count][n] u64 residues.  A warp
 // owns 32/G polynomials (G = min(32, n/2) lanes per polynomial) staged in
 // shared memory; every level is one butterfly (or one slot) per lane per
-// n/(2G), separated by __syncwarp.  Every multiplication in the transforms is
-// by a table constant (Shoup: w and floor(w 2^64 / q)); the Karatsuba
-// products of two data values use Barrett with mu = floor(2^100 / q).  All
-// outputs are canonical residues, so they equal the reference's bit for bit.
+// n/(2G), separated by __syncwarp.
+//
+// Arithmetic: residues below q < 2^50 are exact doubles, so a modular
+// product runs on the FP64 pipe -- h = RN(ab), the exact remainder
+// l = fma(a, b, -h), a quotient c = the integer nearest h*(1/q) (one fma
+// into the 1.5*2^52 rounding constant), and r = fma(-c, q, h) + l, which is
+// exact and lies in (-q, q): |c - ab/q| <= 1/2 + 1/8 + 1/8 because
+// |l| <= 2^46 and q > 2^49.  One conditional add of q makes it canonical, so
+// every output equals the reference's u64 arithmetic bit for bit.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -26,10 +31,6 @@
 
 namespace lc {
 
-struct Shoup50 {
-  uint64_t w, ws;  // ws = floor(w * 2^64 / q)
-};
-
 // Table layout (entries): forward twiddles of level d (2^d blocks) at
 // 2^d - 1, then the inverse constants inv2 * w^-1 at kQ50Inv + 2^d - 1, the
 // leaf gammas at kQ50Gamma, and inv2 at kQ50Inv2.
@@ -38,10 +39,10 @@ constexpr int kQ50Inv = 64, kQ50Gamma = 128, kQ50Inv2 = 192, kQ50Tab = 193;
 }  // namespace lc
 
 struct lc_quad50_plan {
-  uint64_t q = 0, mu = 0, zeta = 0, generator = 0;
+  uint64_t q = 0, zeta = 0, generator = 0;
   uint32_t two_adicity = 0, log_n = 0;
-  lc::Shoup50 tab[lc::kQ50Tab] = {};
-  lc::Shoup50* d_tab = nullptr;
+  uint64_t tab[lc::kQ50Tab] = {};
+  double* d_tab = nullptr;
   lc::HostPipeline staging;
 };
 
@@ -56,34 +57,29 @@ struct Q50Params {
   const uint64_t* b;
   uint64_t* out;
   size_t count;
-  uint64_t q, mu;
-  const Shoup50* tab;
+  double q, qinv;  // qinv = RN(1/q)
+  const double* tab;
 };
 
-LC_D uint64_t q50_add(uint64_t a, uint64_t b, uint64_t q) {
-  const uint64_t s = a + b;
-  return s >= q ? s - q : s;
+constexpr double kRound52 = 6755399441055744.0;  // 1.5 * 2^52: adding it rounds [0, 2^51) to integers
+
+LC_D double q50_add(double a, double b, double q) {
+  const double s = __dadd_rn(a, b);
+  return s >= q ? __dadd_rn(s, -q) : s;
 }
 
-LC_D uint64_t q50_sub(uint64_t a, uint64_t b, uint64_t q) { return a >= b ? a - b : a + (q - b); }
-
-// x * w mod q for a table constant (x < 2^64, w < q): r in [0, 2q) then one correction
-LC_D uint64_t q50_mulc(uint64_t x, Shoup50 c, uint64_t q) {
-  const uint64_t r = x * c.w - __umul64hi(x, c.ws) * q;
-  return r >= q ? r - q : r;
+LC_D double q50_sub(double a, double b, double q) {
+  const double d = __dadd_rn(a, -b);
+  return d < 0.0 ? __dadd_rn(d, q) : d;
 }
 
-// a * b mod q for residues a, b < q < 2^50: Barrett with k = 50 bits,
-// mu = floor(2^100 / q); the quotient estimate is at most 2 below floor(x / q).
-LC_D uint64_t q50_mul(uint64_t a, uint64_t b, uint64_t q, uint64_t mu) {
-  const uint64_t lo = a * b, hi = __umul64hi(a, b);  // x < 2^100
-  const uint64_t x1 = (lo >> 49) | (hi << 15);       // floor(x / 2^49) < 2^51
-  const uint64_t t_lo = x1 * mu, t_hi = __umul64hi(x1, mu);
-  const uint64_t qhat = (t_lo >> 51) | (t_hi << 13);
-  uint64_t r = lo - qhat * q;
-  if (r >= q) r -= q;
-  if (r >= q) r -= q;
-  return r;
+// a * b mod q for residues a, b < q, 2^49 < q < 2^50
+LC_D double q50_mul(double a, double b, double q, double qinv) {
+  const double h = __dmul_rn(a, b);
+  const double l = __fma_rn(a, b, -h);
+  const double c = __dadd_rn(__fma_rn(h, qinv, kRound52), -kRound52);
+  const double r = __dadd_rn(__fma_rn(-c, q, h), l);
+  return r < 0.0 ? __dadd_rn(r, q) : r;
 }
 
 template <int LOG_N>
@@ -96,41 +92,90 @@ struct Q50Geo {
   static constexpr int WE = PW * N;                 // elements per warp
 };
 
+// Register levels: lane l holds elements l + 32 r (r < E) of its warp's
+// region.  For n >= 64 the DIF levels whose half span is at least 32 pair
+// elements of one lane, with a twiddle that depends on r only.
 template <int LOG_N>
-LC_D void q50_forward(uint64_t* x, const Shoup50* tab, uint32_t g, uint64_t q) {
+struct Q50Reg {
+  static constexpr int E = Q50Geo<LOG_N>::WE / 32;         // elements per lane
+  static constexpr int LEVELS = LOG_N >= 6 ? LOG_N - 5 : 0;  // forward d < LEVELS, inverse likewise
+};
+
+template <int LOG_N>
+LC_D void q50_forward_regs(double (&v)[Q50Reg<LOG_N>::E], const double* tab, double q, double qinv) {
+  constexpr int E = Q50Reg<LOG_N>::E;
+#pragma unroll
+  for (int d = 0; d < Q50Reg<LOG_N>::LEVELS; ++d) {
+    const int hr = (1 << (LOG_N - 1 - d)) / 32;  // register distance of the pair
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+      if (r & hr) continue;
+      const double t = q50_mul(v[r + hr], tab[(1 << d) - 1 + r / (2 * hr)], q, qinv);
+      const double L = v[r];
+      v[r] = q50_add(L, t, q);
+      v[r + hr] = q50_sub(L, t, q);
+    }
+  }
+}
+
+template <int LOG_N>
+LC_D void q50_inverse_regs(double (&v)[Q50Reg<LOG_N>::E], const double* tab, double q, double qinv) {
+  constexpr int E = Q50Reg<LOG_N>::E;
+  const double inv2 = tab[kQ50Inv2];
+#pragma unroll
+  for (int d = Q50Reg<LOG_N>::LEVELS - 1; d >= 0; --d) {
+    const int hr = (1 << (LOG_N - 1 - d)) / 32;
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+      if (r & hr) continue;
+      const double L = v[r], H = v[r + hr];
+      v[r] = q50_mul(q50_add(L, H, q), inv2, q, qinv);
+      v[r + hr] = q50_mul(q50_sub(L, H, q), tab[kQ50Inv + (1 << d) - 1 + r / (2 * hr)], q, qinv);
+    }
+  }
+}
+
+// Shared-memory levels d in [Q50Reg::LEVELS, LOG_N - 1) of NX polynomials
+// (one per operand) of this lane's group, interleaved for independent work.
+template <int LOG_N, int NX>
+LC_D void q50_forward_smem(double* const (&x)[NX], const double* tab, uint32_t g, double q, double qinv) {
   using Q = Q50Geo<LOG_N>;
 #pragma unroll
-  for (int d = 0; d + 1 < LOG_N; ++d) {
+  for (int d = Q50Reg<LOG_N>::LEVELS; d + 1 < LOG_N; ++d) {
     const int hb = LOG_N - 1 - d;  // log2 of the half span
 #pragma unroll
     for (int r = 0; r < Q::BPT; ++r) {
       const uint32_t u = g + Q::G * r;
       const uint32_t i = u >> hb, j = u & ((1u << hb) - 1);
       const uint32_t lo = (i << (hb + 1)) + j, hi = lo + (1u << hb);
-      const uint64_t L = x[lo];
-      const uint64_t t = q50_mulc(x[hi], tab[(1u << d) - 1 + i], q);
-      x[lo] = q50_add(L, t, q);
-      x[hi] = q50_sub(L, t, q);
+      const double w = tab[(1u << d) - 1 + i];
+#pragma unroll
+      for (int k = 0; k < NX; ++k) {
+        const double L = x[k][lo];
+        const double t = q50_mul(x[k][hi], w, q, qinv);
+        x[k][lo] = q50_add(L, t, q);
+        x[k][hi] = q50_sub(L, t, q);
+      }
     }
     __syncwarp();
   }
 }
 
 template <int LOG_N>
-LC_D void q50_inverse(uint64_t* x, const Shoup50* tab, uint32_t g, uint64_t q) {
+LC_D void q50_inverse_smem(double* x, const double* tab, uint32_t g, double q, double qinv) {
   using Q = Q50Geo<LOG_N>;
-  const Shoup50 inv2 = tab[kQ50Inv2];
+  const double inv2 = tab[kQ50Inv2];
 #pragma unroll
-  for (int d = LOG_N - 2; d >= 0; --d) {
+  for (int d = LOG_N - 2; d >= Q50Reg<LOG_N>::LEVELS; --d) {
     const int hb = LOG_N - 1 - d;
 #pragma unroll
     for (int r = 0; r < Q::BPT; ++r) {
       const uint32_t u = g + Q::G * r;
       const uint32_t i = u >> hb, j = u & ((1u << hb) - 1);
       const uint32_t lo = (i << (hb + 1)) + j, hi = lo + (1u << hb);
-      const uint64_t L = x[lo], H = x[hi];
-      x[lo] = q50_mulc(q50_add(L, H, q), inv2, q);
-      x[hi] = q50_mulc(q50_sub(L, H, q), tab[kQ50Inv + (1u << d) - 1 + i], q);
+      const double L = x[lo], H = x[hi];
+      x[lo] = q50_mul(q50_add(L, H, q), inv2, q, qinv);
+      x[hi] = q50_mul(q50_sub(L, H, q), tab[kQ50Inv + (1u << d) - 1 + i], q, qinv);
     }
     __syncwarp();
   }
@@ -138,17 +183,16 @@ LC_D void q50_inverse(uint64_t* x, const Shoup50* tab, uint32_t g, uint64_t q) {
 
 // x <- x (*) y slotwise: (u0 + u1 X)(v0 + v1 X) mod (X^2 - gamma_p)
 template <int LOG_N>
-LC_D void q50_slotwise(uint64_t* x, const uint64_t* y, const Shoup50* tab, uint32_t g, uint64_t q,
-                       uint64_t mu) {
+LC_D void q50_slotwise(double* x, const double* y, const double* tab, uint32_t g, double q, double qinv) {
   using Q = Q50Geo<LOG_N>;
 #pragma unroll
   for (int r = 0; r < Q::BPT; ++r) {
     const uint32_t p = g + Q::G * r;
-    const uint64_t u0 = x[2 * p], u1 = x[2 * p + 1], v0 = y[2 * p], v1 = y[2 * p + 1];
-    const uint64_t p0 = q50_mul(u0, v0, q, mu);
-    const uint64_t p1 = q50_mul(u1, v1, q, mu);
-    const uint64_t cross = q50_mul(q50_add(u0, u1, q), q50_add(v0, v1, q), q, mu);
-    x[2 * p] = q50_add(p0, q50_mulc(p1, tab[kQ50Gamma + p], q), q);
+    const double u0 = x[2 * p], u1 = x[2 * p + 1], v0 = y[2 * p], v1 = y[2 * p + 1];
+    const double p0 = q50_mul(u0, v0, q, qinv);
+    const double p1 = q50_mul(u1, v1, q, qinv);
+    const double cross = q50_mul(q50_add(u0, u1, q), q50_add(v0, v1, q), q, qinv);
+    x[2 * p] = q50_add(p0, q50_mul(p1, tab[kQ50Gamma + p], q, qinv), q);
     x[2 * p + 1] = q50_sub(cross, q50_add(p0, p1, q), q);
   }
   __syncwarp();
@@ -159,42 +203,61 @@ constexpr int kQ50Warps = 8;
 template <int LOG_N, int OP>
 __global__ void __launch_bounds__(kQ50Warps * 32) quad50_kernel(const __grid_constant__ Q50Params p) {
   using Q = Q50Geo<LOG_N>;
+  constexpr int E = Q50Reg<LOG_N>::E;
   constexpr bool TWO = OP == kQ50Slot || OP == kQ50Mul;
-  __shared__ Shoup50 s_tab[kQ50Tab];
-  __shared__ __align__(16) uint64_t s_a[kQ50Warps][Q::WE];
-  __shared__ __align__(16) uint64_t s_b[kQ50Warps][TWO ? Q::WE : 1];
+  __shared__ double s_tab[kQ50Tab];
+  __shared__ __align__(16) double s_a[kQ50Warps][Q::WE];
+  __shared__ __align__(16) double s_b[kQ50Warps][TWO ? Q::WE : 1];
   for (int e = threadIdx.x; e < kQ50Tab; e += blockDim.x) s_tab[e] = p.tab[e];
   __syncthreads();
   const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   const uint32_t g = lane % Q::G, poly = lane / Q::G;
   const size_t total = p.count * Q::N;
   const size_t tasks = (p.count + Q::PW - 1) / Q::PW;
-  uint64_t* xa = s_a[warp];
-  uint64_t* xb = s_b[warp];
+  double* xa = s_a[warp];
+  double* xb = s_b[warp];
+  const double q = p.q, qinv = p.qinv;
   for (size_t task = (size_t)blockIdx.x * kQ50Warps + warp; task < tasks; task += (size_t)gridDim.x * kQ50Warps) {
     const size_t base = task * Q::WE;
     const uint32_t valid = total - base < (size_t)Q::WE ? (uint32_t)(total - base) : (uint32_t)Q::WE;
+    double va[E], vb[E];
 #pragma unroll
-    for (uint32_t e = lane; e < (uint32_t)Q::WE; e += 32) {
-      xa[e] = e < valid ? p.a[base + e] : 0;  // plain loads: out may alias a or b
-      if (TWO) xb[e] = e < valid ? p.b[base + e] : 0;
+    for (int r = 0; r < E; ++r) {
+      // plain loads (out may alias a or b); residues < 2^50 convert exactly
+      const uint32_t e = lane + 32 * r;
+      va[r] = e < valid ? __ull2double_rn(p.a[base + e]) : 0.0;
+      if (TWO) vb[r] = e < valid ? __ull2double_rn(p.b[base + e]) : 0.0;
+    }
+    if (OP == kQ50Fwd || OP == kQ50Mul) q50_forward_regs<LOG_N>(va, s_tab, q, qinv);
+    if (OP == kQ50Mul) q50_forward_regs<LOG_N>(vb, s_tab, q, qinv);
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+      xa[lane + 32 * r] = va[r];
+      if (TWO) xb[lane + 32 * r] = vb[r];
     }
     __syncwarp();
-    uint64_t* x = xa + poly * Q::N;
-    if (OP == kQ50Fwd) q50_forward<LOG_N>(x, s_tab, g, p.q);
-    if (OP == kQ50Inv_) q50_inverse<LOG_N>(x, s_tab, g, p.q);
-    if (OP == kQ50Slot) q50_slotwise<LOG_N>(x, xb + poly * Q::N, s_tab, g, p.q, p.mu);
+    double* x = xa + poly * Q::N;
+    double* y = xb + poly * Q::N;
+    if (OP == kQ50Fwd) {
+      double* const xs[1] = {x};
+      q50_forward_smem<LOG_N, 1>(xs, s_tab, g, q, qinv);
+    }
+    if (OP == kQ50Inv_) q50_inverse_smem<LOG_N>(x, s_tab, g, q, qinv);
+    if (OP == kQ50Slot) q50_slotwise<LOG_N>(x, y, s_tab, g, q, qinv);
     if (OP == kQ50Mul) {
-      uint64_t* y = xb + poly * Q::N;
-      q50_forward<LOG_N>(x, s_tab, g, p.q);
-      q50_forward<LOG_N>(y, s_tab, g, p.q);
-      q50_slotwise<LOG_N>(x, y, s_tab, g, p.q, p.mu);
-      q50_inverse<LOG_N>(x, s_tab, g, p.q);
+      double* const xs[2] = {x, y};
+      q50_forward_smem<LOG_N, 2>(xs, s_tab, g, q, qinv);
+      q50_slotwise<LOG_N>(x, y, s_tab, g, q, qinv);
+      q50_inverse_smem<LOG_N>(x, s_tab, g, q, qinv);
     }
-    __syncwarp();
 #pragma unroll
-    for (uint32_t e = lane; e < (uint32_t)Q::WE; e += 32)
-      if (e < valid) p.out[base + e] = xa[e];
+    for (int r = 0; r < E; ++r) va[r] = xa[lane + 32 * r];
+    if (OP == kQ50Inv_ || OP == kQ50Mul) q50_inverse_regs<LOG_N>(va, s_tab, q, qinv);
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+      const uint32_t e = lane + 32 * r;
+      if (e < valid) p.out[base + e] = __double2ull_rn(va[r]);
+    }
     __syncwarp();
   }
 }
@@ -203,7 +266,7 @@ template <int LOG_N, int OP>
 static int q50_launch(const lc_quad50_plan* plan, const uint64_t* a, const uint64_t* b, uint64_t* out,
                       size_t count, cudaStream_t st) {
   using Q = Q50Geo<LOG_N>;
-  Q50Params p{a, b, out, count, plan->q, plan->mu, plan->d_tab};
+  Q50Params p{a, b, out, count, (double)plan->q, 1.0 / (double)plan->q, plan->d_tab};
   const size_t tasks = (count + Q::PW - 1) / Q::PW;
   const size_t want = (tasks + kQ50Warps - 1) / kQ50Warps;
   const size_t cap = (size_t)std::max(1, device_sm_count()) * 8;
@@ -254,8 +317,6 @@ static uint64_t hpow(uint64_t b, uint64_t e, uint64_t q) {
   return acc;
 }
 
-static Shoup50 shoup(uint64_t w, uint64_t q) { return Shoup50{w, (uint64_t)(((u128)w << 64) / q)}; }
-
 static uint32_t rev_bits(uint32_t x, uint32_t bits) {
   uint32_t r = 0;
   for (uint32_t b = 0; b < bits; ++b) r |= ((x >> b) & 1u) << (bits - 1 - b);
@@ -279,7 +340,6 @@ LC_API int lc_quad50_plan_create(uint64_t q, uint32_t two_adicity, uint64_t gene
   lc_quad50_plan* p = new (std::nothrow) lc_quad50_plan();
   if (!p) return LC_ERR_OUT_OF_MEMORY;
   p->q = q;
-  p->mu = (uint64_t)(((u128)1 << 100) / q);
   p->zeta = zeta;
   p->generator = generator;
   p->two_adicity = two_adicity;
@@ -289,15 +349,17 @@ LC_API int lc_quad50_plan_create(uint64_t q, uint32_t two_adicity, uint64_t gene
     for (uint32_t i = 0; i < (1u << d); ++i) {
       const uint64_t e = ((2 * (uint64_t)rev_bits(i, d) + 1) << (5 - d)) % 128;
       const uint64_t w = hpow(zeta, e, q);
-      p->tab[(1u << d) - 1 + i] = shoup(w, q);
-      p->tab[kQ50Inv + (1u << d) - 1 + i] = shoup(hmul(inv2, hpow(w, q - 2, q), q), q);
+      p->tab[(1u << d) - 1 + i] = w;
+      p->tab[kQ50Inv + (1u << d) - 1 + i] = hmul(inv2, hpow(w, q - 2, q), q);
     }
   }
   for (uint32_t s = 0; s < (1u << (log_n - 1)); ++s) {  // :291-296
     const uint64_t e = ((2 * (uint64_t)rev_bits(s, log_n - 1) + 1) << (7 - log_n)) % 128;
-    p->tab[kQ50Gamma + s] = shoup(hpow(zeta, e, q), q);
+    p->tab[kQ50Gamma + s] = hpow(zeta, e, q);
   }
-  p->tab[kQ50Inv2] = shoup(inv2, q);
+  p->tab[kQ50Inv2] = inv2;
+  double dtab[kQ50Tab];
+  for (int i = 0; i < kQ50Tab; ++i) dtab[i] = (double)p->tab[i];  // < 2^50: exact
   if (device_sm_count() <= 0) {
     delete p;
     return LC_ERR_NO_DEVICE;
@@ -307,7 +369,7 @@ LC_API int lc_quad50_plan_create(uint64_t q, uint32_t two_adicity, uint64_t gene
     delete p;
     return LC_ERR_OUT_OF_MEMORY;
   }
-  cudaError_t e = cudaMemcpy(p->d_tab, p->tab, sizeof(p->tab), cudaMemcpyHostToDevice);
+  cudaError_t e = cudaMemcpy(p->d_tab, dtab, sizeof(dtab), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     cudaFree(p->d_tab);
     delete p;
@@ -328,7 +390,7 @@ LC_API int lc_quad50_plan_info(const lc_quad50_plan* plan, uint64_t* zeta, uint6
   if (!plan) return LC_ERR_INVALID_ARGUMENT;
   if (zeta) *zeta = plan->zeta;
   if (slot_constants)
-    for (uint32_t s = 0; s < (1u << (plan->log_n - 1)); ++s) slot_constants[s] = plan->tab[lc::kQ50Gamma + s].w;
+    for (uint32_t s = 0; s < (1u << (plan->log_n - 1)); ++s) slot_constants[s] = plan->tab[lc::kQ50Gamma + s];
   return LC_OK;
 }
 
