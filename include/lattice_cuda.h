@@ -397,6 +397,43 @@ LC_API int lc_quad50_mul(const lc_quad50_plan *plan, const uint64_t *a, const ui
 LC_API int lc_quad50_mul_host(lc_quad50_plan *plan, const uint64_t *a, const uint64_t *b, uint64_t *out,
                               size_t count);
 
+/* ---------------------------------------------------------------------------
+ * labinius Ajtai commitment over R_648 = Z_q[X]/(X^648 - X^324 + 1)
+ * (crates/lattice-labinius).  Limb primes: 3889, 9721, 17497, 19441 (fully
+ * splitting, params.rs:20-30) and 2917, 4861, 12637 (quadratic slots,
+ * params.rs:306-315); the first listed is the base limb.
+ *
+ * A key holds A: per limb nr = len_f162 / 4 rows of 648 transform-domain
+ * residues (CommitmentKey::a, key.rs:45-57), centered int16 on the host
+ * side.  len_f162 must be a positive multiple of 4 (at most 2^18) and no
+ * prime may repeat (key.rs:96-106), else LC_ERR_INVALID_ARGUMENT. */
+typedef struct lc_lb_key lc_lb_key;
+/* CommitmentKey::random (key.rs:94-137), bit-identical rows */
+LC_API int lc_lb_key_random(size_t len_f162, uint64_t seed, const uint16_t *primes, uint32_t limbs,
+                            lc_lb_key **out);
+/* a key from explicit centered rows a = [limbs][nr][648] (host) */
+LC_API int lc_lb_key_create(size_t len_f162, const uint16_t *primes, uint32_t limbs, const int16_t *a,
+                            lc_lb_key **out);
+LC_API void lc_lb_key_destroy(lc_lb_key *key);
+/* len_f162, limbs, primes[limbs] and the centered rows [limbs][nr][648] (host), each if non-null */
+LC_API int lc_lb_key_info(const lc_lb_key *key, size_t *len_f162, uint32_t *limbs, uint16_t *primes, int16_t *a);
+/* ntt_of (ring.rs:322-333) with limb `limb`'s prime: count elements [count][648] u32 (device) */
+LC_API int lc_lb_ntt(const lc_lb_key *key, uint32_t limb, const uint32_t *in, uint32_t *out, size_t count,
+                     lc_stream stream);
+/* CommitmentKey::commit_with (key.rs:237-474): witness = r * len_f162 F162
+ * elements as [..][3] u64 (device), r a power of two in [2, 2^15].  Outputs
+ * (device): raw = [limbs][r][648] u32 in [0, q) (AuxData::raw), matrix =
+ * [4][r][limbs][162] centered int16 (CommitmentMatrix::value[row][column]
+ * [modulus]), batches = [r * nr][648] u32, the base limb's transform of every
+ * lifted ring element (AuxData::batches), or null to skip it. */
+LC_API int lc_lb_commit(lc_lb_key *key, const uint64_t *witness, uint32_t r, uint32_t *raw, int16_t *matrix,
+                        uint32_t *batches, lc_stream stream);
+/* the same over host buffers, synchronous */
+LC_API int lc_lb_commit_host(lc_lb_key *key, const uint64_t *witness, uint32_t r, uint32_t *raw, int16_t *matrix,
+                             uint32_t *batches);
+/* random_elems (binfield.rs:177-189): n F162 elements [n][3] u64 into host memory */
+LC_API int lc_lb_random_elems(size_t n, uint64_t seed, uint64_t *out);
+
 /* Benchmark/test utility, no counterpart in the reference: fill `count`
  * elements of `out` (device) with the seeded counter-based synthetic stream
  * x_i = H(seed, stream, offset + i): kind 0 raw u64, 1 u32 residues mod q

@@ -117,6 +117,14 @@ def _declare(L):
         "lc_quad50_slotwise_mul": (i32, [P, P, P, P, sz, P]),
         "lc_quad50_mul": (i32, [P, P, P, P, sz, P]),
         "lc_quad50_mul_host": (i32, [P, P, P, P, sz]),
+        "lc_lb_key_random": (i32, [sz, C.c_uint64, P, u32, C.POINTER(P)]),
+        "lc_lb_key_create": (i32, [sz, P, u32, P, C.POINTER(P)]),
+        "lc_lb_key_destroy": (None, [P]),
+        "lc_lb_key_info": (i32, [P, P, P, P, P]),
+        "lc_lb_ntt": (i32, [P, u32, P, P, sz, P]),
+        "lc_lb_commit": (i32, [P, P, u32, P, P, P, P]),
+        "lc_lb_commit_host": (i32, [P, P, u32, P, P, P]),
+        "lc_lb_random_elems": (i32, [sz, C.c_uint64, P]),
     }
     optional = {
     }

@@ -138,6 +138,20 @@ def _declare(lib):
         "orc_quad50_slotwise_mul": (i32, [P, P, P, P, sz]),
         "orc_quad50_mul": (i32, [P, P, P, P, sz]),
         "orc_quad50_mul_batch": (i32, [P, P, P, P, sz, i32]),
+        "orc_lb_quadratic": (i32, [u32]),
+        "orc_lb_psi": (u32, [u32]),
+        "orc_lb_tables": (None, [P, P, P, P, P]),
+        "orc_lb_ntt": (None, [u32, P, P]),
+        "orc_lb_eval_at": (u32, [u32, P, u32]),
+        "orc_lb_eval_quad_at": (None, [u32, P, u32, P]),
+        "orc_lb_mul_mod_phi": (None, [u32, P, P, P]),
+        "orc_lb_mul_quad_slots": (None, [u32, P, P, P]),
+        "orc_lb_components": (None, [u32, P, P]),
+        "orc_lb_r162_from_coeffs": (None, [u32, P, P]),
+        "orc_lb_random_elems": (None, [sz, u64, P]),
+        "orc_lb_lift": (None, [P, sz, P]),
+        "orc_lb_key_random": (None, [sz, u64, P, sz, P]),
+        "orc_lb_commit": (i32, [P, P, sz, sz, P, sz, P, P, P, i32]),
         "orc_keccak_f1600": (None, [P]),
         "orc_sha3_256": (None, [P, sz, P]),
         "orc_shake256": (None, [P, sz, P, sz]),
@@ -527,6 +541,113 @@ class QuadSlotTables50:
         out = np.empty_like(a)
         lib().orc_quad50_mul_batch(C.byref(self.t), ptr(a), ptr(b), ptr(out), a.size // self.n, nthreads)
         return out
+
+
+# ----------------------------------------------------------------- labinius (R_648)
+
+LB_PRIMES_SPLIT = (3889, 9721, 17497, 19441)   # lattice-labinius/src/params.rs:27-30
+LB_PRIMES_QUAD = (2917, 4861, 12637)           # params.rs:308
+
+
+class lb:
+    """labinius restatement (oracle/labinius.c): transforms, decomposition, key, commit."""
+
+    N, N162 = 648, 162
+
+    @staticmethod
+    def quadratic(q):
+        return bool(lib().orc_lb_quadratic(q))
+
+    @staticmethod
+    def psi(q):
+        return lib().orc_lb_psi(q)
+
+    @staticmethod
+    def tables():
+        se = np.empty(648, np.uint16)
+        qse = np.empty(324, np.uint16)
+        p3 = np.empty(162, np.uint16)
+        s648 = np.empty((4, 162), np.uint16)
+        qcs = np.empty((2, 162), np.uint16)
+        lib().orc_lb_tables(ptr(se), ptr(qse), ptr(p3), ptr(s648), ptr(qcs))
+        return {"slot_exp": se, "quad_slot_exp": qse, "pow3_slot_exp": p3, "slot_648": s648,
+                "quad_class_slot": qcs}
+
+    @staticmethod
+    def ntt(q, a):
+        a = np.ascontiguousarray(a, dtype=np.uint32)
+        out = np.empty(648, np.uint32)
+        lib().orc_lb_ntt(q, ptr(a), ptr(out))
+        return out
+
+    @staticmethod
+    def eval_at(q, a, u):
+        return lib().orc_lb_eval_at(q, ptr(np.ascontiguousarray(a, dtype=np.uint32)), u)
+
+    @staticmethod
+    def eval_quad_at(q, a, u):
+        out = np.empty(2, np.uint32)
+        lib().orc_lb_eval_quad_at(q, ptr(np.ascontiguousarray(a, dtype=np.uint32)), u, ptr(out))
+        return tuple(int(x) for x in out)
+
+    @staticmethod
+    def mul_mod_phi(q, a, b):
+        out = np.empty(648, np.uint32)
+        lib().orc_lb_mul_mod_phi(q, ptr(np.ascontiguousarray(a, dtype=np.uint32)),
+                                 ptr(np.ascontiguousarray(b, dtype=np.uint32)), ptr(out))
+        return out
+
+    @staticmethod
+    def mul_quad_slots(q, a, b):
+        out = np.empty(648, np.uint32)
+        lib().orc_lb_mul_quad_slots(q, ptr(np.ascontiguousarray(a, dtype=np.uint32)),
+                                    ptr(np.ascontiguousarray(b, dtype=np.uint32)), ptr(out))
+        return out
+
+    @staticmethod
+    def components(q, y):
+        out = np.empty((4, 162), np.int16)
+        lib().orc_lb_components(q, ptr(np.ascontiguousarray(y, dtype=np.uint32)), ptr(out))
+        return out
+
+    @staticmethod
+    def r162_from_coeffs(q, c):
+        out = np.empty(162, np.int16)
+        lib().orc_lb_r162_from_coeffs(q, ptr(np.ascontiguousarray(c, dtype=np.int64)), ptr(out))
+        return out
+
+    @staticmethod
+    def random_elems(n, seed):
+        out = np.empty((n, 3), np.uint64)
+        lib().orc_lb_random_elems(n, seed, ptr(out))
+        return out
+
+    @staticmethod
+    def lift(elems, r):
+        out = np.empty(648, np.uint32)
+        lib().orc_lb_lift(ptr(np.ascontiguousarray(elems, dtype=np.uint64)), r, ptr(out))
+        return out
+
+    @staticmethod
+    def key_random(len_f162, seed, primes):
+        primes = np.ascontiguousarray(primes, dtype=np.uint32)
+        a = np.empty((primes.size, len_f162 // 4, 648), np.int16)
+        lib().orc_lb_key_random(len_f162, seed, ptr(primes), primes.size, ptr(a))
+        return a
+
+    @staticmethod
+    def commit(a, primes, len_f162, witness, r, batches=True, nthreads=0):
+        """commit_scalar: (raw [limbs][r][648], matrix [4][r][limbs][162], batches [r*nr][648])."""
+        primes = np.ascontiguousarray(primes, dtype=np.uint32)
+        a = np.ascontiguousarray(a, dtype=np.int16)
+        witness = np.ascontiguousarray(witness, dtype=np.uint64)
+        limbs, nr = primes.size, len_f162 // 4
+        raw = np.empty((limbs, r, 648), np.uint32)
+        mat = np.empty((4, r, limbs, 162), np.int16)
+        bat = np.empty((r * nr, 648), np.uint32) if batches else None
+        lib().orc_lb_commit(ptr(a), ptr(primes), limbs, len_f162, ptr(witness), r, ptr(raw), ptr(mat),
+                            ptr(bat) if batches else None, nthreads)
+        return raw, mat, bat
 
 
 # ----------------------------------------------------------------- hashing

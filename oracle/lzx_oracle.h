@@ -201,6 +201,27 @@ int orc_quad50_mul(const orc_quad50 *t, const uint64_t *a, const uint64_t *b, ui
 int orc_quad50_mul_batch(const orc_quad50 *t, const uint64_t *a, const uint64_t *b, uint64_t *out,
                          size_t count, int nthreads);
 
+/* ---------------- labinius commitment over R_648 (labinius.c) --------------
+ * (crates/lattice-labinius: params.rs, scalar.rs, ring.rs, binfield.rs, key.rs) */
+
+int orc_lb_quadratic(uint32_t q);
+uint32_t orc_lb_psi(uint32_t q); /* psi (order 1944) or psi' (order 972) */
+/* SLOT_EXP[648], QUAD_SLOT_EXP[324], POW3_SLOT_EXP[162], SLOT_648[4][162], QUAD_CLASS_SLOT[2][162] */
+void orc_lb_tables(uint16_t *slot_exp, uint16_t *quad_slot_exp, uint16_t *pow3_slot_exp, uint16_t *slot_648,
+                   uint16_t *quad_class_slot);
+void orc_lb_ntt(uint32_t q, const uint32_t *a, uint32_t *out);
+uint32_t orc_lb_eval_at(uint32_t q, const uint32_t *a, uint32_t u);
+void orc_lb_eval_quad_at(uint32_t q, const uint32_t *a, uint32_t u, uint32_t out[2]);
+void orc_lb_mul_mod_phi(uint32_t q, const uint32_t *a, const uint32_t *b, uint32_t *out);
+void orc_lb_mul_quad_slots(uint32_t q, const uint32_t *a, const uint32_t *b, uint32_t *out);
+void orc_lb_components(uint32_t q, const uint32_t *y, int16_t *out);
+void orc_lb_r162_from_coeffs(uint32_t q, const int64_t *c, int16_t *out);
+void orc_lb_random_elems(size_t n, uint64_t seed, uint64_t *out);
+void orc_lb_lift(const uint64_t *elems, size_t r, uint32_t *out);
+void orc_lb_key_random(size_t len_f162, uint64_t seed, const uint32_t *primes, size_t limbs, int16_t *a);
+int orc_lb_commit(const int16_t *a, const uint32_t *primes, size_t limbs, size_t len_f162, const uint64_t *witness,
+                  size_t r, uint32_t *raw, int16_t *matrix, uint32_t *batches, int nthreads);
+
 /* ---------------- Keccak / transcript (keccak.rs, transcript.rs) ---------- */
 
 void orc_keccak_f1600(uint64_t st[25]);
