@@ -61,7 +61,8 @@ def parse():
     ap.add_argument("--no-commit", action="store_true", help="skip the Ajtai commit measurement")
     ap.add_argument("--commit-only", action="store_true",
                     help="run only the commit measurement (1 GPU) and print its JSON object")
-    ap.add_argument("--only", choices=["commit", "fold", "single", "uneven", "keygen", "quad50"], default=None,
+    ap.add_argument("--only", choices=["commit", "fold", "single", "uneven", "keygen", "quad50", "labinius"],
+                    default=None,
                     help="run only one secondary measurement (1 GPU) and print its JSON object")
     ap.add_argument("--no-fold", action="store_true", help="skip the folding-step measurement")
     ap.add_argument("--fold-m", type=int, default=1 << 20, help="ring elements of the folding-step witness")
@@ -72,6 +73,9 @@ def parse():
     ap.add_argument("--uneven-steps", type=int, default=3)
     ap.add_argument("--uneven-profile", action="store_true",
                     help="run only the batch, untuned and without the one-by-one arm (for profilers)")
+    ap.add_argument("--labinius-log-len", type=int, default=18, help="log2 of the F162 witness length")
+    ap.add_argument("--labinius-log-cols", type=int, default=7, help="log2 of the column (chunk) count")
+    ap.add_argument("--labinius-steps", type=int, default=10)
     ap.add_argument("--quad50-count", type=int, default=1 << 20, help="ring products per quadratic-slot step")
     ap.add_argument("--quad50-steps", type=int, default=10)
     ap.add_argument("--commit-steps", type=int, default=5)
@@ -755,6 +759,97 @@ def bench_quad50(args, rank, max_over_ranks, barrier, world):
     return res
 
 
+# ------------------------------------------------------------------ labinius commitment
+
+# The reference's published AVX-512 and scalar timings of commit_with at this
+# shape (suite sizem: 2^18 F162 in 128 columns, moduli 3889 + 2917).
+LB_REF_MS = {"avx512": 84.8, "scalar": 3197.6}
+
+
+def bench_labinius(args, rank, max_over_ranks, barrier, world):
+    """CommitmentKey::commit at suite sizem: 2^18 F162 in 2^7 columns, limbs
+    3889 (split) + 2917 (quadratic), the base limb's transform kept (AuxData::batches)."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from lzx_b200 import _lib
+    from lzx_b200.labinius import CommitmentKey, Modulus, random_witness
+    L = _lib.lib()
+    n_f162, r = 1 << args.labinius_log_len, 1 << args.labinius_log_cols
+    len_f162 = n_f162 // r
+    nr = len_f162 // 4
+    limbs = [Modulus.Q3889_FS_S, Modulus.Q2917_Q_S]
+    key = CommitmentKey.random(len_f162, 7, limbs[0], limbs[1:])
+    w_host = random_witness(n_f162, rank_seed(42, rank))
+    w = torch.from_numpy(w_host.view(np.int64)).cuda()
+    raw = torch.empty((2, r, 648), dtype=torch.int32, device="cuda")
+    mat = torch.empty((4, r, 2, 162), dtype=torch.int16, device="cuda")
+    bat = torch.empty((r * nr, 648), dtype=torch.int32, device="cuda")
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    ptrs = [C.c_void_p(t.data_ptr()) for t in (w, raw, mat, bat)]
+
+    def run():
+        return L.lc_lb_commit(key.handle, ptrs[0], r, ptrs[1], ptrs[2], ptrs[3], st)
+    for _ in range(3):
+        _lib.check(run(), "lc_lb_commit")
+    K = args.labinius_steps
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    ev0.record()
+    for _ in range(K):
+        run()
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(ev0.elapsed_time(ev1) / K)
+    # algorithmic bytes: witness in, A rows once, raw + matrix + kept transform out
+    alg = n_f162 * 24 + key.bytes() + 2 * r * 648 * 4 + 4 * r * 2 * 162 * 2 + r * nr * 648 * 4
+    peak, peak_kind = peaks()
+    achieved = alg / (ms / 1e3) / 1e9
+    res = {"workload": f"labinius CommitmentKey::commit, 2^{args.labinius_log_len} F162 in {r} columns, "
+                       f"limbs 3889 + 2917, base-limb transform kept",
+           "value": world / (ms / 1e3), "unit": "commitments/s", "ms_per_commit": ms,
+           "reference_published_ms": LB_REF_MS,
+           "speedup_vs_published_avx512": LB_REF_MS["avx512"] / ms if args.labinius_log_len == 18 and r == 128
+           else None,
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak, "algorithmic_bytes_per_launch": alg,
+                        "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
+           "gpu_launches": 2 * K}
+    # end to end through the host-buffer entry point (witness in, all outputs back)
+    hraw = np.empty((2, r, 648), np.uint32)
+    hmat = np.empty((4, r, 2, 162), np.int16)
+    hbat = np.empty((r * nr, 648), np.uint32)
+    hp = [x.ctypes.data_as(C.c_void_p) for x in (w_host, hraw, hmat, hbat)]
+    _lib.check(L.lc_lb_commit_host(key.handle, hp[0], r, hp[1], hp[2], hp[3]), "lc_lb_commit_host")
+    assert np.array_equal(hmat, mat.cpu().numpy())
+    t0 = time.perf_counter()
+    for _ in range(3):
+        L.lc_lb_commit_host(key.handle, hp[0], r, hp[1], hp[2], hp[3])
+    e2e_ms = (time.perf_counter() - t0) / 3 * 1e3
+    res["e2e"] = {"value": world / (e2e_ms / 1e3), "unit": "commitments/s", "ms_per_commit": e2e_ms,
+                  "h2d_bytes_per_step": n_f162 * 24,
+                  "d2h_bytes_per_step": hraw.nbytes + hmat.nbytes + hbat.nbytes,
+                  "api": "lc_lb_commit_host (synchronous, pageable host buffers)"}
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracle
+        oracle.prefer_native(True)
+        a = key.a
+        cols = 8
+        nt = host_threads()
+        t0 = time.perf_counter()
+        oraw, omat, _ = oracle.lb.commit(a, [3889, 2917], len_f162, w_host[: cols * len_f162], cols, nthreads=nt)
+        dt = time.perf_counter() - t0
+        assert np.array_equal(omat, mat.cpu().numpy()[:, :cols])
+        res["cpu_baseline"] = {"value": 1.0 / (dt * r / cols), "unit": "commitments/s", "cores": nt,
+                               "kind": "port",
+                               "sample": f"{cols} of {r} columns (oracle restatement of commit_scalar, "
+                                         f"{nt} threads), scaled to the full commitment"}
+    return res
+
+
 # ------------------------------------------------------------------ single commitment latency
 
 S_KAPPA, S_M = 8, 256
@@ -923,6 +1018,8 @@ def run_ours(args):
     torch.cuda.empty_cache()
     quad50 = bench_quad50(args, rank, max_over_ranks, barrier, world)
     torch.cuda.empty_cache()
+    labinius = bench_labinius(args, rank, max_over_ranks, barrier, world)
+    torch.cuda.empty_cache()
 
     ctx.close()
     if rank != 0:
@@ -982,6 +1079,7 @@ def run_ours(args):
         "key_from_seed": keygen,
         "single_commit": single,
         "quad_slot_mul": quad50,
+        "labinius_commit": labinius,
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -991,7 +1089,7 @@ def run_only(args, which):
     import torch
     torch.cuda.set_device(0)
     fn = {"commit": bench_commit, "fold": bench_fold, "single": bench_single, "uneven": bench_uneven,
-          "keygen": bench_keygen, "quad50": bench_quad50}[which]
+          "keygen": bench_keygen, "quad50": bench_quad50, "labinius": bench_labinius}[which]
     res = fn(args, 0, lambda x: x, lambda: None, 1)
     print(json.dumps(res), flush=True)
     return 0
