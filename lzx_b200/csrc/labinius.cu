@@ -211,54 +211,53 @@ static int ensure_maps() {
 
 // ------------------------------------------------------------------ device arithmetic
 
-LC_D uint32_t lb_add(uint32_t a, uint32_t b, uint32_t q) {
-  const uint32_t s = a + b;
-  return s >= q ? s - q : s;
-}
-LC_D uint32_t lb_sub(uint32_t a, uint32_t b, uint32_t q) { return a >= b ? a - b : a + q - b; }
-// x * w mod q, x < 2^32, w < q with ws = floor(w 2^32 / q): r in [0, 2q), one correction
-LC_D uint32_t lb_mulc(uint32_t x, uint32_t w, uint32_t ws, uint32_t q) {
-  const uint32_t r = x * w - __umulhi(x, ws) * q;
-  return r >= q ? r - q : r;
-}
+// x * w mod q, x < 2^32, w < q with ws = floor(w 2^32 / q): a representative in [0, 2q)
+LC_D uint32_t lb_mulc(uint32_t x, uint32_t w, uint32_t ws, uint32_t q) { return x * w - __umulhi(x, ws) * q; }
 
 struct LbTw {  // shared-memory copy of the limb's twiddles
   uint32_t tw[kLbTw], tws[kLbTw], tw2[kLbTw], tw2s[kLbTw];
 };
 
-// one radix-P level: NSUB sub-rings of degree DEG, twiddles at offset OFF
+// One radix-P level: NSUB sub-rings of degree DEG, twiddles at offset OFF.
+// Lazy: products are representatives in [0, 2q) and differences add 2q or 4q,
+// so a radix-2 level raises the bound on every value by 2q and a radix-3 level
+// by 4q; the transform's values stay below 24q < 2^20.
 template <int NSUB, int DEG, int P, int OFF>
 LC_D void lb_level(uint32_t* v, const LbTw& T, uint32_t q, uint32_t om, uint32_t oms, uint32_t lane) {
   constexpr int M = DEG / P, BF = NSUB * M;
+  const uint32_t q2 = 2 * q;
   for (int b = lane; b < BF; b += 32) {
     const int k = b / M, i = b - k * M, base = k * DEG;
     if (P == 2) {
       const uint32_t a0 = v[base + i];
       const uint32_t t = lb_mulc(v[base + M + i], T.tw[OFF + k], T.tws[OFF + k], q);
-      v[base + i] = lb_add(a0, t, q);
-      v[base + M + i] = lb_sub(a0, t, q);
+      v[base + i] = a0 + t;
+      v[base + M + i] = a0 + q2 - t;
     } else {
       // a0 + w t1 + w^2 t2 = a0 - t2 + w (t1 - t2) and a0 + w^2 t1 + w t2 = a0 - t1 - w (t1 - t2)
       const uint32_t a0 = v[base + i];
       const uint32_t t1 = lb_mulc(v[base + M + i], T.tw[OFF + k], T.tws[OFF + k], q);
       const uint32_t t2 = lb_mulc(v[base + 2 * M + i], T.tw2[OFF + k], T.tw2s[OFF + k], q);
-      const uint32_t u = lb_mulc(lb_sub(t1, t2, q), om, oms, q);
-      v[base + i] = lb_add(lb_add(a0, t1, q), t2, q);
-      v[base + M + i] = lb_add(lb_sub(a0, t2, q), u, q);
-      v[base + 2 * M + i] = lb_sub(lb_sub(a0, t1, q), u, q);
+      const uint32_t u = lb_mulc(t1 + q2 - t2, om, oms, q);
+      v[base + i] = a0 + t1 + t2;
+      v[base + M + i] = a0 + q2 - t2 + u;
+      v[base + 2 * M + i] = a0 + 2 * q2 - t1 - u;
     }
   }
   __syncwarp();
 }
 
-// the whole forward transform of one ring element in warp-private shared memory
+// The whole forward transform of one ring element in warp-private shared
+// memory, canonical residues out.  Inputs are canonical; BINARY inputs
+// (0/1 coefficients) take the Phi_6 split's product a1 * zeta6 as a select.
+template <bool BINARY>
 LC_D void lb_transform(uint32_t* v, const LbTw& T, const LbLimb& L, uint32_t lane) {
   const uint32_t q = L.q;
-  for (int i = lane; i < 324; i += 32) {  // Phi_6 split
+  for (int i = lane; i < 324; i += 32) {  // Phi_6 split: (a0 + t, a0 + a1 - t), t = zeta6 a1
     const uint32_t a0 = v[i], a1 = v[i + 324];
-    const uint32_t t = lb_mulc(a1, L.z6, L.z6s, q);
-    v[i] = lb_add(a0, t, q);
-    v[i + 324] = lb_sub(lb_add(a0, a1, q), t, q);
+    const uint32_t t = BINARY ? (a1 ? L.z6 : 0u) : lb_mulc(a1, L.z6, L.z6s, q);
+    v[i] = a0 + t;
+    v[i + 324] = a0 + a1 + 2 * q - t;
   }
   __syncwarp();
   if (L.quad) {
@@ -275,6 +274,13 @@ LC_D void lb_transform(uint32_t* v, const LbTw& T, const LbLimb& L, uint32_t lan
     lb_level<72, 9, 3, 38>(v, T, q, L.om, L.oms, lane);
     lb_level<216, 3, 3, 110>(v, T, q, L.om, L.oms, lane);
   }
+  // canonical: Barrett with floor(2^32 / q) leaves [0, 2q) for values < 2^20
+  const uint32_t bm = 0xFFFFFFFFu / q;
+  for (int x = lane; x < kLbN; x += 32) {
+    uint32_t r = v[x] - __umulhi(v[x], bm) * q;
+    v[x] = r >= q ? r - q : r;
+  }
+  __syncwarp();
 }
 
 struct LbCommitParams {
@@ -323,7 +329,7 @@ __global__ void __launch_bounds__(kLbWarps * 32) lb_commit_kernel(const __grid_c
       v[x] = (uint32_t)(w[3 * kk + (m >> 6)] >> (m & 63)) & 1u;
     }
     __syncwarp();
-    lb_transform(v, s_tw, L, lane);
+    lb_transform<true>(v, s_tw, L, lane);
     if (k == 0 && p.batches) {
       uint32_t* dst = p.batches + ((size_t)c * p.nr + i) * kLbN;
       for (int x = lane; x < kLbN; x += 32) dst[x] = v[x];
@@ -444,7 +450,7 @@ __global__ void __launch_bounds__(kLbWarps * 32)
   for (size_t i = (size_t)blockIdx.x * kLbWarps + warp; i < count; i += (size_t)gridDim.x * kLbWarps) {
     for (int x = lane; x < kLbN; x += 32) v[x] = in[i * kLbN + x] % L.q;
     __syncwarp();
-    lb_transform(v, s_tw, L, lane);
+    lb_transform<false>(v, s_tw, L, lane);
     for (int x = lane; x < kLbN; x += 32) out[i * kLbN + x] = v[x];
     __syncwarp();
   }
@@ -631,9 +637,11 @@ LC_API int lc_lb_commit(lc_lb_key* key, const uint64_t* witness, uint32_t r, uin
   if (r < 2 || (r & (r - 1)) || r > (1u << 15)) return LC_ERR_INVALID_ARGUMENT;  // key.rs:388-391
   const uint32_t nr = (uint32_t)key->nr;
   const int sms = std::max(1, device_sm_count());
-  // enough CTAs for about four per SM, at least 16 ring elements per CTA
-  uint32_t splits = (uint32_t)std::max<size_t>(1, (size_t)4 * sms / ((size_t)r * key->limbs));
-  splits = std::min<uint32_t>(splits, std::max<uint32_t>(1, nr / 16));
+  // at least 16 CTAs per SM when the problem allows, about 8 ring elements per
+  // warp (64 per CTA), so the last wave is a small fraction of the launch
+  uint32_t splits = (uint32_t)std::max<size_t>(1, (size_t)16 * sms / ((size_t)r * key->limbs));
+  splits = std::max<uint32_t>(splits, nr / (8 * kLbWarps));
+  splits = std::min<uint32_t>(splits, std::max<uint32_t>(1, nr / kLbWarps));
   const uint32_t per = (nr + splits - 1) / splits;
   splits = (nr + per - 1) / per;
   int rc = grow((void**)&key->d_partial, &key->partial_bytes, (size_t)key->limbs * r * splits * kLbN * 4);
