@@ -170,8 +170,15 @@ LC_D uint64_t gl_add(uint64_t a, uint64_t b) {
 
 LC_D uint64_t gl_sub(uint64_t a, uint64_t b) {
   uint64_t d = a - b;
-  if (a < b) d -= kGlEps;  // == d + p (mod 2^64)
-  return d;                // a, b < p  =>  result < p
+  if (a < b) d -= kGlEps;  // == d + p (mod 2^64); no second borrow for b < p
+  return d;                // a, b < p  =>  result < p; any a  =>  congruent, in [0, 2^64)
+}
+
+// a + b for any a and b < p: congruent, in [0, 2^64) -- a + b - 2^64 + eps = a + b - p < a
+LC_D uint64_t gl_add_lazy(uint64_t a, uint64_t b) {
+  uint64_t s = a + b;
+  if (s < b) s += kGlEps;
+  return s;
 }
 
 struct Goldilocks {
@@ -179,10 +186,13 @@ struct Goldilocks {
   using Tw = uint64_t;
 
   LC_D Goldilocks() {}
+  // Forward values are lazy (any u64 congruent to the canonical one): the
+  // product t = y * w is canonical, so x + t and x - t need one fold each,
+  // and fwd_final makes the output canonical.
   LC_D void fwd(uint64_t& x, uint64_t& y, Tw w) const {
-    uint64_t t = gl_mul(y, w);
-    uint64_t X = x;
-    x = gl_add(X, t);
+    const uint64_t t = gl_mul(y, w);
+    const uint64_t X = x;
+    x = gl_add_lazy(X, t);
     y = gl_sub(X, t);
   }
   LC_D void inv(uint64_t& x, uint64_t& y, Tw w) const {
@@ -198,7 +208,7 @@ struct Goldilocks {
     y = gl_mul(gl_sub(X, Y), wninv);
   }
   LC_D void scale(uint64_t& x, Tw c) const { x = gl_mul(x, c); }
-  LC_D uint64_t fwd_final(uint64_t x) const { return x; }
+  LC_D uint64_t fwd_final(uint64_t x) const { return gl_canon(x); }
   LC_D uint64_t inv_final(uint64_t x) const { return x; }
 };
 
