@@ -13,7 +13,8 @@
 //   2. product: a warp's item is (chunk of ring elements, slot t, block of 16
 //      jobs active at the chunk's start); each thread holds 2 rows x 4 jobs
 //      (160-bit accumulators) and streams the key's rows Ahat[t][j][..] --
-//      read once per lane of jobs, not once per job -- and the staircase;
+//      read once per lane of jobs, not once per job -- and the staircase,
+//      with the next 32 ring elements' rows prefetched into L2;
 //   3. finish: an item is one job: the sum over its chunks (mod q), then the
 //      inverse NTT of its kappa rows straight into the job's output.
 // A CTA claims `claim` items at a time from the phase's counter
@@ -87,10 +88,12 @@ struct SubJob {
 struct BatchParams {
   const LaneDesc* lanes;
   const SubJob* subs;
-  unsigned long long* counters;  // [3]
+  unsigned long long* counters;  // [4]: witness, Goldilocks products, finish, u32 products
   uint32_t* err;
   uint64_t total[3];
+  uint64_t prod_split;  // product items of the Goldilocks lanes (they come first)
   uint32_t nlanes, chunk, claim;
+  uint32_t lane_split;  // first lane of a u32 modulus
 };
 
 template <class A, int LOG_N, int LOG_V>
@@ -250,39 +253,59 @@ LC_D void product_warp_item(const LaneDesc& L, const SubJob* __restrict__ subs, 
     const uint32_t b = 4 * bq + u;
     nq[u] = b < L.nb ? subs[L.sub0 + b].n : 0;  // sorted: nq[0] >= nq[1] >= ...
   }
-  const uint32_t jend = min(j1, nq[0]);
+  // warp-uniform end: lanes 0-7 hold the block's first (longest) job, the
+  // other quads' shorter jobs are masked by j < nq[u]
+  const uint32_t jend = __shfl_sync(0xffffffffu, min(j1, nq[0]), 0);
   const E* A = reinterpret_cast<const E*>(L.ahat) + (size_t)t * L.a_m * kIPad + 2 * ip;
   const E* W = reinterpret_cast<const E*>(L.what) + (size_t)t * L.S + 4 * bq;
   const uint64_t* R = L.R;
+  // The staircase offsets of 32 ring elements arrive in one coalesced load and
+  // are broadcast by shuffles; the key and witness loads of JU ring elements
+  // issue together before their multiply-adds, so a warp keeps several
+  // independent loads in flight instead of one dependent pair per element.
+  constexpr int JU = sizeof(E) == 8 ? 2 : 4;
   Acc160 acc[2][4];
-  uint32_t j = j0;
-  for (; j + 2 <= jend; j += 2) {
-    const uint64_t r0 = __ldg(R + j), r1 = __ldg(R + j + 1);
-    E a[2][2], w[2][4];
-    load_pair<E>(A + (size_t)j * kIPad, a[0][0], a[0][1]);
-    load_pair<E>(A + (size_t)(j + 1) * kIPad, a[1][0], a[1][1]);
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      w[0][u] = j < nq[u] ? __ldg(W + r0 + u) : E(0);
-      w[1][u] = j + 1 < nq[u] ? __ldg(W + r1 + u) : E(0);
+  // Lane l also prefetches into L2 the key row and this block's 16 staircase
+  // entries of ring element jb + 32 + l, so the next block's loads hit L2.
+  const uint32_t b16 = 16 * blk;
+  for (uint32_t jb = j0; jb < jend; jb += 32) {
+    const uint32_t nj = min(32u, jend - jb);
+    const uint64_t rl = (uint32_t)lane < nj ? __ldg(R + jb + lane) : 0;
+    const uint32_t jp = jb + 32 + lane;
+    if (jp < jend) {
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(A - 2 * ip + (size_t)jp * kIPad));
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(W - 4 * bq + __ldg(R + jp) + b16));
     }
+    uint32_t s = 0;
+    for (; s + JU <= nj; s += JU) {
+      E a[JU][2], w[JU][4];
 #pragma unroll
-    for (int q = 0; q < 2; ++q)
+      for (int x = 0; x < JU; ++x) {
+        const uint32_t j = jb + s + x;
+        const uint64_t rj = __shfl_sync(0xffffffffu, rl, s + x);
+        load_pair<E>(A + (size_t)j * kIPad, a[x][0], a[x][1]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) w[x][u] = j < nq[u] ? __ldg(W + rj + u) : E(0);
+      }
+#pragma unroll
+      for (int x = 0; x < JU; ++x)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          mac<E>(acc[0][u], a[x][0], w[x][u]);
+          mac<E>(acc[1][u], a[x][1], w[x][u]);
+        }
+    }
+    for (; s < nj; ++s) {
+      const uint32_t j = jb + s;
+      const uint64_t rj = __shfl_sync(0xffffffffu, rl, s);
+      E a0, a1;
+      load_pair<E>(A + (size_t)j * kIPad, a0, a1);
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
-        mac<E>(acc[0][u], a[q][0], w[q][u]);
-        mac<E>(acc[1][u], a[q][1], w[q][u]);
+        const E wv = j < nq[u] ? __ldg(W + rj + u) : E(0);
+        mac<E>(acc[0][u], a0, wv);
+        mac<E>(acc[1][u], a1, wv);
       }
-  }
-  if (j < jend) {
-    const uint64_t r0 = __ldg(R + j);
-    E a0, a1;
-    load_pair<E>(A + (size_t)j * kIPad, a0, a1);
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const E wv = j < nq[u] ? __ldg(W + r0 + u) : E(0);
-      mac<E>(acc[0][u], a0, wv);
-      mac<E>(acc[1][u], a1, wv);
     }
   }
   // jobs active at j0 own a partial of this chunk (the finish launch reads
@@ -377,25 +400,29 @@ __global__ void __launch_bounds__(kBatchThreads, 2) batch_kernel(const __grid_co
   }
 }
 
-__global__ void __launch_bounds__(kBatchThreads) product_kernel(const __grid_constant__ BatchParams p) {
+// Products of one element type: the Goldilocks lanes' items [0, prod_split)
+// or the u32 lanes' items [prod_split, total), each launch with its own
+// counter, so neither carries the other's registers.
+template <class E>
+__global__ void __launch_bounds__(kBatchThreads, sizeof(E) == 8 ? 2 : 3)
+    product_kernel(const __grid_constant__ BatchParams p) {
+  constexpr bool WIDE = sizeof(E) == 8;
   const int lane = threadIdx.x & 31;
-  const uint64_t total = p.total[1];
-  uint32_t li = 0;
+  const uint64_t lo = WIDE ? 0 : p.prod_split, hi = WIDE ? p.prod_split : p.total[1];
+  unsigned long long* ctr = &p.counters[WIDE ? 1 : 3];
+  uint32_t li = WIDE ? 0 : p.lane_split;
   for (;;) {
     unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(&p.counters[1], (unsigned long long)p.claim);
+    if (lane == 0) base = atomicAdd(ctr, (unsigned long long)p.claim);
     base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= total) return;
-    const uint64_t end = min((uint64_t)base + p.claim, total);
-    for (uint64_t it = base; it < end; ++it) {
+    const uint64_t first = lo + base;
+    if (first >= hi) return;
+    const uint64_t end = min(first + p.claim, hi);
+    for (uint64_t it = first; it < end; ++it) {
       // a warp's claims only grow, so its lane index only moves forward
       while (li + 1 < p.nlanes && p.lanes[li + 1].item0[1] <= it) ++li;
       const LaneDesc& L = p.lanes[li];
-      const uint64_t k = it - L.item0[1];
-      if (L.kind == (uint32_t)PlanKind::Goldilocks)
-        product_warp_item<uint64_t>(L, p.subs, p.chunk, k);
-      else
-        product_warp_item<uint32_t>(L, p.subs, p.chunk, k);
+      product_warp_item<E>(L, p.subs, p.chunk, it - L.item0[1]);
     }
   }
 }
@@ -446,6 +473,8 @@ struct lc_batch {
   unsigned long long* d_counters = nullptr;
   uint32_t* d_err = nullptr;
   uint64_t total[3] = {0, 0, 0};
+  uint64_t prod_split = 0;  // product items of the Goldilocks lanes, which come first
+  uint32_t lane_split = 0;
   size_t smem[3] = {0, 0, 0};
   uint32_t chunk = 4096, ctas = 2, claim = 1;
   uint32_t flags = 0;
@@ -517,6 +546,14 @@ static int batch_layout(lc_batch* b) {
     }
   }
   for (int ph = 0; ph < 3; ++ph) b->total[ph] = base[ph];
+  b->lane_split = (uint32_t)b->lanes.size();
+  b->prod_split = b->total[1];
+  for (size_t l = 0; l < b->lanes.size(); ++l)
+    if (b->lanes[l].kind != (uint32_t)PlanKind::Goldilocks) {
+      b->lane_split = (uint32_t)l;
+      b->prod_split = b->lanes[l].item0[1];
+      break;
+    }
   if (cudaMemcpy(b->d_lanes, b->lanes.data(), b->lanes.size() * sizeof(LaneDesc), cudaMemcpyHostToDevice) !=
       cudaSuccess)
     return map_cuda(cudaGetLastError());
@@ -525,7 +562,7 @@ static int batch_layout(lc_batch* b) {
 }
 
 static int batch_launch(lc_batch* b, cudaStream_t st) {
-  cudaError_t e = cudaMemsetAsync(b->d_counters, 0, 3 * sizeof(unsigned long long), st);
+  cudaError_t e = cudaMemsetAsync(b->d_counters, 0, 4 * sizeof(unsigned long long), st);
   if (e != cudaSuccess) return map_cuda(e);
   BatchParams p{};
   p.lanes = b->d_lanes;
@@ -534,6 +571,8 @@ static int batch_launch(lc_batch* b, cudaStream_t st) {
   p.err = b->d_err;
   for (int ph = 0; ph < 3; ++ph) p.total[ph] = b->total[ph];
   p.nlanes = (uint32_t)b->lanes.size();
+  p.prod_split = b->prod_split;
+  p.lane_split = b->lane_split;
   p.chunk = b->chunk;
   p.claim = b->claim;
   const unsigned grid = (unsigned)std::max(1, device_sm_count()) * b->ctas;
@@ -542,7 +581,8 @@ static int batch_launch(lc_batch* b, cudaStream_t st) {
     if (e != cudaSuccess) return map_cuda(e);
   }
   batch_kernel<0><<<grid, kBatchThreads, b->smem[0], st>>>(p);
-  product_kernel<<<grid, kBatchThreads, 0, st>>>(p);
+  product_kernel<uint64_t><<<grid, kBatchThreads, 0, st>>>(p);
+  product_kernel<uint32_t><<<grid, kBatchThreads, 0, st>>>(p);
   batch_kernel<2><<<grid, kBatchThreads, b->smem[2], st>>>(p);
   return map_cuda(cudaGetLastError());
 }
@@ -587,7 +627,12 @@ LC_API int lc_batch_create(const lc_commit_class* classes, uint32_t num_classes,
   std::vector<size_t> r_off, ij_off;
   size_t what_bytes = 0, partial_bytes = 0;
   std::vector<size_t> what_off, part_off;
-  for (uint32_t c = 0; c < num_classes; ++c) {
+  // Goldilocks classes first, so each element type's product items are one range
+  std::vector<uint32_t> corder;
+  for (int pass = 0; pass < 2; ++pass)
+    for (uint32_t c = 0; c < num_classes; ++c)
+      if (classes[c].keys[0]->wide == (pass == 0)) corder.push_back(c);
+  for (uint32_t c : corder) {
     std::vector<uint32_t> idx;
     for (uint32_t i = 0; i < num_jobs; ++i)
       if (jobs[i].cls == c) idx.push_back(i);
@@ -662,7 +707,7 @@ LC_API int lc_batch_create(const lc_commit_class* classes, uint32_t num_classes,
       cudaMalloc(&b->d_itemj, std::max<size_t>(1, itemj_all.size()) * 4) != cudaSuccess ||
       cudaMalloc(&b->d_what, what_bytes + 256) != cudaSuccess ||  // + slack for 16-byte copy rounding
       cudaMalloc(&b->d_partial, std::max<size_t>(256, partial_bytes)) != cudaSuccess ||
-      cudaMalloc(&b->d_counters, 3 * sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&b->d_counters, 4 * sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&b->d_err, 4) != cudaSuccess) {
     cudaGetLastError();
     batch_free(b);
