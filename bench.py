@@ -921,7 +921,7 @@ def run_ours(args):
     from lzx_b200 import CRT_SET_30BIT, NttTables, _lib, synth
 
     ctx = RankContext("nccl", "cuda")
-    world, rank, dist = ctx.world, ctx.rank, ctx.dist
+    world, rank, local = ctx.world, ctx.rank, ctx.local
     barrier, max_over_ranks = ctx.barrier, ctx.max_over_ranks
 
     L = _lib.lib()

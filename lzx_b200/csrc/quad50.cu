@@ -200,8 +200,9 @@ LC_D void q50_slotwise(double* x, const double* y, const double* tab, uint32_t g
 
 constexpr int kQ50Warps = 8;
 
+// five CTAs per SM (48 registers, no spills): the kernel is latency-bound at four
 template <int LOG_N, int OP>
-__global__ void __launch_bounds__(kQ50Warps * 32) quad50_kernel(const __grid_constant__ Q50Params p) {
+__global__ void __launch_bounds__(kQ50Warps * 32, 5) quad50_kernel(const __grid_constant__ Q50Params p) {
   using Q = Q50Geo<LOG_N>;
   constexpr int E = Q50Reg<LOG_N>::E;
   constexpr bool TWO = OP == kQ50Slot || OP == kQ50Mul;
