@@ -818,11 +818,14 @@ def bench_labinius(args, rank, max_over_ranks, barrier, world):
                         "frac": achieved / peak, "algorithmic_bytes_per_launch": alg,
                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
            "gpu_launches": 2 * K}
-    # end to end through the host-buffer entry point (witness in, all outputs back)
-    hraw = np.empty((2, r, 648), np.uint32)
-    hmat = np.empty((4, r, 2, 162), np.int16)
-    hbat = np.empty((r * nr, 648), np.uint32)
-    hp = [x.ctypes.data_as(C.c_void_p) for x in (w_host, hraw, hmat, hbat)]
+    # end to end through the host-buffer entry point (witness in, all outputs
+    # back), pinned host buffers
+    pw = torch.from_numpy(w_host.view(np.int64)).pin_memory()
+    praw = torch.empty((2, r, 648), dtype=torch.int32).pin_memory()
+    pmat = torch.empty((4, r, 2, 162), dtype=torch.int16).pin_memory()
+    pbat = torch.empty((r * nr, 648), dtype=torch.int32).pin_memory()
+    hraw, hmat, hbat = praw.numpy(), pmat.numpy(), pbat.numpy()
+    hp = [C.c_void_p(x.data_ptr()) for x in (pw, praw, pmat, pbat)]
     _lib.check(L.lc_lb_commit_host(key.handle, hp[0], r, hp[1], hp[2], hp[3]), "lc_lb_commit_host")
     assert np.array_equal(hmat, mat.cpu().numpy())
     t0 = time.perf_counter()
@@ -832,7 +835,7 @@ def bench_labinius(args, rank, max_over_ranks, barrier, world):
     res["e2e"] = {"value": world / (e2e_ms / 1e3), "unit": "commitments/s", "ms_per_commit": e2e_ms,
                   "h2d_bytes_per_step": n_f162 * 24,
                   "d2h_bytes_per_step": hraw.nbytes + hmat.nbytes + hbat.nbytes,
-                  "api": "lc_lb_commit_host (synchronous, pageable host buffers)"}
+                  "api": "lc_lb_commit_host (synchronous, pinned host buffers)"}
     if rank == 0 and not args.no_cpu_baseline:
         import oracle
         oracle.prefer_native(True)
