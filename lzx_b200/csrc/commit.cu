@@ -805,6 +805,7 @@ LC_API void lc_ajtai_key_destroy(lc_ajtai_key* key) {
                   key->d_out, (void*)key->d_err})
     if (p) cudaFree(p);
   if (key->host_stream) cudaStreamDestroy(key->host_stream);
+  if (key->h_flags) cudaFreeHost(key->h_flags);
   if (key->plan) lc_ntt_plan_destroy(key->plan);
   tc_tables_destroy(key->tc);
   delete key;
@@ -903,6 +904,10 @@ static int commit_host(lc_ajtai_key* key, const void* s, size_t in_elem, size_t 
   if (rc) return rc;
   if (!key->host_stream && cudaStreamCreateWithFlags(&key->host_stream, cudaStreamNonBlocking) != cudaSuccess)
     return map_cuda(cudaGetLastError());
+  if (!key->h_flags && cudaMallocHost(&key->h_flags, 2 * sizeof(uint32_t)) != cudaSuccess) {
+    key->h_flags = nullptr;
+    return map_cuda(cudaGetLastError());
+  }
   cudaStream_t st = key->host_stream;
   if (cudaMemcpyAsync(key->d_in, s, in_bytes, cudaMemcpyHostToDevice, st) != cudaSuccess)
     return map_cuda(cudaGetLastError());
@@ -912,7 +917,18 @@ static int commit_host(lc_ajtai_key* key, const void* s, size_t in_elem, size_t 
   if (rc) return rc;
   if (cudaMemcpyAsync(out, key->d_out, out_bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess)
     return map_cuda(cudaGetLastError());
-  return lc_ajtai_key_check(key, st);
+  // both error words come back with the result: one synchronisation per call
+  cudaMemcpyAsync(key->h_flags, key->d_err, 4, cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(key->h_flags + 1, key->plan->d_err, 4, cudaMemcpyDeviceToHost, st);
+  const cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return map_cuda(e);
+  if (key->h_flags[0] | key->h_flags[1]) {
+    cudaMemsetAsync(key->d_err, 0, 4, st);
+    cudaMemsetAsync(key->plan->d_err, 0, 4, st);
+    cudaStreamSynchronize(st);
+    return LC_ERR_TIMEOUT;
+  }
+  return LC_OK;
 }
 
 LC_API int lc_ajtai_commit_host(lc_ajtai_key* key, const void* s, size_t batch, void* out) {

@@ -98,6 +98,7 @@ struct lc_ajtai_key {
   void* d_out = nullptr;
   size_t out_bytes = 0;
   cudaStream_t host_stream = nullptr;
+  uint32_t* h_flags = nullptr;  // pinned: the key's and the plan's error words (host API)
   uint32_t* d_err = nullptr;
   lc_tc_tables* tc = nullptr;  // tensor-core engine tables (LC_KEY_TENSOR_I8)
   int engine = LC_ENGINE_NTT;
