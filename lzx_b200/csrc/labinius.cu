@@ -642,6 +642,8 @@ LC_API int lc_lb_commit(lc_lb_key* key, const uint64_t* witness, uint32_t r, uin
   uint32_t splits = (uint32_t)std::max<size_t>(1, (size_t)16 * sms / ((size_t)r * key->limbs));
   splits = std::max<uint32_t>(splits, nr / (8 * kLbWarps));
   splits = std::min<uint32_t>(splits, std::max<uint32_t>(1, nr / kLbWarps));
+  // at most about 64 CTAs per SM in all: bounds the partial sums [limb][column][split][648]
+  splits = std::min<uint32_t>(splits, (uint32_t)std::max<size_t>(1, (size_t)64 * sms / ((size_t)r * key->limbs)));
   const uint32_t per = (nr + splits - 1) / splits;
   splits = (nr + per - 1) / per;
   int rc = grow((void**)&key->d_partial, &key->partial_bytes, (size_t)key->limbs * r * splits * kLbN * 4);
