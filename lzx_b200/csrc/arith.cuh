@@ -155,10 +155,53 @@ LC_D uint64_t gl_reduce128_lazy(uint64_t hi, uint64_t lo) {
 
 LC_D uint64_t gl_canon(uint64_t x) { return x >= kGlP ? x - kGlP : x; }
 
+// a * b mod p, canonical, for any a, b < 2^64: the 128-bit product from four
+// 32x32 partial products, then p3:p2:p1:p0 == (p1:p0) - p3 + p2 (2^32 - 1),
+// each wrap of 2^64 folded as 2^64 == 2^32 - 1, and r >= p  <=>  r + eps
+// carries out of 64 bits (that sum minus 2^64 is r - p).
 LC_D uint64_t gl_mul(uint64_t a, uint64_t b) {
-  uint64_t hi, lo;
-  mul64x64(a, b, hi, lo);
-  return gl_canon(gl_reduce128_lazy(hi, lo));
+  uint32_t r0, r1;
+  asm("{\n\t"
+      ".reg .u32 a0, a1, b0, b1, p0, p1, p2, p3, m, u0, u1, c, t0, t1, e;\n\t"
+      ".reg .pred q;\n\t"
+      "mov.b64 {a0, a1}, %2;\n\t"
+      "mov.b64 {b0, b1}, %3;\n\t"
+      "mov.u32 e, 0xFFFFFFFF;\n\t"
+      "mul.lo.u32 p0, a0, b0;\n\t"
+      "mul.hi.u32 p1, a0, b0;\n\t"
+      "mul.lo.u32 p2, a1, b1;\n\t"
+      "mul.hi.u32 p3, a1, b1;\n\t"
+      "mad.lo.cc.u32 p1, a0, b1, p1;\n\t"
+      "madc.hi.cc.u32 p2, a0, b1, p2;\n\t"
+      "addc.u32 p3, p3, 0;\n\t"
+      "mad.lo.cc.u32 p1, a1, b0, p1;\n\t"
+      "madc.hi.cc.u32 p2, a1, b0, p2;\n\t"
+      "addc.u32 p3, p3, 0;\n\t"
+      // (p1:p0) - p3; a borrow wrapped by +2^64, so subtract eps
+      "sub.cc.u32 p0, p0, p3;\n\t"
+      "subc.cc.u32 p1, p1, 0;\n\t"
+      "subc.u32 m, 0, 0;\n\t"
+      "sub.cc.u32 p0, p0, m;\n\t"
+      "subc.u32 p1, p1, 0;\n\t"
+      // + p2 * 2^32 - p2; a carry lost 2^64, so add eps
+      "sub.cc.u32 u0, 0, p2;\n\t"
+      "subc.u32 u1, p2, 0;\n\t"
+      "add.cc.u32 p0, p0, u0;\n\t"
+      "addc.cc.u32 p1, p1, u1;\n\t"
+      "addc.u32 c, 0, 0;\n\t"
+      "mad.lo.cc.u32 p0, c, e, p0;\n\t"
+      "addc.u32 p1, p1, 0;\n\t"
+      // canonical
+      "add.cc.u32 t0, p0, e;\n\t"
+      "addc.cc.u32 t1, p1, 0;\n\t"
+      "addc.u32 c, 0, 0;\n\t"
+      "setp.ne.u32 q, c, 0;\n\t"
+      "selp.b32 %0, t0, p0, q;\n\t"
+      "selp.b32 %1, t1, p1, q;\n\t"
+      "}"
+      : "=r"(r0), "=r"(r1)
+      : "l"(a), "l"(b));
+  return ((uint64_t)r1 << 32) | r0;
 }
 
 // Canonical inputs -> canonical output.
@@ -176,9 +219,40 @@ LC_D uint64_t gl_sub(uint64_t a, uint64_t b) {
 
 // a + b for any a and b < p: congruent, in [0, 2^64) -- a + b - 2^64 + eps = a + b - p < a
 LC_D uint64_t gl_add_lazy(uint64_t a, uint64_t b) {
-  uint64_t s = a + b;
-  if (s < b) s += kGlEps;
-  return s;
+  uint32_t r0, r1;
+  asm("{\n\t"
+      ".reg .u32 a0, a1, b0, b1, c, e;\n\t"
+      "mov.b64 {a0, a1}, %2;\n\t"
+      "mov.b64 {b0, b1}, %3;\n\t"
+      "mov.u32 e, 0xFFFFFFFF;\n\t"
+      "add.cc.u32 %0, a0, b0;\n\t"
+      "addc.cc.u32 %1, a1, b1;\n\t"
+      "addc.u32 c, 0, 0;\n\t"
+      "mad.lo.cc.u32 %0, c, e, %0;\n\t"
+      "addc.u32 %1, %1, 0;\n\t"
+      "}"
+      : "=r"(r0), "=r"(r1)
+      : "l"(a), "l"(b));
+  return ((uint64_t)r1 << 32) | r0;
+}
+
+// a - b for any a and b < p: congruent, in [0, 2^64) (a borrow wrapped by
+// +2^64 == eps, so eps is taken off again; that cannot borrow for b < p)
+LC_D uint64_t gl_sub_lazy(uint64_t a, uint64_t b) {
+  uint32_t r0, r1;
+  asm("{\n\t"
+      ".reg .u32 a0, a1, b0, b1, m;\n\t"
+      "mov.b64 {a0, a1}, %2;\n\t"
+      "mov.b64 {b0, b1}, %3;\n\t"
+      "sub.cc.u32 %0, a0, b0;\n\t"
+      "subc.cc.u32 %1, a1, b1;\n\t"
+      "subc.u32 m, 0, 0;\n\t"
+      "sub.cc.u32 %0, %0, m;\n\t"
+      "subc.u32 %1, %1, 0;\n\t"
+      "}"
+      : "=r"(r0), "=r"(r1)
+      : "l"(a), "l"(b));
+  return ((uint64_t)r1 << 32) | r0;
 }
 
 struct Goldilocks {
@@ -193,7 +267,7 @@ struct Goldilocks {
     const uint64_t t = gl_mul(y, w);
     const uint64_t X = x;
     x = gl_add_lazy(X, t);
-    y = gl_sub(X, t);
+    y = gl_sub_lazy(X, t);
   }
   LC_D void inv(uint64_t& x, uint64_t& y, Tw w) const {
     uint64_t X = x, Y = y;
