@@ -105,11 +105,12 @@ struct BCfg {
   static constexpr int GROUPS = kBatchThreads / G::T;
   static constexpr int SS = BatchSlotStride<A, LOG_N>::value;
   // polynomials per thread group in a witness item: as many as keep the
-  // item's slots within 80 KB (a few per group amortise the item's fixed
-  // costs: counter claim, twiddles, four barriers)
+  // item's slots within 72 KB (a few per group amortise the item's fixed
+  // costs: counter claim, twiddles, four barriers), so three witness CTAs
+  // fit in an SM's shared memory
   static constexpr size_t POLY_BYTES = (size_t)SS * sizeof(T);
-  static constexpr int IT = (size_t)GROUPS * 4 * POLY_BYTES <= 80 * 1024   ? 4
-                            : (size_t)GROUPS * 2 * POLY_BYTES <= 80 * 1024 ? 2
+  static constexpr int IT = (size_t)GROUPS * 4 * POLY_BYTES <= 72 * 1024   ? 4
+                            : (size_t)GROUPS * 2 * POLY_BYTES <= 72 * 1024 ? 2
                                                                            : 1;
   static constexpr int PB = GROUPS * IT;  // polynomials per witness item
   static constexpr int TWE = G::fwd_entries() > G::inv_entries() ? G::fwd_entries() : G::inv_entries();
@@ -379,8 +380,9 @@ LC_D void run_item(const BatchParams& p, const LaneDesc& L, uint64_t k, unsigned
 #undef LC_BATCH_CASE
 }
 
+// the witness launch at three CTAs per SM (79 registers, no spills)
 template <int PHASE>
-__global__ void __launch_bounds__(kBatchThreads, 2) batch_kernel(const __grid_constant__ BatchParams p) {
+__global__ void __launch_bounds__(kBatchThreads, PHASE == 0 ? 3 : 2) batch_kernel(const __grid_constant__ BatchParams p) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ unsigned long long s_base;
   const uint64_t total = p.total[PHASE];
