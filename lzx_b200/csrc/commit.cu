@@ -510,6 +510,15 @@ static int witness_ntt_as(lc_ajtai_key* key, const S* w, size_t batch, uint32_t 
 template <class S>
 static int witness_ntt(lc_ajtai_key* key, const S* w, size_t batch, uint32_t b_pad, cudaStream_t st) {
   const PlanKind kind = key->plan->kind;
+  if constexpr (std::is_same<S, int8_t>::value || std::is_same<S, uint8_t>::value) {
+    // d = 64 Goldilocks byte digits: the transform as exact INT8 tensor-core
+    // products when the shape allows (large problems), identical residues
+    if (kind == PlanKind::Goldilocks && key->log_n == 6) {
+      const int rc = tc_witness_ntt(w, std::is_same<S, int8_t>::value, batch, key->m, b_pad,
+                                    reinterpret_cast<uint64_t*>(key->d_what_t), key->d_err, st);
+      if (rc != LC_ERR_UNSUPPORTED) return rc;
+    }
+  }
   if constexpr (!std::is_same<S, uint32_t>::value) {
     if (kind == PlanKind::Goldilocks) return witness_ntt_as<Goldilocks, S>(key, w, batch, b_pad, st);
   }
@@ -761,6 +770,9 @@ LC_API int lc_ajtai_key_create_ex(const lc_ntt_plan* plan, uint32_t k, uint32_t 
   cudaMemset(key->d_err, 0, 4);
   cudaMemcpy(tmp, matrix, elems * eb, matrix_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice);
   // rotation-limb tables from the coefficient form (before it is transformed in place)
+  // the tensor-core witness transform's matrix image (once per device; a
+  // failure only leaves the CUDA-core transform in use)
+  if (plan->kind == PlanKind::Goldilocks && plan->log_n == 6) tc_ntt_prepare();
   if (flags & LC_KEY_TENSOR_I8) {
     rc = tc_tables_create(static_cast<const uint64_t*>(tmp), k, m, &key->tc);
     if (rc) {

@@ -121,4 +121,11 @@ int crt_residues(const lc_ntt_plan* plan, const uint64_t* z, size_t count, uint3
 // w: int8 digits (s8 = true) or unsigned byte digits (s8 = false)
 int tc_commit(lc_tc_tables* t, const void* w, bool s8, size_t batch, uint64_t* out, uint32_t* err,
               cudaStream_t st);
+// Goldilocks d = 64 witness NTT of byte digits on the INT8 tensor cores:
+// What_T[64][m][b_pad] from w[batch][m][64]; LC_ERR_UNSUPPORTED for shapes it
+// does not take (the caller then runs the CUDA-core transform).  The matrix
+// image is made by tc_ntt_prepare (once per device, outside stream capture).
+int tc_ntt_prepare();
+int tc_witness_ntt(const void* w, bool s8, size_t batch, uint32_t m, uint32_t b_pad, uint64_t* what_t,
+                   uint32_t* err, cudaStream_t st);
 }  // namespace lc

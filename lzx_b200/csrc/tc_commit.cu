@@ -38,6 +38,7 @@
 #include <algorithm>
 #include <mutex>
 #include <new>
+#include <vector>
 
 #include "../../include/lattice_cuda.h"
 #include "arith.cuh"
@@ -369,6 +370,219 @@ __global__ void tc_reduce_kernel(const int64_t* __restrict__ partial, uint64_t* 
   }
 }
 
+// ------------------------------------------------------------------ witness NTT on the tensor cores
+//
+// For d = 64 the forward transform of a digit vector w is a fixed matrix
+// product, What[t] = sum_c V[t][c] w[c] (mod p) with V[t][c] = psi^((2t+1)c)
+// (the natural-order negacyclic NTT, out[t] = w(psi^(2t+1))).  With the
+// residues V split into 8 byte limbs, D_l[r][t] = sum_c W[r][c] V_l[t][c] is
+// exact in int32 (64 * 128 * 255 < 2^21, u8 digits 64 * 255 * 255 < 2^22) and
+// What = sum_l 2^(8l) D_l (mod p).  An M = 128 tile holds BB witnesses x HB
+// segments of their ring elements (BB * HB = 128, read by a 3-D TMA view of
+// w[b][j][64] with the 128-byte swizzle, two ring elements per 128-byte row);
+// each ring element is four MMAs (two limb groups N = 256, K = 64 as two
+// K-steps) into all 512 TMEM columns.  Eight epilogue warps read the limbs
+// back, fold them (int64, then 128-bit plus p*2^16 to make it positive) and
+// reduce mod p, writing What_T[t][j][b] coalesced along b.
+constexpr int kTnSlots = 4;
+constexpr int kTnATile = 128 * 128;
+constexpr int kTnVTile = 256 * 128;
+constexpr int kTnOffV = kTnSlots * kTnATile;
+constexpr int kTnOffBar = kTnOffV + 2 * kTnVTile;
+constexpr size_t kTnSmem = 1024 + kTnOffBar + 256;
+constexpr int kTnThreads = 320;
+static_assert(kTnSmem <= 227 * 1024, "shared memory");
+
+struct TnParams {
+  const uint4* vimg;  // [2][256][128] bytes: the limb tiles in their swizzled shared-memory image
+  uint64_t* what_t;   // [64][m][b_pad]
+  uint32_t m, b_pad, batch, L, BB, HB, npairs;
+  uint64_t items;
+  uint32_t* err;
+};
+
+LC_D void tmem_ld8(uint32_t addr, uint32_t (&v)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+               : "r"(addr));
+}
+
+LC_D void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+          smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// sum_l 2^(8l) D_l mod p for one output (|D_l| < 2^22)
+LC_D uint64_t tn_fold(const uint32_t (&d)[8][8], int u) {
+  const int64_t e0 = (int64_t)(int32_t)d[0][u] + (int64_t)(int32_t)d[1][u] * 256 +
+                     (int64_t)(int32_t)d[2][u] * 65536 + (int64_t)(int32_t)d[3][u] * 16777216;
+  const int64_t e1 = (int64_t)(int32_t)d[4][u] + (int64_t)(int32_t)d[5][u] * 256 +
+                     (int64_t)(int32_t)d[6][u] * 65536 + (int64_t)(int32_t)d[7][u] * 16777216;
+  // |e0 + e1 2^32| < 2^79 < p 2^16
+  const __int128 v = (__int128)e1 * ((__int128)1 << 32) + e0 + ((__int128)kGlP << 16);
+  const uint64_t hi = (uint64_t)(v >> 64), lo = (uint64_t)v;  // hi < 2^17
+  const uint64_t t = hi * kGlEps;                              // hi 2^64 == hi (2^32 - 1)
+  uint64_t r = lo + t;
+  if (r < t) r += kGlEps;  // no second carry: lo + t - 2^64 < t < 2^49
+  return gl_canon(r);
+}
+
+template <bool S8>
+__global__ void __launch_bounds__(kTnThreads, 1)
+    tc_ntt_kernel(const __grid_constant__ CUtensorMap wmap, const __grid_constant__ TnParams p) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char* base =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + kTnOffBar);
+  uint64_t* loaded = bars;        // [4] A tile of a slot landed (tx bytes)
+  uint64_t* freed = bars + 4;     // [4] the MMAs that read a slot finished
+  uint64_t* acc_full = bars + 8;  // MMAs of a ring element finished
+  uint64_t* acc_empty = bars + 9; // 8 epilogue warps read TMEM
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 10);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 11);
+  uint64_t* all_done = bars + 12;  // final commit: every MMA issued has finished
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  if (tid == 0) {
+    for (int s = 0; s < kTnSlots; ++s) {
+      mbar_init(&loaded[s], 1);
+      mbar_init(&freed[s], 1);
+    }
+    mbar_init(acc_full, 1);
+    mbar_init(acc_empty, 8);
+    mbar_init(all_done, 1);
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 9) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(512));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  // the two limb-group tiles, already in their swizzled layout
+  uint4* vs = reinterpret_cast<uint4*>(base + kTnOffV);
+  for (int i = tid; i < 2 * kTnVTile / 16; i += kTnThreads) vs[i] = __ldg(p.vimg + i);
+  fence_proxy_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  const uint64_t n_my = p.items > blockIdx.x ? (p.items - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  auto a_slot = [&](uint64_t i) { return base + (i % kTnSlots) * kTnATile; };
+  auto fail = [&]() {
+    record_error(p.err, LC_DEVERR_TIMEOUT);
+    *abort_flag = 1;
+  };
+  int64_t last_loaded = -1;
+
+  if (warp == 8) {
+    // ---------------- TMA producer
+    if (lane == 0) {
+      for (uint64_t i = 0; i < n_my && !*abort_flag; ++i) {
+        if (i >= kTnSlots && !mbar_wait(&freed[i % kTnSlots], (uint32_t)(((i - kTnSlots) / kTnSlots) & 1))) {
+          fail();
+          break;
+        }
+        const uint64_t item = blockIdx.x + i * gridDim.x;
+        const uint32_t jp = (uint32_t)(item % p.npairs), bt = (uint32_t)(item / p.npairs);
+        mbar_arrive_expect_tx(&loaded[i % kTnSlots], kTnATile);
+        tma_load_3d(a_slot(i), &wmap, (int)(jp * 128), (int)(bt * p.BB), 0, &loaded[i % kTnSlots]);
+        last_loaded = (int64_t)i;
+      }
+    }
+  } else if (warp == 9) {
+    // ---------------- MMA issuer
+    if (lane == 0) {
+      uint64_t e = 0;  // ring elements issued
+      for (uint64_t i = 0; i < n_my && !*abort_flag; ++i) {
+        if (!mbar_wait(&loaded[i % kTnSlots], (uint32_t)((i / kTnSlots) & 1))) {
+          fail();
+          break;
+        }
+        bool ok = true;
+        for (int jj = 0; jj < 2 && ok; ++jj, ++e) {
+          if (e >= 1 && !mbar_wait(acc_empty, (uint32_t)((e - 1) & 1))) {
+            fail();
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t aa = smem_u32(a_slot(i)) + 64 * jj;
+#pragma unroll
+          for (int g = 0; g < 2; ++g) {
+            const uint32_t va = smem_u32(base + kTnOffV + g * kTnVTile);
+#pragma unroll
+            for (int ks = 0; ks < 2; ++ks)
+              mma_i8(tmem + g * 256, umma_desc_sw128(aa + 32 * ks), umma_desc_sw128(va + 32 * ks),
+                     TcIdesc<S8>::value, ks > 0 ? 1u : 0u);
+          }
+          mma_commit(acc_full);
+        }
+        if (!ok) break;
+        mma_commit(&freed[i % kTnSlots]);
+      }
+      mma_commit(all_done);
+      if (!mbar_wait(all_done, 0)) fail();
+    }
+  } else {
+    // ---------------- epilogue: warp w reads TMEM lanes 32 (w % 4).., slots 32 (w / 4)..
+    const uint32_t q = warp & 3, half = warp >> 2;
+    const uint32_t row = 32 * q + lane;
+    const uint32_t hh = row / p.BB, bb = row % p.BB;
+    uint64_t e = 0;
+    for (uint64_t i = 0; i < n_my; ++i) {
+      const uint64_t item = blockIdx.x + i * gridDim.x;
+      const uint32_t jp = (uint32_t)(item % p.npairs), bt = (uint32_t)(item / p.npairs);
+      const uint32_t b = bt * p.BB + bb;
+      bool stop = false;
+      for (int jj = 0; jj < 2; ++jj, ++e) {
+        if (*abort_flag || !mbar_wait(acc_full, (uint32_t)(e & 1))) {
+          fail();
+          stop = true;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t jl = 2 * jp + jj;
+        const bool valid = b < p.b_pad && jl < p.L;
+        const uint32_t j = hh * p.L + jl;
+#pragma unroll 1
+        for (int tb = 0; tb < 4; ++tb) {
+          const uint32_t t0 = 32 * half + 8 * tb;
+          uint32_t d[8][8];
+#pragma unroll
+          for (int l = 0; l < 8; ++l) tmem_ld8(tmem + ((32 * q) << 16) + (l >> 2) * 256 + (l & 3) * 64 + t0, d[l]);
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          if (valid) {
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+              p.what_t[((size_t)(t0 + u) * p.m + j) * p.b_pad + b] = tn_fold(d, u);
+          }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(acc_empty);
+      }
+      if (stop) break;
+    }
+  }
+  // ---------------- nothing in flight when TMEM and shared memory go
+  __syncthreads();
+  if (warp == 8 && lane == 0) {
+    for (int64_t i = last_loaded >= kTnSlots - 1 ? last_loaded - (kTnSlots - 1) : 0; i <= last_loaded; ++i)
+      mbar_wait(&loaded[i % kTnSlots], (uint32_t)((i / kTnSlots) & 1));
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 9) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+  }
+}
+
 // ------------------------------------------------------------------ host side
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -479,6 +693,105 @@ int tc_commit(lc_tc_tables* t, const void* w, bool s8, size_t batch, uint64_t* o
   const size_t total = (size_t)t->groups * btiles * 256 * 128;
   const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, (size_t)device_sm_count() * 16);
   tc_reduce_kernel<<<blocks, 256, 0, st>>>(t->partial, out, (uint32_t)batch, t->k, t->groups, splits, btiles);
+  return map_cuda(cudaGetLastError());
+}
+
+
+// The limb tiles of V in their shared-memory image: tile g, row n = 64 (l - 4g) + t,
+// 16-byte chunk c16 of the 128-byte row at n*128 + ((c16 ^ (n & 7)) << 4);
+// bytes 0..63 hold limb l of V[t][c], bytes 64..127 are zero.
+static void tn_build_image(std::vector<uint8_t>& img) {
+  img.assign(2 * kTnVTile, 0);
+  auto mulp = [](uint64_t a, uint64_t b) { return (uint64_t)((unsigned __int128)a * b % kGlP); };
+  auto powp = [&](uint64_t x, uint64_t e) {
+    uint64_t r = 1;
+    while (e) {
+      if (e & 1) r = mulp(r, x);
+      x = mulp(x, x);
+      e >>= 1;
+    }
+    return r;
+  };
+  const uint64_t psi = powp(7, (kGlP - 1) >> 7);  // primitive 128th root (generator 7)
+  for (int g = 0; g < 2; ++g)
+    for (int n = 0; n < 256; ++n) {
+      const int l = 4 * g + n / 64, t = n % 64;
+      for (int c = 0; c < 64; ++c) {
+        const uint64_t v = powp(psi, (uint64_t)((2 * t + 1) * c) % 128);
+        const int c16 = c / 16;
+        img[(size_t)g * kTnVTile + n * 128 + ((c16 ^ (n & 7)) << 4) + c % 16] = (uint8_t)(v >> (8 * l));
+      }
+    }
+}
+
+static std::mutex g_tn_mu;
+static uint4* g_tn_img[64] = {};
+
+int tc_ntt_prepare() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    return LC_ERR_CUDA;
+  }
+  std::lock_guard<std::mutex> lk(g_tn_mu);
+  if (g_tn_img[dev]) return LC_OK;
+  std::vector<uint8_t> img;
+  tn_build_image(img);
+  uint4* d = nullptr;
+  if (cudaMalloc(&d, img.size()) != cudaSuccess) {
+    cudaGetLastError();
+    return LC_ERR_OUT_OF_MEMORY;
+  }
+  if (cudaMemcpy(d, img.data(), img.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(d);
+    return LC_ERR_CUDA;
+  }
+  g_tn_img[dev] = d;
+  return LC_OK;
+}
+
+int tc_witness_ntt(const void* w, bool s8, size_t batch, uint32_t m, uint32_t b_pad, uint64_t* what_t,
+                   uint32_t* err, cudaStream_t st) {
+  if (batch == 0) return LC_OK;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    return LC_ERR_UNSUPPORTED;
+  }
+  const uint4* img = g_tn_img[dev];
+  EncodeTiledFn enc = encode_fn();
+  if (!img || !enc || (reinterpret_cast<uintptr_t>(w) & 15)) return LC_ERR_UNSUPPORTED;
+  if ((size_t)m * b_pad < ((size_t)1 << 16) || (size_t)m * 64 > 0x7FFFFFFF) return LC_ERR_UNSUPPORTED;
+  // M tile: BB witnesses x HB segments of m / HB ring elements
+  uint32_t BB;
+  if (b_pad % 128 == 0)
+    BB = 128;
+  else if (b_pad < 128 && (b_pad & (b_pad - 1)) == 0)
+    BB = b_pad;
+  else
+    return LC_ERR_UNSUPPORTED;
+  const uint32_t HB = 128 / BB;
+  if (m % HB) return LC_ERR_UNSUPPORTED;
+  const uint32_t L = m / HB, npairs = (L + 1) / 2;
+  const uint64_t items = (uint64_t)((b_pad + BB - 1) / BB) * npairs;
+  // w[b][j][64] as a 3-D byte array: x = 64 j_lo + c, y = b, z = segment; the
+  // rows past batch and the bytes past L*64 (odd L) read as zero
+  CUtensorMap map;
+  const cuuint64_t dims[3] = {(cuuint64_t)L * 64, (cuuint64_t)batch, (cuuint64_t)HB};
+  const cuuint64_t strides[2] = {(cuuint64_t)m * 64, (cuuint64_t)L * 64};
+  const cuuint32_t box[3] = {128, BB, HB};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult cr = enc(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(w), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (cr != CUDA_SUCCESS) return LC_ERR_UNSUPPORTED;
+  auto kern = s8 ? tc_ntt_kernel<true> : tc_ntt_kernel<false>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTnSmem);
+  if (e != cudaSuccess) return map_cuda(e);
+  const TnParams prm{img, what_t, m, b_pad, (uint32_t)batch, L, BB, HB, npairs, items, err};
+  const unsigned grid = (unsigned)std::min<uint64_t>(items, (uint64_t)std::max(1, device_sm_count()));
+  kern<<<grid, kTnThreads, kTnSmem, st>>>(map, prm);
   return map_cuda(cudaGetLastError());
 }
 

@@ -161,6 +161,27 @@ def test_goldilocks_batches_small_and_tiled(batch):
     assert np.array_equal(got[idx], oracle_gl_commit(A, kappa, m, W[idx]))
 
 
+@pytest.mark.parametrize("batch,m", [(8, 8192), (16, 4096), (32, 2048), (4, 16384), (1, 65536), (64, 1024),
+                                     (130, 512), (128, 513)])
+@pytest.mark.parametrize("digits", ["i8", "u8"])
+def test_goldilocks_byte_digit_transform_shapes(batch, m, digits):
+    """Shapes whose d = 64 witness transform runs as INT8 tensor-core products:
+    tiles of BB witnesses x 128/BB segments of their ring elements (BB = 128,
+    32, 16, 8, 4, 1), padded batches, an odd ring-element count per row."""
+    kappa = 2
+    A, key = gl_key(kappa, m, seed=batch + m)
+    if digits == "i8":
+        W = synth.synth_i8(9, batch, batch * m * 64).reshape(batch, m, 64)
+        Wo = W
+    else:
+        W = synth.synth_i8(9, batch, batch * m * 64).reshape(batch, m, 64).view(np.uint8)
+        Wo = W.astype(np.uint64)
+    got = key.commit(W)
+    for _ in range(2):  # repeated calls reuse the key's scratch
+        assert np.array_equal(key.commit(W), got)
+    assert np.array_equal(got, oracle_gl_commit(A, kappa, m, Wo))
+
+
 @pytest.mark.parametrize("log_d,kappa", [(5, 3), (7, 16), (8, 5), (9, 2)])
 def test_goldilocks_other_degrees(log_d, kappa):
     d, m, batch = 1 << log_d, 40, 130
