@@ -381,7 +381,7 @@ __global__ void tc_reduce_kernel(const int64_t* __restrict__ partial, uint64_t* 
 // segments of their ring elements (BB * HB = 128, read by a 3-D TMA view of
 // w[b][j][64] with the 128-byte swizzle, two ring elements per 128-byte row);
 // each ring element is four MMAs (two limb groups N = 256, K = 64 as two
-// K-steps) into all 512 TMEM columns.  Eight epilogue warps read the limbs
+// K-steps) into all 512 TMEM columns.  Sixteen epilogue warps read the limbs
 // back, fold them (int64, then 128-bit plus p*2^16 to make it positive) and
 // reduce mod p, writing What_T[t][j][b] coalesced along b.
 constexpr int kTnSlots = 4;
@@ -390,7 +390,8 @@ constexpr int kTnVTile = 256 * 128;
 constexpr int kTnOffV = kTnSlots * kTnATile;
 constexpr int kTnOffBar = kTnOffV + 2 * kTnVTile;
 constexpr size_t kTnSmem = 1024 + kTnOffBar + 256;
-constexpr int kTnThreads = 320;
+constexpr int kTnEpiWarps = 16;  // 4 per TMEM lane quarter, 16 slots each
+constexpr int kTnThreads = (kTnEpiWarps + 2) * 32;
 static_assert(kTnSmem <= 227 * 1024, "shared memory");
 
 struct TnParams {
@@ -440,7 +441,7 @@ __global__ void __launch_bounds__(kTnThreads, 1)
   uint64_t* loaded = bars;        // [4] A tile of a slot landed (tx bytes)
   uint64_t* freed = bars + 4;     // [4] the MMAs that read a slot finished
   uint64_t* acc_full = bars + 8;  // MMAs of a ring element finished
-  uint64_t* acc_empty = bars + 9; // 8 epilogue warps read TMEM
+  uint64_t* acc_empty = bars + 9; // the epilogue warps read TMEM
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 10);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 11);
   uint64_t* all_done = bars + 12;  // final commit: every MMA issued has finished
@@ -452,12 +453,13 @@ __global__ void __launch_bounds__(kTnThreads, 1)
       mbar_init(&freed[s], 1);
     }
     mbar_init(acc_full, 1);
-    mbar_init(acc_empty, 8);
+    mbar_init(acc_empty, kTnEpiWarps);
     mbar_init(all_done, 1);
     *abort_flag = 0;
     fence_mbar_init();
   }
-  if (warp == 9) {
+  constexpr int kTmaWarp = kTnEpiWarps, kMmaWarp = kTnEpiWarps + 1;
+  if (warp == kMmaWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"(512));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -479,7 +481,7 @@ __global__ void __launch_bounds__(kTnThreads, 1)
   };
   int64_t last_loaded = -1;
 
-  if (warp == 8) {
+  if (warp == kTmaWarp) {
     // ---------------- TMA producer
     if (lane == 0) {
       for (uint64_t i = 0; i < n_my && !*abort_flag; ++i) {
@@ -494,7 +496,7 @@ __global__ void __launch_bounds__(kTnThreads, 1)
         last_loaded = (int64_t)i;
       }
     }
-  } else if (warp == 9) {
+  } else if (warp == kMmaWarp) {
     // ---------------- MMA issuer
     if (lane == 0) {
       uint64_t e = 0;  // ring elements issued
@@ -529,8 +531,8 @@ __global__ void __launch_bounds__(kTnThreads, 1)
       if (!mbar_wait(all_done, 0)) fail();
     }
   } else {
-    // ---------------- epilogue: warp w reads TMEM lanes 32 (w % 4).., slots 32 (w / 4)..
-    const uint32_t q = warp & 3, half = warp >> 2;
+    // ---------------- epilogue: warp w reads TMEM lanes 32 (w % 4).., slots 16 (w / 4)..
+    const uint32_t q = warp & 3, part = warp >> 2;
     const uint32_t row = 32 * q + lane;
     const uint32_t hh = row / p.BB, bb = row % p.BB;
     uint64_t e = 0;
@@ -549,17 +551,19 @@ __global__ void __launch_bounds__(kTnThreads, 1)
         const uint32_t jl = 2 * jp + jj;
         const bool valid = b < p.b_pad && jl < p.L;
         const uint32_t j = hh * p.L + jl;
+        const size_t stride = (size_t)p.m * p.b_pad;  // one slot t
+        uint64_t* dst = p.what_t + (size_t)(16 * part) * stride + (size_t)j * p.b_pad + b;
 #pragma unroll 1
-        for (int tb = 0; tb < 4; ++tb) {
-          const uint32_t t0 = 32 * half + 8 * tb;
+        for (int tb = 0; tb < 2; ++tb) {
+          const uint32_t t0 = 16 * part + 8 * tb;
           uint32_t d[8][8];
 #pragma unroll
           for (int l = 0; l < 8; ++l) tmem_ld8(tmem + ((32 * q) << 16) + (l >> 2) * 256 + (l & 3) * 64 + t0, d[l]);
           asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-          if (valid) {
 #pragma unroll
-            for (int u = 0; u < 8; ++u)
-              p.what_t[((size_t)(t0 + u) * p.m + j) * p.b_pad + b] = tn_fold(d, u);
+          for (int u = 0; u < 8; ++u) {
+            if (valid) *dst = tn_fold(d, u);
+            dst += stride;
           }
         }
         tc_fence_before();
@@ -571,13 +575,13 @@ __global__ void __launch_bounds__(kTnThreads, 1)
   }
   // ---------------- nothing in flight when TMEM and shared memory go
   __syncthreads();
-  if (warp == 8 && lane == 0) {
+  if (warp == kTmaWarp && lane == 0) {
     for (int64_t i = last_loaded >= kTnSlots - 1 ? last_loaded - (kTnSlots - 1) : 0; i <= last_loaded; ++i)
       mbar_wait(&loaded[i % kTnSlots], (uint32_t)((i / kTnSlots) & 1));
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 9) {
+  if (warp == kMmaWarp) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
   }
