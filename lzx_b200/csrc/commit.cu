@@ -301,7 +301,9 @@ __global__ void __launch_bounds__(256)
 // Small-batch product for b_pad a multiple of 4: one thread per (split, t,
 // row pair, 4 witnesses), 8 accumulators, so each A pair and each witness
 // quad is loaded once per 8 multiply-adds.  Lanes run along the row pairs
-// (one 128-byte A row per slot), then the witness quads (broadcast loads).
+// (one 128-byte A row per slot), then the witness quads (broadcast loads);
+// both streams are prefetched into L2 16 ring elements ahead (the loop is
+// otherwise bound by DRAM latency).
 template <class E>
 __global__ void __launch_bounds__(256)
     mac_quad_kernel(const E* __restrict__ ahat_t, uint32_t am, const E* __restrict__ what_t, E* __restrict__ partial,
@@ -321,6 +323,11 @@ __global__ void __launch_bounds__(256)
     const E* wp = what_t + ((size_t)t * m + j0) * b_pad + 4 * bq;
 #pragma unroll 2
     for (uint32_t j = j0; j < j1; ++j) {
+      // both streams run along j: bring the rows 16 ring elements ahead into L2
+      if (j + 16 < j1) {
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(ap + 16 * kIPad));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(wp + (size_t)16 * b_pad));
+      }
       const E a0 = ap[0], a1 = ap[1];
       E wv[4];
 #pragma unroll
