@@ -87,7 +87,9 @@ LC_API int lc_ntt_plan_info(const lc_ntt_plan *plan, uint32_t *log_n, uint32_t *
 /* Tuning hook (no counterpart in the reference, which has no kernels): picks
  * one of the instantiated tile shapes / pipeline depths of this plan's
  * transform kernels, 0 = the default.  Results are identical for every
- * variant; only the speed changes.  LC_ERR_INVALID_ARGUMENT outside 0..4. */
+ * variant; only the speed changes.  LC_ERR_INVALID_ARGUMENT outside
+ * 0 .. LC_NTT_NUM_VARIANTS - 1. */
+#define LC_NTT_NUM_VARIANTS 7
 LC_API int lc_ntt_plan_set_variant(lc_ntt_plan *plan, int variant);
 
 /* Batched forward transform, device pointers.  Replaces

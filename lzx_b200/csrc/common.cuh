@@ -41,6 +41,10 @@ LC_D void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
                : "memory");
 }
 
+LC_D void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 // Returns true once the phase with the given parity has completed, false if
 // the spin bound expired first.
 LC_D bool mbar_wait(uint64_t* bar, uint32_t parity) {

@@ -133,10 +133,10 @@ int map_cuda(cudaError_t e) {
 
 // ---------------------------------------------------------------- launch
 
-template <class A, int LOG_N, int LOG_V, int NT, int IT, int STAGES, bool INV>
+template <class A, int LOG_N, int LOG_V, int NT, int IT, int STAGES, bool INV, int OPT = 0>
 static int launch_tile_cfg(const NttParams& p, cudaStream_t s) {
   using C = NttKernelCfg<A, LOG_N, LOG_V, NT, IT, STAGES, INV>;
-  auto kern = ntt_tile_kernel<A, LOG_N, LOG_V, NT, IT, STAGES, INV>;
+  auto kern = ntt_tile_kernel<A, LOG_N, LOG_V, NT, IT, STAGES, INV, OPT>;
   constexpr size_t smem = C::SMEM;
   static bool attr_done = false;
   if (!attr_done) {
@@ -203,13 +203,16 @@ static int launch_tile(const NttParams& p, int variant, cudaStream_t s) {
     (void)variant;
     return launch_tile_cfg<A, LOG_N, LOG_V, 128, default_it<A, LOG_N, LOG_V, 128>(), 2, INV>(p, s);
   } else {
-  // variant 0 is the tuned default; 1..4 are alternatives kept for the tuner
+  // variant 0 is the default; 1..6 are alternatives kept for the tuner
+  constexpr int IT1 = default_it<A, LOG_N, LOG_V, 128>();
   switch (variant) {
-    case 1: return launch_tile_cfg<A, LOG_N, LOG_V, 128, default_it<A, LOG_N, LOG_V, 128>(), 3, INV>(p, s);
+    case 1: return launch_tile_cfg<A, LOG_N, LOG_V, 128, IT1, 3, INV>(p, s);
     case 2: return launch_tile_cfg<A, LOG_N, LOG_V, 256, default_it<A, LOG_N, LOG_V, 256>(), 2, INV>(p, s);
     case 3: return launch_warp_cfg<A, LOG_N, LOG_V, 4, 1, 2, INV>(p, s);
     case 4: return launch_warp_cfg<A, LOG_N, LOG_V, 4, 1, 3, INV>(p, s);
-    default: return launch_tile_cfg<A, LOG_N, LOG_V, 128, default_it<A, LOG_N, LOG_V, 128>(), 2, INV>(p, s);
+    case 5: return launch_tile_cfg<A, LOG_N, LOG_V, 128, IT1, 2, INV, kOptSwz>(p, s);
+    case 6: return launch_tile_cfg<A, LOG_N, LOG_V, 128, IT1, 2, INV, kOptSwz | kOptRegTw>(p, s);
+    default: return launch_tile_cfg<A, LOG_N, LOG_V, 128, IT1, 2, INV>(p, s);
   }
   }
 }
@@ -437,7 +440,7 @@ LC_API void lc_ntt_plan_destroy(lc_ntt_plan* plan) {
 }
 
 LC_API int lc_ntt_plan_set_variant(lc_ntt_plan* plan, int variant) {
-  if (!plan || variant < 0 || variant > 4) return LC_ERR_INVALID_ARGUMENT;
+  if (!plan || variant < 0 || variant >= LC_NTT_NUM_VARIANTS) return LC_ERR_INVALID_ARGUMENT;
   plan->variant = variant;
   return LC_OK;
 }

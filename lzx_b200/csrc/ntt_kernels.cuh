@@ -137,16 +137,61 @@ struct NttKernelCfg {
   static_assert(STAGE_BYTES % 16 == 0, "stage alignment");
 };
 
+// Twiddles whose index includes the thread's lane bits (forward phase 1,
+// inverse phase 0), one set per thread for the whole kernel.  With
+// LOG_V == LOG_N - LOG_V there are V - 1 of them: level b holds
+// V >> (b + 1) entries, at register offset (V >> (b + 1)) - 1 (forward,
+// levels LO0-1 .. 0) or V - (V >> b) (inverse, levels 0 .. LOG_V-1).
+template <class A, int LOG_N, int LOG_V>
+struct LaneTw {
+  using G = Geo<LOG_N, LOG_V>;
+  static constexpr bool kHeld = G::LO0 == LOG_V;
+  typename A::Tw w[kHeld ? G::V - 1 : 1];
+};
+
+template <class A, int LOG_N, int LOG_V, bool INVERSE>
+LC_D void load_lane_tw(LaneTw<A, LOG_N, LOG_V>& lt, const typename A::Tw* tw, uint32_t t) {
+  using G = Geo<LOG_N, LOG_V>;
+  constexpr int V = G::V, TT = G::T;
+  static_assert(LaneTw<A, LOG_N, LOG_V>::kHeld, "register twiddles need LOG_V == LOG_N - LOG_V");
+#pragma unroll
+  for (int b = 0; b < LOG_V; ++b) {
+#pragma unroll
+    for (int j = 0; j < (V >> (b + 1)); ++j) {
+      if (!INVERSE)
+        lt.w[((V >> (b + 1)) - 1) + j] = tw[G::fwd_phase1_off(b) + j * TT + t];
+      else
+        lt.w[(V - (V >> b)) + j] = tw[G::inv_phase0_off(b) + j * TT + t];
+    }
+  }
+}
+
+// Transposing copy for u32 values, V = T = 16: element e = 16*row + col is
+// kept at row*16 + ((col>>2) ^ ((row>>1)&3))*4 + (col&3), an XOR swizzle of
+// the 16-byte chunks of each row.  Column accesses (16 lanes, one row) hit
+// 16 distinct banks; row accesses go as four 16-byte vector accesses, and
+// every quarter-warp of them covers 8 distinct chunk banks.
+LC_HD constexpr int swz16(int e) { return (e & ~12) | ((((e >> 2) & 3) ^ ((e >> 5) & 3)) << 2); }
+
+// Options of the transform: kOptRegTw takes the lane twiddles from `lt`
+// (registers); kOptSwz, for u32 values with V = T = 16, uses the swizzled
+// transposing copy with 16-byte vector accesses on its row side.
+enum : int { kOptRegTw = 1, kOptSwz = 2 };
+
 // One polynomial held by a group of T threads: the complete forward
 // (natural coefficients -> natural evaluations) or inverse transform of the
 // shared-memory slot, in place.
-template <class A, int LOG_N, int LOG_V, bool INVERSE>
-LC_D void transform_slot(typename A::T* slot, const typename A::Tw* tw, const A& ar, uint32_t t) {
+template <class A, int LOG_N, int LOG_V, bool INVERSE, int OPT>
+LC_D void transform_slot_x(typename A::T* slot, const typename A::Tw* tw, const A& ar, uint32_t t,
+                           const LaneTw<A, LOG_N, LOG_V>& lt) {
   using G = Geo<LOG_N, LOG_V>;
   using SL = Slots<A, LOG_N, LOG_V>;
   using T = typename A::T;
   using Tw = typename A::Tw;
   constexpr int V = G::V, LO0 = G::LO0, TT = G::T;
+  constexpr bool REGTW = (OPT & kOptRegTw) != 0;
+  constexpr bool SWZ = (OPT & kOptSwz) != 0 && sizeof(T) == 4 && LOG_V == 4 && LO0 == 4;
+  static_assert(!REGTW || LaneTw<A, LOG_N, LOG_V>::kHeld, "register twiddles need LOG_V == LOG_N - LOG_V");
   T v[V];
   if (!INVERSE) {
     // ---- phase 0: natural-order coefficients, register bits [LO0, LOG_N)
@@ -166,19 +211,38 @@ LC_D void transform_slot(typename A::T* slot, const typename A::Tw* tw, const A&
       }
     }
     __syncwarp();
+    if constexpr (SWZ) {
 #pragma unroll
-    for (int r = 0; r < V; ++r) slot[SL::padded((r << LO0) | t)] = v[r];
+      for (int r = 0; r < V; ++r) slot[swz16((r << LO0) | (int)t)] = v[r];
+    } else {
+#pragma unroll
+      for (int r = 0; r < V; ++r) slot[SL::padded((r << LO0) | t)] = v[r];
+    }
     __syncwarp();
     // ---- phase 1: register bits [0, LOG_V), levels b < LO0
+    if constexpr (SWZ) {
+      const uint32_t sx = (t >> 1) & 3u;
 #pragma unroll
-    for (int r = 0; r < V; ++r) v[r] = slot[SL::padded((t << LOG_V) | r)];
+      for (int c = 0; c < 4; ++c) {
+        const uint4 q4 = *reinterpret_cast<const uint4*>(slot + (t << 4) + ((c ^ sx) << 2));
+        v[4 * c] = q4.x;
+        v[4 * c + 1] = q4.y;
+        v[4 * c + 2] = q4.z;
+        v[4 * c + 3] = q4.w;
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < V; ++r) v[r] = slot[SL::padded((t << LOG_V) | r)];
+    }
 #pragma unroll
     for (int b = LO0 - 1; b >= 0; --b) {
       const int rb = 1 << b;
 #pragma unroll
       for (int r = 0; r < V; ++r) {
         if (r & rb) continue;
-        const Tw w = tw[G::fwd_phase1_off(b) + (r >> (b + 1)) * TT + t];
+        Tw w;
+        if constexpr (REGTW) w = lt.w[((V >> (b + 1)) - 1) + (r >> (b + 1))];
+        else w = tw[G::fwd_phase1_off(b) + (r >> (b + 1)) * TT + t];
         ar.fwd(v[r], v[r | rb], w);
       }
     }
@@ -198,7 +262,9 @@ LC_D void transform_slot(typename A::T* slot, const typename A::Tw* tw, const A&
 #pragma unroll
       for (int r = 0; r < V; ++r) {
         if (r & rb) continue;
-        const Tw w = tw[G::inv_phase0_off(b) + (r >> (b + 1)) * TT + t];
+        Tw w;
+        if constexpr (REGTW) w = lt.w[(V - (V >> b)) + (r >> (b + 1))];
+        else w = tw[G::inv_phase0_off(b) + (r >> (b + 1)) * TT + t];
         if (b == 0)
           ar.inv_first(v[r], v[r | rb], w);
         else
@@ -206,12 +272,25 @@ LC_D void transform_slot(typename A::T* slot, const typename A::Tw* tw, const A&
       }
     }
     __syncwarp();
+    if constexpr (SWZ) {
+      const uint32_t sx = (t >> 1) & 3u;
 #pragma unroll
-    for (int r = 0; r < V; ++r) slot[SL::padded((t << LOG_V) | r)] = v[r];
+      for (int c = 0; c < 4; ++c)
+        *reinterpret_cast<uint4*>(slot + (t << 4) + ((c ^ sx) << 2)) =
+            make_uint4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+    } else {
+#pragma unroll
+      for (int r = 0; r < V; ++r) slot[SL::padded((t << LOG_V) | r)] = v[r];
+    }
     __syncwarp();
     // ---- phase 1: register bits [LO0, LOG_N), levels b >= LOG_V (uniform twiddles)
+    if constexpr (SWZ) {
 #pragma unroll
-    for (int r = 0; r < V; ++r) v[r] = slot[SL::padded((r << LO0) | t)];
+      for (int r = 0; r < V; ++r) v[r] = slot[swz16((r << LO0) | (int)t)];
+    } else {
+#pragma unroll
+      for (int r = 0; r < V; ++r) v[r] = slot[SL::padded((r << LO0) | t)];
+    }
     constexpr int P1 = G::inv_phase1_off();
 #pragma unroll
     for (int b = LOG_V; b < LOG_N; ++b) {
@@ -233,8 +312,15 @@ LC_D void transform_slot(typename A::T* slot, const typename A::Tw* tw, const A&
   }
 }
 
-// Persistent tile loop over a ring of STAGES shared-memory tile buffers.
-template <class A, int LOG_N, int LOG_V, int NT, int IT, int STAGES, bool INVERSE>
+template <class A, int LOG_N, int LOG_V, bool INVERSE>
+LC_D void transform_slot(typename A::T* slot, const typename A::Tw* tw, const A& ar, uint32_t t) {
+  const LaneTw<A, LOG_N, LOG_V> unused{};
+  transform_slot_x<A, LOG_N, LOG_V, INVERSE, 0>(slot, tw, ar, t, unused);
+}
+
+// Persistent tile loop over a ring of STAGES shared-memory tile buffers;
+// OPT: kOpt* flags of the transform.
+template <class A, int LOG_N, int LOG_V, int NT, int IT, int STAGES, bool INVERSE, int OPT>
 __global__ void __launch_bounds__(NT) ntt_tile_kernel(const __grid_constant__ NttParams p) {
   using C = NttKernelCfg<A, LOG_N, LOG_V, NT, IT, STAGES, INVERSE>;
   using G = typename C::G;
@@ -263,6 +349,8 @@ __global__ void __launch_bounds__(NT) ntt_tile_kernel(const __grid_constant__ Nt
     fence_mbar_init();
   }
   __syncthreads();
+  LaneTw<A, LOG_N, LOG_V> lt;
+  if constexpr ((OPT & kOptRegTw) != 0) load_lane_tw<A, LOG_N, LOG_V, INVERSE>(lt, tw, t);
 
   const T* in = reinterpret_cast<const T*>(p.in) + (size_t)mi * p.count * N;
   T* out = reinterpret_cast<T*>(p.out) + (size_t)mi * p.count * N;
@@ -317,7 +405,7 @@ __global__ void __launch_bounds__(NT) ntt_tile_kernel(const __grid_constant__ Nt
     T* stage = data + (size_t)s * (C::STAGE_BYTES / sizeof(T));
 #pragma unroll 1
     for (int it = 0; it < IT; ++it)
-      transform_slot<A, LOG_N, LOG_V, INVERSE>(stage + (it * C::GROUPS + grp) * S, tw, ar, t);
+      transform_slot_x<A, LOG_N, LOG_V, INVERSE, OPT>(stage + (it * C::GROUPS + grp) * S, tw, ar, t, lt);
 
     fence_proxy_async_smem();
     __syncthreads();

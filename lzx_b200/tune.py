@@ -12,13 +12,15 @@ import ctypes as C
 
 from . import _lib
 
-NUM_VARIANTS = 5
+NUM_VARIANTS = 7  # LC_NTT_NUM_VARIANTS
 VARIANT_SHAPES = {
     0: "CTA-wide TMA ring: 128 threads, 2 stages",
     1: "CTA-wide TMA ring: 128 threads, 3 stages",
     2: "CTA-wide TMA ring: 256 threads, 2 stages",
     3: "warp-autonomous TMA rings: 4 warps/CTA, 2 stages",
     4: "warp-autonomous TMA rings: 4 warps/CTA, 3 stages",
+    5: "CTA-wide TMA ring: 128 threads, 2 stages, swizzled vector transpose (u32, d = 256)",
+    6: "CTA-wide TMA ring: 128 threads, 2 stages, swizzled vector transpose, lane twiddles in registers",
 }
 _cache: dict = {}
 

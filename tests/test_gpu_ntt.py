@@ -14,7 +14,7 @@ import pytest
 import oracle
 from lzx_b200 import (CRT_SET_30BIT, GoldilocksNttTables, Modulus32, NttError, NttTables, RingConfig,
                       RingElement, _lib)
-from lzx_b200 import synth
+from lzx_b200 import synth, tune
 
 pytestmark = pytest.mark.gpu
 
@@ -198,10 +198,10 @@ def test_ring_element_api():
     assert np.array_equal(u.coeffs(), oracle.uniform_from_seed(om, 6, b"ajtai-A", bytes([42]) * 32, 7))
 
 
-@pytest.mark.parametrize("variant", range(5))
+@pytest.mark.parametrize("variant", range(tune.NUM_VARIANTS))
 def test_every_kernel_variant_is_bit_exact(variant):
     """The tuner may pick any instantiated kernel shape; all must agree with the oracle."""
-    count = 1000  # not a multiple of any tile size
+    count = 1003  # not a multiple of any tile size
     a = synth.crt_batch(31, CRT_SET_30BIT, count, 256)
     t = NttTables(CRT_SET_30BIT, 8)
     assert _lib.lib().lc_ntt_plan_set_variant(t.handle, variant) == 0
@@ -215,7 +215,48 @@ def test_every_kernel_variant_is_bit_exact(variant):
     fg = tg.forward_fast(g.copy())
     assert np.array_equal(fg, oracle.NttTablesGl(6).forward_batch(g))
     assert np.array_equal(tg.inverse_fast(fg.copy()), g)
-    assert _lib.lib().lc_ntt_plan_set_variant(t.handle, 5) == _lib.LC_ERR_INVALID_ARGUMENT
+    assert _lib.lib().lc_ntt_plan_set_variant(t.handle, tune.NUM_VARIANTS) == _lib.LC_ERR_INVALID_ARGUMENT
+    assert _lib.lib().lc_ntt_plan_set_variant(t.handle, -1) == _lib.LC_ERR_INVALID_ARGUMENT
+
+
+@pytest.mark.parametrize("variant", range(tune.NUM_VARIANTS))
+def test_every_kernel_variant_on_many_tiles_per_cta(variant):
+    """2^17 + 3 polynomials per prime: about ten tiles per CTA, so each
+    variant's load/store ring wraps several times.  Inputs come from the device
+    generator; full round trip on the device plus oracle rows from the host
+    generator at three places of the batch."""
+    count, n = (1 << 17) + 3, 256
+    t = NttTables(CRT_SET_30BIT, 8)
+    L = _lib.lib()
+    assert L.lc_ntt_plan_set_variant(t.handle, variant) == 0
+    x = torch.empty(len(CRT_SET_30BIT) * count * n, dtype=torch.int32, device="cuda")
+    for i, m in enumerate(CRT_SET_30BIT):
+        synth.fill_device(x[i * count * n:(i + 1) * count * n], "mod32", 77, i, q=m.q)
+    y, z = torch.empty_like(x), torch.empty_like(x)
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    assert L.lc_ntt_forward(t.handle, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), count, st) == 0
+    assert L.lc_ntt_inverse(t.handle, C.c_void_p(y.data_ptr()), C.c_void_p(z.data_ptr()), count, st) == 0
+    assert L.lc_ntt_plan_check(t.handle, st) == 0
+    assert torch.equal(z, x)
+    got = from_dev(y, np.uint32).reshape(len(CRT_SET_30BIT), count, n)
+    for i, m in enumerate(CRT_SET_30BIT):
+        for r0, r1 in ((0, 24), (70_000, 70_016), (count - 24, count)):
+            a = synth.synth_mod32(77, i, m.q, (r1 - r0) * n, offset=r0 * n).reshape(-1, n)
+            assert np.array_equal(got[i][r0:r1], ora_tables(m, 8).forward_batch(a))
+    cg = 300_007
+    g = torch.empty(cg * 64, dtype=torch.int64, device="cuda")
+    synth.fill_device(g, "gl", 78, 0)
+    tg = GoldilocksNttTables(6)
+    assert L.lc_ntt_plan_set_variant(tg.handle, variant) == 0
+    fg, bg = torch.empty_like(g), torch.empty_like(g)
+    assert L.lc_ntt_forward(tg.handle, C.c_void_p(g.data_ptr()), C.c_void_p(fg.data_ptr()), cg, st) == 0
+    assert L.lc_ntt_inverse(tg.handle, C.c_void_p(fg.data_ptr()), C.c_void_p(bg.data_ptr()), cg, st) == 0
+    assert L.lc_ntt_plan_check(tg.handle, st) == 0
+    assert torch.equal(bg, g)
+    fh = from_dev(fg, np.uint64).reshape(cg, 64)
+    for r0, r1 in ((0, 32), (cg - 32, cg)):
+        a = synth.synth_gl(78, 0, (r1 - r0) * 64, offset=r0 * 64).reshape(-1, 64)
+        assert np.array_equal(fh[r0:r1], oracle.NttTablesGl(6).forward_batch(a))
 
 
 def test_device_synth_matches_host_generator():
