@@ -873,30 +873,42 @@ def bench_single(args, rank, max_over_ranks, barrier, world):
     L = _lib.lib()
     st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
     h, wp, op = key.handle, C.c_void_p(W.data_ptr()), C.c_void_p(out.data_ptr())
-    for _ in range(20):
-        _lib.check(L.lc_ajtai_commit_i8(h, wp, 1, op, st), "commit")
-    torch.cuda.synchronize()
-    K = 200
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record()
-    for _ in range(K):
-        L.lc_ajtai_commit_i8(h, wp, 1, op, st)
-    b.record()
-    torch.cuda.synchronize()
-    dev_us = a.elapsed_time(b) / K * 1e3
     hw = W.cpu().numpy()
     hout = torch.empty((1, S_KAPPA, 64), dtype=torch.int64)
     hp, hop = hw.ctypes.data_as(C.c_void_p), C.c_void_p(hout.data_ptr())
-    for _ in range(5):
-        _lib.check(L.lc_ajtai_commit_i8_host(h, hp, 1, hop), "commit host")
-    t0 = time.perf_counter()
-    for _ in range(50):
-        L.lc_ajtai_commit_i8_host(h, hp, 1, hop)
-    host_us = (time.perf_counter() - t0) / 50 * 1e6
-    assert torch.equal(hout, out.cpu())
+
+    def timed():
+        for _ in range(20):
+            _lib.check(L.lc_ajtai_commit_i8(h, wp, 1, op, st), "commit")
+        torch.cuda.synchronize()
+        K = 200
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(K):
+            L.lc_ajtai_commit_i8(h, wp, 1, op, st)
+        b.record()
+        torch.cuda.synchronize()
+        dev = a.elapsed_time(b) / K * 1e3
+        for _ in range(5):
+            _lib.check(L.lc_ajtai_commit_i8_host(h, hp, 1, hop), "commit host")
+        t0 = time.perf_counter()
+        for _ in range(50):
+            L.lc_ajtai_commit_i8_host(h, hp, 1, hop)
+        host = (time.perf_counter() - t0) / 50 * 1e6
+        assert torch.equal(hout, out.cpu())
+        return dev, host, out.clone()
+
+    dev_us, host_us, fused_out = timed()  # one launch per commitment (the default)
+    key.fused = False
+    st_dev_us, st_host_us, staged_out = timed()
+    key.fused = True
+    assert torch.equal(fused_out, staged_out)
     res = {"workload": "single commitment, d=64 Goldilocks, kappa=8, n=256 int8 digits",
            "device_us_per_commit": dev_us, "e2e_us_per_commit": host_us,
-           "e2e_api": "lc_ajtai_commit_i8_host (synchronous, pageable host buffers)"}
+           "form": "single launch (commit_fused_kernel)",
+           "e2e_api": "lc_ajtai_commit_i8_host (synchronous, pageable host buffers)",
+           "staged": {"device_us_per_commit": st_dev_us, "e2e_us_per_commit": st_host_us,
+                      "form": "witness NTT, product, split sum, inverse NTT launches"}}
     if rank == 0 and not args.no_cpu_baseline:
         import oracle
         oracle.prefer_native(True)

@@ -223,6 +223,18 @@ LC_API int lc_ajtai_key_create_ex(const lc_ntt_plan *plan, uint32_t k, uint32_t 
 LC_API int lc_ajtai_key_set_engine(lc_ajtai_key *key, int engine);
 LC_API int lc_ajtai_key_get_engine(const lc_ajtai_key *key);
 
+/* Single-launch form of the NTT engine, on by default: a commitment of at
+ * most 4 witnesses, at most 2048 ring elements and at most 2^20
+ * multiply-adds (batch * m * n * k), log_n 6..8, runs as one kernel -- the
+ * witness forward transforms, the pointwise products against the cached
+ * NTT(A), their sum over the whole witness and the row inverse transforms,
+ * i.e. the whole body of AjtaiPublicKey::commit (ajtai.rs:118-153) -- rather
+ * than the staged launches.  Identical results; enable = 0 turns it off for
+ * this key (every commit then runs staged), 1 turns it back on.
+ * lc_ajtai_key_get_fused returns 1 or 0 (-1 for a null key). */
+LC_API int lc_ajtai_key_set_fused(lc_ajtai_key *key, int enable);
+LC_API int lc_ajtai_key_get_fused(const lc_ajtai_key *key);
+
 /* Commit without allocating any device memory.  No counterpart in the
  * reference: it exists for callers that cannot call cudaMalloc while they
  * commit -- code that records work into a CUDA graph, processes whose device

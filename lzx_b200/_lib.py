@@ -85,6 +85,8 @@ def _declare(L):
         "lc_ajtai_key_create_ex": (i32, [P, u32, u32, P, i32, u32, C.POINTER(P)]),
         "lc_ajtai_key_set_engine": (i32, [P, i32]),
         "lc_ajtai_key_get_engine": (i32, [P]),
+        "lc_ajtai_key_set_fused": (i32, [P, i32]),
+        "lc_ajtai_key_get_fused": (i32, [P]),
         "lc_ajtai_commit_u8": (i32, [P, P, sz, P, P]),
         "lc_ajtai_commit_u8_host": (i32, [P, P, sz, P]),
         "lc_decomp_b": (i32, [P, sz, u32, P, P]),

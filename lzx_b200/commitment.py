@@ -83,6 +83,15 @@ class _DeviceKey:
     def engine(self, value: int):
         check(_lib.lib().lc_ajtai_key_set_engine(self._h, int(value)), "lc_ajtai_key_set_engine")
 
+    @property
+    def fused(self) -> bool:
+        """Whether small commitments run as one launch (lc_ajtai_key_set_fused)."""
+        return _lib.lib().lc_ajtai_key_get_fused(self._h) == 1
+
+    @fused.setter
+    def fused(self, value: bool):
+        check(_lib.lib().lc_ajtai_key_set_fused(self._h, 1 if value else 0), "lc_ajtai_key_set_fused")
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and _lib._lib is not None:
@@ -181,6 +190,15 @@ class AjtaiPublicKey:
         for idx in range(total):
             mat[idx] = ring.uniform_from_seed(b"ajtai-A", seed, idx).coeffs()
         return cls(params, seed, mat)
+
+    @property
+    def fused(self) -> bool:
+        """Small commitments as one launch (the default); False runs them staged."""
+        return self._dev.fused
+
+    @fused.setter
+    def fused(self, value: bool):
+        self._dev.fused = value
 
     def entry(self, i: int, j: int):
         if i < self.params.k and j < self.params.m:
@@ -291,6 +309,16 @@ class GoldilocksAjtaiKey:
     @engine.setter
     def engine(self, value: int):
         self._dev.engine = value
+
+    @property
+    def fused(self) -> bool:
+        """Small commitments (at most 4 witnesses, 2048 ring elements, 2^20
+        multiply-adds) as one launch; False runs every commit staged."""
+        return self._dev.fused
+
+    @fused.setter
+    def fused(self, value: bool):
+        self._dev.fused = value
 
     def commit(self, w, out=None):
         return self._dev.commit_array(w, out)

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 #include <mutex>
 #include <new>
 #include <type_traits>
@@ -368,6 +369,138 @@ __global__ void mac_small_kernel(const E* __restrict__ ahat_t, uint32_t am, cons
   }
 }
 
+// ------------------------------------------------------------------ single-launch commit
+//
+// A small commitment (at most 4 witnesses, a few thousand ring elements) in
+// one kernel: CTA c takes ring elements [c*jc, c*jc + jc) of every witness,
+// runs their forward transforms in shared memory, multiplies them against
+// the cached NTT(A) slots of every row and adds each canonical partial sum v
+// into two 64-bit accumulators in global memory, one for the low and one for
+// the high 32 bits of v (atomic adds whose result is not read back; neither
+// sum can wrap for fewer than 2^32 CTAs).  The CTA that takes the last
+// ticket forms low + high * 2^32 as a 128-bit value, reduces it mod q, zeroes
+// the accumulators and the ticket for the next call, runs the batch x kappa
+// inverse transforms in shared memory and writes the rows.  No CTA ever
+// waits for another; the accumulators and the ticket are zero between calls.
+struct FusedCommitParams {
+  const void* w;      // [batch][m][n] witness (residues or byte digits)
+  const void* ahat_t; // Ahat_T[t][j][i_pad]
+  unsigned long long* acc;  // [batch][kappa][n] x {sum of low halves, sum of high halves}
+  uint32_t* ticket;
+  void* out;          // [batch][kappa][n]
+  const void* twf;    // forward / inverse twiddle tables of the plan
+  const void* twi;
+  uint32_t batch, m, am, kappa, jc, nc, q, qinv;
+};
+
+template <class A, int LOG_N, int LOG_V>
+struct FusedCommitCfg {
+  using G = Geo<LOG_N, LOG_V>;
+  using T = typename A::T;
+  using Tw = typename A::Tw;
+  static constexpr int NT = 256;
+  static constexpr int GROUPS = NT / G::T;  // polynomials per transform pass
+  static constexpr int SS = WitnessSlotStride<A, LOG_N>::value;
+  static constexpr int MAX_ROWS = 4 * kIPad;  // batch x kappa rows of the last CTA
+  static constexpr int SLOTS = GROUPS > MAX_ROWS ? GROUPS : MAX_ROWS;
+  static constexpr size_t TWF = ((size_t)G::fwd_entries() * sizeof(Tw) + 15) / 16 * 16;
+  static constexpr size_t TWI = ((size_t)G::inv_entries() * sizeof(Tw) + 15) / 16 * 16;
+  static constexpr size_t SMEM = TWF + TWI + (size_t)SLOTS * SS * sizeof(T);
+  static_assert(MAX_ROWS % GROUPS == 0, "inverse passes stay inside the slots");
+};
+
+template <class A, class S, int LOG_N, int LOG_V>
+__global__ void __launch_bounds__(256) commit_fused_kernel(const __grid_constant__ FusedCommitParams p) {
+  using C = FusedCommitCfg<A, LOG_N, LOG_V>;
+  using G = typename C::G;
+  using E = typename A::T;
+  using Tw = typename A::Tw;
+  constexpr int N = G::N, SS = C::SS, NT = C::NT;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ uint32_t is_last;
+  Tw* twf = reinterpret_cast<Tw*>(smem_raw);
+  Tw* twi = reinterpret_cast<Tw*>(smem_raw + C::TWF);
+  E* slots = reinterpret_cast<E*>(smem_raw + C::TWF + C::TWI);
+  const int tid = threadIdx.x;
+  const uint32_t j0 = blockIdx.x * p.jc;
+  const uint32_t jn = min(p.jc, p.m - j0);
+  const E* ahat = reinterpret_cast<const E*>(p.ahat_t);
+  // this CTA's rows of Ahat_T (one run of jn * 16 entries per slot) into L2
+  // while the witness is loaded and transformed
+  {
+    constexpr uint32_t kLine = 128 / sizeof(E);
+    const uint32_t run = jn * kIPad, lines = (run + kLine - 1) / kLine;
+    for (uint32_t e = tid; e < N * lines; e += NT) {
+      const E* a = ahat + ((size_t)(e / lines) * p.am + j0) * kIPad + (e % lines) * kLine;
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+    }
+  }
+  for (int i = tid; i < G::fwd_entries(); i += NT) twf[i] = reinterpret_cast<const Tw*>(p.twf)[i];
+  for (int i = tid; i < G::inv_entries(); i += NT) twi[i] = reinterpret_cast<const Tw*>(p.twi)[i];
+
+  // ---- witness ring elements of this CTA: polynomial jj*batch + b in slot jj*batch + b
+  const uint32_t pp = jn * p.batch;
+  const S* w = reinterpret_cast<const S*>(p.w);
+  for (int e = tid; e < C::GROUPS * N; e += NT) {
+    const uint32_t pi = e / N, c = e % N;
+    E v = 0;
+    if (pi < pp) {
+      const uint32_t jj = pi / p.batch, b = pi % p.batch;
+      v = to_residue<E, S>(w[((size_t)b * p.m + j0 + jj) * N + c], p.q);
+    }
+    slots[pi * SS + c] = v;
+  }
+  __syncthreads();
+  const A ar = make_arith_q<A>(p.q, p.qinv);
+  const int grp = tid / G::T;
+  const uint32_t t = (uint32_t)(tid % G::T);
+  transform_slot<A, LOG_N, LOG_V, false>(slots + grp * SS, twf, ar, t);
+  __syncthreads();
+
+  // ---- products of this CTA's ring elements; output (b, slot tt, row i), i fastest
+  const uint32_t outs = p.batch * N * p.kappa;
+  for (uint32_t o = tid; o < outs; o += NT) {
+    const uint32_t i = o % p.kappa, tt = (o / p.kappa) % N, b = o / (p.kappa * N);
+    const E* ap = ahat + ((size_t)tt * p.am + j0) * kIPad + i;
+    Acc160 acc;
+#pragma unroll 4
+    for (uint32_t jj = 0; jj < jn; ++jj) mac<E>(acc, ap[(size_t)jj * kIPad], slots[(jj * p.batch + b) * SS + tt]);
+    const uint64_t v = (uint64_t)acc_reduce<E>(acc, p.q);
+    unsigned long long* a2 = p.acc + 2 * (((size_t)b * p.kappa + i) * N + tt);
+    atomicAdd(a2, (unsigned long long)(v & 0xffffffffu));
+    if (v >> 32) atomicAdd(a2 + 1, (unsigned long long)(v >> 32));
+  }
+  __threadfence();  // this thread's additions are visible before the ticket
+  __syncthreads();
+  if (tid == 0) is_last = atomicAdd(p.ticket, 1u) == p.nc - 1 ? 1u : 0u;
+  __syncthreads();
+  if (!is_last) return;
+  __threadfence();
+
+  // ---- last CTA: accumulators -> canonical evaluations -> inverse transforms
+  const uint32_t rows = p.batch * p.kappa;
+  for (uint32_t e = tid; e < rows * N; e += NT) {
+    const uint32_t r = e / N, tt = e % N;
+    unsigned long long* a2 = p.acc + 2 * ((size_t)r * N + tt);
+    const uint64_t sl = __ldcg(a2), sh = __ldcg(a2 + 1);
+    // x = sl + sh * 2^32 < 2^96
+    const uint64_t lo = sl + (sh << 32);
+    const uint64_t hi = (sh >> 32) + (lo < sl ? 1u : 0u);
+    slots[r * SS + tt] = Field<E>::reduce160((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi,
+                                             (uint32_t)(hi >> 32), 0, p.q);
+    __stcg(a2, 0ull);
+    __stcg(a2 + 1, 0ull);
+  }
+  if (tid == 0) *p.ticket = 0;
+  __syncthreads();
+  // whole passes of GROUPS slots: groups past `rows` transform unused slots
+  for (uint32_t base = 0; base < rows; base += C::GROUPS)
+    transform_slot<A, LOG_N, LOG_V, true>(slots + (base + grp) * SS, twi, ar, t);
+  __syncthreads();
+  E* out = reinterpret_cast<E*>(p.out);
+  for (uint32_t e = tid; e < rows * N; e += NT) out[e] = slots[(e / N) * SS + e % N];
+}
+
 // Chat[b][i][t] = sum_split partial[split][t][i][b]  (mod q)
 template <class E>
 __global__ void reduce_partials_kernel(const E* __restrict__ partial, E* __restrict__ chat,
@@ -596,10 +729,94 @@ static int commit_core(lc_ajtai_key* key, size_t batch, uint32_t b_pad, void* ou
   return run_ntt(key->plan, key->d_chat, out, (size_t)batch * kappa, true, st);
 }
 
+// Single-launch commit (commit_fused_kernel) for small problems: at most
+// kFusedMaxBatch witnesses, kFusedMaxM ring elements and kFusedMaxMacs
+// multiply-adds, where the staged launches cost more than their work.
+constexpr size_t kFusedMaxBatch = 4;
+constexpr uint32_t kFusedMaxM = 2048;
+constexpr size_t kFusedMaxMacs = (size_t)1 << 20;
+
+template <class A, class S, int LOG_N, int LOG_V>
+static int launch_commit_fused(lc_ajtai_key* key, const S* w, size_t batch, void* out, cudaStream_t st) {
+  using C = FusedCommitCfg<A, LOG_N, LOG_V>;
+  constexpr uint32_t N = 1u << LOG_N;
+  // accumulators for the largest batch of this key, zeroed once; every call
+  // leaves them zero again
+  if (!key->d_fused) {
+    const size_t bytes = 16 + kFusedMaxBatch * key->k * N * 16;
+    int rc = grow(&key->d_fused, &key->fused_bytes, bytes);
+    if (rc) return rc;
+    rc = map_cuda(cudaMemsetAsync(key->d_fused, 0, bytes, st));
+    if (rc) return rc;
+  }
+  auto kern = commit_fused_kernel<A, S, LOG_N, LOG_V>;
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+    if (e != cudaSuccess) return map_cuda(e);
+    attr_done = true;
+  }
+  // ring elements per CTA: about 16 multiply-adds per thread and at least 8
+  // (few atomic additions per product), within one transform pass
+  const uint32_t per_thread = (uint32_t)((batch * N * key->k + C::NT - 1) / C::NT);
+  uint32_t jc = std::max<uint32_t>(8, 16 / std::max<uint32_t>(1, per_thread));
+  jc = std::max<uint32_t>(1, std::min<uint32_t>(jc, (uint32_t)(C::GROUPS / batch)));
+  FusedCommitParams p{};
+  p.w = w;
+  p.ahat_t = key->d_ahat_t;
+  p.ticket = static_cast<uint32_t*>(key->d_fused);
+  p.acc = reinterpret_cast<unsigned long long*>(static_cast<unsigned char*>(key->d_fused) + 16);
+  p.out = out;
+  p.twf = key->plan->d_tw_fwd;
+  p.twi = key->plan->d_tw_inv;
+  p.batch = (uint32_t)batch;
+  p.m = key->m;
+  p.am = key->a_m;
+  p.kappa = key->k;
+  p.jc = jc;
+  p.nc = (key->m + jc - 1) / jc;
+  p.q = key->plan->q[0];
+  p.qinv = key->plan->qinv[0];
+  kern<<<p.nc, C::NT, C::SMEM, st>>>(p);
+  return map_cuda(cudaGetLastError());
+}
+
+template <class A, class S>
+static int commit_fused_as(lc_ajtai_key* key, const S* w, size_t batch, void* out, cudaStream_t st) {
+  switch (key->log_n) {
+    case 6: return launch_commit_fused<A, S, 6, 3>(key, w, batch, out, st);
+    case 7: return launch_commit_fused<A, S, 7, 4>(key, w, batch, out, st);
+    case 8: return launch_commit_fused<A, S, 8, 4>(key, w, batch, out, st);
+    default: return LC_ERR_UNSUPPORTED;
+  }
+}
+
+// LC_ERR_UNSUPPORTED when the problem is not small enough for one launch.
+template <class S>
+static int commit_fused(lc_ajtai_key* key, const S* w, size_t batch, void* out, cudaStream_t st) {
+  if (!key->fused || batch > kFusedMaxBatch || key->m > kFusedMaxM || key->log_n < 6 || key->log_n > 8)
+    return LC_ERR_UNSUPPORTED;
+  if ((size_t)key->m * batch * key->n * key->k > kFusedMaxMacs) return LC_ERR_UNSUPPORTED;
+  const PlanKind kind = key->plan->kind;
+  if constexpr (!std::is_same<S, uint32_t>::value) {
+    if (kind == PlanKind::Goldilocks) return commit_fused_as<Goldilocks, S>(key, w, batch, out, st);
+  }
+  if constexpr (!std::is_same<S, uint64_t>::value) {
+    if (kind == PlanKind::U32Lazy) return commit_fused_as<ShoupLazy, S>(key, w, batch, out, st);
+    if (kind == PlanKind::U32Mont) return commit_fused_as<MontCanon, S>(key, w, batch, out, st);
+  }
+  return LC_ERR_UNSUPPORTED;
+}
+
 template <class S>
 static int commit_any(lc_ajtai_key* key, const S* w, size_t batch, void* out, cudaStream_t st) {
   if (batch == 0) return LC_OK;
   if (batch > (1u << 24)) return LC_ERR_INVALID_ARGUMENT;
+  {
+    const int rc = commit_fused<S>(key, w, batch, out, st);
+    key->last_fused = rc == LC_OK;
+    if (rc != LC_ERR_UNSUPPORTED) return rc;
+  }
   // tiles of 128 witnesses from 64 on; from 4 on a multiple of 4 (zero
   // columns) for the quad product
   const uint32_t b_pad = batch >= 64 ? (uint32_t)((batch + kBTile - 1) / kBTile * kBTile)
@@ -820,11 +1037,13 @@ LC_API int lc_ajtai_key_create_ex(const lc_ntt_plan* plan, uint32_t k, uint32_t 
 LC_API void lc_ajtai_key_destroy(lc_ajtai_key* key) {
   if (!key) return;
   if (key->owns_ahat && key->d_ahat_t) cudaFree(key->d_ahat_t);
-  for (void* p : {key->d_what_t, key->d_partial, key->d_chat, key->d_wtmp, key->d_in,
+  for (void* p : {key->d_what_t, key->d_partial, key->d_chat, key->d_wtmp, key->d_fused, key->d_in,
                   key->d_out, (void*)key->d_err})
     if (p) cudaFree(p);
   if (key->host_stream) cudaStreamDestroy(key->host_stream);
   if (key->h_flags) cudaFreeHost(key->h_flags);
+  if (key->h_stage_in) cudaFreeHost(key->h_stage_in);
+  if (key->h_stage_out) cudaFreeHost(key->h_stage_out);
   if (key->plan) lc_ntt_plan_destroy(key->plan);
   tc_tables_destroy(key->tc);
   delete key;
@@ -868,6 +1087,14 @@ LC_API int lc_ajtai_key_set_engine(lc_ajtai_key* key, int engine) {
 
 LC_API int lc_ajtai_key_get_engine(const lc_ajtai_key* key) { return key ? key->engine : -1; }
 
+LC_API int lc_ajtai_key_set_fused(lc_ajtai_key* key, int enable) {
+  if (!key || (enable != 0 && enable != 1)) return LC_ERR_INVALID_ARGUMENT;
+  key->fused = enable == 1;
+  return LC_OK;
+}
+
+LC_API int lc_ajtai_key_get_fused(const lc_ajtai_key* key) { return key ? (key->fused ? 1 : 0) : -1; }
+
 }  // extern "C"
 
 namespace lc {
@@ -878,7 +1105,7 @@ uint64_t commit_scratch_signature(const lc_ajtai_key* key) {
   uint64_t h = 1469598103934665603ull;
   for (uintptr_t v : {(uintptr_t)key->d_what_t, (uintptr_t)key->d_partial, (uintptr_t)key->d_chat,
                       (uintptr_t)key->d_wtmp, (uintptr_t)key->what_bytes, (uintptr_t)key->partial_bytes,
-                      (uintptr_t)key->chat_bytes, (uintptr_t)key->wtmp_bytes})
+                      (uintptr_t)key->chat_bytes, (uintptr_t)key->wtmp_bytes, (uintptr_t)key->d_fused})
     h = (h ^ (uint64_t)v) * 1099511628211ull;
   return h;
 }
@@ -911,6 +1138,35 @@ LC_API int lc_ajtai_commit_u8(lc_ajtai_key* key, const uint8_t* s, size_t batch,
   return commit_any<uint8_t>(key, s, batch, out, (cudaStream_t)stream);
 }
 
+// Host buffers of at most kHostStageMax bytes that are not page-locked go
+// through pinned staging buffers of the key: a CPU copy of a few KB costs far
+// less than the driver's synchronous path for pageable memory.  Page-locked
+// (or larger) buffers are copied directly.
+constexpr size_t kHostStageMax = (size_t)1 << 20;
+
+static bool host_pinned(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+static int grow_pinned(void** p, size_t* have, size_t need) {
+  if (need <= *have) return LC_OK;
+  if (*p) cudaFreeHost(*p);
+  *p = nullptr;
+  *have = 0;
+  if (cudaMallocHost(p, need) != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return LC_ERR_OUT_OF_MEMORY;
+  }
+  *have = need;
+  return LC_OK;
+}
+
 static int commit_host(lc_ajtai_key* key, const void* s, size_t in_elem, size_t batch, void* out,
                        bool i8) {
   if (!key || (!s && batch) || (!out && batch)) return LC_ERR_INVALID_ARGUMENT;
@@ -927,21 +1183,40 @@ static int commit_host(lc_ajtai_key* key, const void* s, size_t in_elem, size_t 
     key->h_flags = nullptr;
     return map_cuda(cudaGetLastError());
   }
+  const bool stage_in = in_bytes <= kHostStageMax && !host_pinned(s);
+  const bool stage_out = out_bytes <= kHostStageMax && !host_pinned(out);
+  if (stage_in) {
+    rc = grow_pinned(&key->h_stage_in, &key->h_stage_in_bytes, in_bytes);
+    if (rc) return rc;
+    std::memcpy(key->h_stage_in, s, in_bytes);
+  }
+  if (stage_out) {
+    rc = grow_pinned(&key->h_stage_out, &key->h_stage_out_bytes, out_bytes);
+    if (rc) return rc;
+  }
   cudaStream_t st = key->host_stream;
-  if (cudaMemcpyAsync(key->d_in, s, in_bytes, cudaMemcpyHostToDevice, st) != cudaSuccess)
+  if (cudaMemcpyAsync(key->d_in, stage_in ? key->h_stage_in : s, in_bytes, cudaMemcpyHostToDevice, st) !=
+      cudaSuccess)
     return map_cuda(cudaGetLastError());
+  key->last_fused = false;
   rc = in_elem == 1 ? (i8 ? lc_ajtai_commit_i8(key, (const int8_t*)key->d_in, batch, key->d_out, st)
                           : lc_ajtai_commit_u8(key, (const uint8_t*)key->d_in, batch, key->d_out, st))
                     : lc_ajtai_commit(key, key->d_in, batch, key->d_out, st);
   if (rc) return rc;
-  if (cudaMemcpyAsync(out, key->d_out, out_bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+  // the single-launch kernel has no bounded waits and never sets an error word
+  const bool flags = !key->last_fused;
+  if (cudaMemcpyAsync(stage_out ? key->h_stage_out : out, key->d_out, out_bytes, cudaMemcpyDeviceToHost, st) !=
+      cudaSuccess)
     return map_cuda(cudaGetLastError());
   // both error words come back with the result: one synchronisation per call
-  cudaMemcpyAsync(key->h_flags, key->d_err, 4, cudaMemcpyDeviceToHost, st);
-  cudaMemcpyAsync(key->h_flags + 1, key->plan->d_err, 4, cudaMemcpyDeviceToHost, st);
+  if (flags) {
+    cudaMemcpyAsync(key->h_flags, key->d_err, 4, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(key->h_flags + 1, key->plan->d_err, 4, cudaMemcpyDeviceToHost, st);
+  }
   const cudaError_t e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return map_cuda(e);
-  if (key->h_flags[0] | key->h_flags[1]) {
+  if (stage_out) std::memcpy(out, key->h_stage_out, out_bytes);
+  if (flags && (key->h_flags[0] | key->h_flags[1])) {
     cudaMemsetAsync(key->d_err, 0, 4, st);
     cudaMemsetAsync(key->plan->d_err, 0, 4, st);
     cudaStreamSynchronize(st);

@@ -93,10 +93,18 @@ struct lc_ajtai_key {
   size_t chat_bytes = 0;
   void* d_wtmp = nullptr;  // generic witness path: converted + transformed witnesses
   size_t wtmp_bytes = 0;
+  void* d_fused = nullptr;  // single-launch commit: ticket (16 B), then 128-bit accumulators
+  size_t fused_bytes = 0;
+  bool fused = true;        // small commits as one launch (lc_ajtai_key_set_fused)
+  bool last_fused = false;  // the last commit on this key ran as one launch
   void* d_in = nullptr;  // host-API staging
   size_t in_bytes = 0;
   void* d_out = nullptr;
   size_t out_bytes = 0;
+  void* h_stage_in = nullptr;  // pinned staging of small pageable host buffers (host API)
+  size_t h_stage_in_bytes = 0;
+  void* h_stage_out = nullptr;
+  size_t h_stage_out_bytes = 0;
   cudaStream_t host_stream = nullptr;
   uint32_t* h_flags = nullptr;  // pinned: the key's and the plan's error words (host API)
   uint32_t* d_err = nullptr;
