@@ -223,6 +223,15 @@ LC_API int lc_ajtai_key_create_ex(const lc_ntt_plan *plan, uint32_t k, uint32_t 
 LC_API int lc_ajtai_key_set_engine(lc_ajtai_key *key, int engine);
 LC_API int lc_ajtai_key_get_engine(const lc_ajtai_key *key);
 
+/* Measured INT8 tensor rate (no counterpart in the reference): one CTA per
+ * SM issues `iters` x 4 tcgen05.mma.kind::i8 (M = 128, N = 256, K = 32, the
+ * shape of the tensor-core engines; s8 != 0: signed x unsigned operands,
+ * else unsigned x unsigned) on operands resident in shared memory, timed
+ * with CUDA events after a warm-up launch.  *ops_per_s = integer operations
+ * (2 per multiply-add) per second over the whole GPU; *ms (optional) the
+ * timed launch.  The roofline denominator of the INT8 engines. */
+LC_API int lc_tc_i8_rate(uint32_t iters, int s8, double *ops_per_s, float *ms);
+
 /* Single-launch form of the NTT engine, on by default: a commitment of at
  * most 4 witnesses, at most 2048 ring elements and at most 2^20
  * multiply-adds (batch * m * n * k), log_n 6..8, runs as one kernel -- the

@@ -86,6 +86,7 @@ def _declare(L):
         "lc_ajtai_key_set_engine": (i32, [P, i32]),
         "lc_ajtai_key_get_engine": (i32, [P]),
         "lc_ajtai_key_set_fused": (i32, [P, i32]),
+        "lc_tc_i8_rate": (i32, [u32, i32, C.POINTER(C.c_double), C.POINTER(C.c_float)]),
         "lc_ajtai_key_get_fused": (i32, [P]),
         "lc_ajtai_commit_u8": (i32, [P, P, sz, P, P]),
         "lc_ajtai_commit_u8_host": (i32, [P, P, sz, P]),

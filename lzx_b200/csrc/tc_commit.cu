@@ -270,7 +270,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       if (s >= 2) ok = mbar_wait(&mma_done[(s - 2) & 3], ((s - 2) >> 2) & 1);  // rotation slot free
       ok = ok && mbar_wait(&loaded[s & 3], (s >> 2) & 1);
       if (!ok) fail();
-      if (*abort_flag) break;
+      // warp-uniform: the loop below synchronises the warp
+      if (__any_sync(0xffffffffu, *abort_flag)) break;
       const unsigned char* fbase = f_slot(s) + jj * kTcFHalf;
 #pragma unroll
       for (int it = 0; it < 4; ++it) {
@@ -302,9 +303,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 
   // ---------------- drain the accumulators (builder warps)
   __syncthreads();
-  if (!*abort_flag && nst > 0 && warp < 8) {
+  if (nst > 0 && warp < 8 && !__any_sync(0xffffffffu, *abort_flag)) {
     const int ls = nst - 1;
-    if (!mbar_wait(&mma_done[ls & 3], (ls >> 2) & 1)) {
+    // warp-uniform decision: the TMEM loads below are .sync.aligned
+    if (!__all_sync(0xffffffffu, mbar_wait(&mma_done[ls & 3], (ls >> 2) & 1))) {
       fail();
     } else {
       tc_fence_after();
@@ -538,7 +540,9 @@ __global__ void __launch_bounds__(kTnThreads, 1)
       const uint32_t b = bt * p.BB + bb;
       bool stop = false;
       for (int jj = 0; jj < 2; ++jj, ++e) {
-        if (*abort_flag || !mbar_wait(acc_full, (uint32_t)(e & 1))) {
+        // warp-uniform decision: the TMEM loads below are .sync.aligned
+        const bool ok = !*abort_flag && mbar_wait(acc_full, (uint32_t)(e & 1));
+        if (!__all_sync(0xffffffffu, ok)) {
           fail();
           stop = true;
           break;
@@ -796,3 +800,107 @@ int tc_witness_ntt(const void* w, bool s8, size_t batch, uint32_t m, uint32_t b_
 }
 
 }  // namespace lc
+
+// ------------------------------------------------------------------ INT8 tensor rate
+//
+// Measurement kernel for the INT8 tensor roofline: one CTA per SM keeps its
+// tensor pipe busy with tcgen05.mma.kind::i8 of the commit engines' shape
+// (M = 128, N = 256, K = 32, int32 accumulators in TMEM) on operands that
+// stay in shared memory, with no global traffic.  One MMA is 2*128*256*32
+// integer operations; the products are discarded.
+namespace lc {
+
+constexpr int kRateThreads = 128;
+constexpr int kRateOperandBytes = 128 * 128 + 256 * 128;  // A tile, B tile (K = 128 bytes each)
+// more shared memory than two CTAs could hold: one CTA per SM
+constexpr size_t kRateSmem = 116 * 1024;
+static_assert(1024 + kRateOperandBytes + 64 <= (int)kRateSmem, "rate kernel layout");
+
+static __device__ uint32_t g_rate_err;
+
+template <bool S8>
+__global__ void __launch_bounds__(kRateThreads, 1) tc_rate_kernel(uint32_t iters) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char* base =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* done = reinterpret_cast<uint64_t*>(base + kRateOperandBytes);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  uint32_t* words = reinterpret_cast<uint32_t*>(base);
+  for (int i = tid; i < kRateOperandBytes / 4; i += kRateThreads) words[i] = 0x9E3779B9u * (uint32_t)(i + 1);
+  if (tid == 0) {
+    mbar_init(done, 1);
+    fence_mbar_init();
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(256));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  fence_proxy_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  if (tid == 0) {
+    const uint32_t sa = smem_u32(base), sb = smem_u32(base + 128 * 128);
+    for (uint32_t it = 0; it < iters; ++it) {
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks)
+        mma_i8(tmem, umma_desc_sw128(sa + 32 * ks), umma_desc_sw128(sb + 32 * ks), TcIdesc<S8>::value,
+               (it | (uint32_t)ks) ? 1u : 0u);
+    }
+    mma_commit(done);
+    if (!mbar_wait(done, 0)) record_error(&g_rate_err, LC_DEVERR_TIMEOUT);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256));
+  }
+}
+
+}  // namespace lc
+
+extern "C" {
+
+LC_API int lc_tc_i8_rate(uint32_t iters, int s8, double* ops_per_s, float* ms) {
+  if (!ops_per_s || iters == 0 || iters > (1u << 24)) return LC_ERR_INVALID_ARGUMENT;
+  const int sms = lc::device_sm_count();
+  if (sms <= 0) return LC_ERR_NO_DEVICE;
+  auto kern = s8 ? lc::tc_rate_kernel<true> : lc::tc_rate_kernel<false>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lc::kRateSmem);
+  if (e != cudaSuccess) return lc::map_cuda(e);
+  uint32_t* err = nullptr;
+  e = cudaGetSymbolAddress(reinterpret_cast<void**>(&err), lc::g_rate_err);
+  if (e != cudaSuccess) return lc::map_cuda(e);
+  cudaStream_t st = nullptr;
+  cudaEvent_t a = nullptr, b = nullptr;
+  e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&a);
+  if (e == cudaSuccess) e = cudaEventCreate(&b);
+  float t = 0.f;
+  uint32_t flag = 0;
+  if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, 4, st);
+  if (e == cudaSuccess) {
+    kern<<<sms, lc::kRateThreads, lc::kRateSmem, st>>>(iters / 8 + 1);  // warm-up
+    cudaEventRecord(a, st);
+    kern<<<sms, lc::kRateThreads, lc::kRateSmem, st>>>(iters);
+    cudaEventRecord(b, st);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&t, a, b);
+  if (e == cudaSuccess) e = cudaMemcpy(&flag, err, 4, cudaMemcpyDeviceToHost);
+  if (a) cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
+  if (st) cudaStreamDestroy(st);
+  if (e != cudaSuccess) return lc::map_cuda(e);
+  if (flag) return LC_ERR_TIMEOUT;
+  *ops_per_s = 2.0 * 128 * 256 * 32 * 4 * (double)iters * sms / (t * 1e-3);
+  if (ms) *ms = t;
+  return LC_OK;
+}
+
+}  // extern "C"

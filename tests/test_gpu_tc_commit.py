@@ -158,3 +158,18 @@ def test_tc_config3_full_batch():
     Wh = W[idx].cpu().numpy()
     assert np.array_equal(tc[idx].cpu().numpy().view(np.uint64), oracle_commit(A, kappa, m, Wh))
     assert _lib.lib().lc_ajtai_key_check(key.handle, None) == 0
+
+
+def test_int8_tensor_rate_measurement():
+    """lc_tc_i8_rate: the INT8 tensor roofline denominator, measured with
+    tcgen05.mma.kind::i8 of the engines' shape; positive, bounded by a few
+    times the dense specification (4.5e15 ops/s), errors on bad arguments."""
+    import ctypes as C
+    L = _lib.lib()
+    rate, ms = C.c_double(0.0), C.c_float(0.0)
+    for s8 in (1, 0):
+        assert L.lc_tc_i8_rate(4096, s8, C.byref(rate), C.byref(ms)) == 0
+        assert ms.value > 0
+        assert 1e14 < rate.value < 1e16
+    assert L.lc_tc_i8_rate(0, 1, C.byref(rate), None) == _lib.LC_ERR_INVALID_ARGUMENT
+    assert L.lc_tc_i8_rate(16, 1, None, None) == _lib.LC_ERR_INVALID_ARGUMENT
