@@ -23,13 +23,18 @@
 // columns).  The rotation tiles are Toeplitz: row r of the 64-byte K block of
 // ring element j is the window F[63-r .. 126-r] of the 127-byte source
 //   F[v] = limb(a[63-v]) (v < 64),  limb(p - a[127-v]) (64 <= v < 127),
-// so the key is stored as F rows (128 bytes, zero tail) and builder threads
-// expand them: rows r = 4q+3 start 4-byte aligned, one thread loads 5 words
-// and emits rows 4q..4q+3 with compile-time funnel shifts.
+// so the key is stored as F rows (128 bytes, zero tail).  With the operand
+// rows in reversed coefficient order r' = 63 - r, the 8-row x 16-byte block
+// (g, c) of a tile depends on u = g + 2c only: C_u, row x = F[8u + x ..
+// 8u + x + 16).  The builders store the 14 blocks C_u of each row i (7 KB per
+// limb and ring element instead of a 16 KB tile) and the MMA reads the tile
+// through a no-swizzle K-major descriptor that revisits them (8-row group
+// 4g + i at 128 (4g + i), next K chunk at +1024); one thread loads 5 aligned
+// words and emits 4 rows of a block with funnel shifts.
 //
-// Warp roles: 0-7 build rotation tiles (and drain TMEM at the end), 8 issues
+// Warp roles: 0-7 build rotation blocks (and drain TMEM at the end), 8 issues
 // the TMA loads, 9 owns TMEM and issues the MMAs.  Rings: 4 slots of
-// (W tile + F rows), 2 slots of rotation tiles; mbarrier hand-offs, every
+// (W tile + F rows), 4 slots of rotation blocks; mbarrier hand-offs, every
 // wait bounded (on expiry the kernel records LC_DEVERR_TIMEOUT, waits --
 // again bounded -- for its copies and MMAs in flight, frees TMEM, returns).
 #include <cuda.h>
@@ -54,12 +59,19 @@ struct TcJPer {
 };
 constexpr int kTcFRow = 128;             // bytes per F row
 constexpr int kTcWBytes = 128 * 128;     // W tile: 128 witnesses x 128 bytes (2 ring elements)
-constexpr int kTcRotBytes = 256 * 128;   // one limb's rotation tile: 256 rows x 128 bytes
+// One limb's rotation operand for one ring element, compact: with the
+// coefficient order reversed (r' = 63 - r) the 8-row x 16-byte block (g, c)
+// of the Toeplitz tile is C_u, u = g + 2c, row x = F[8u + x .. 8u + x + 16);
+// C_u of row i sits at (4u + i) * 128, so the no-swizzle K-major descriptor
+// with SBO = 128 (8-row group 4g + i) and LBO = 1024 (next 16-byte K chunk)
+// walks the full 256 x 64 tile over 14 x 4 blocks.
+constexpr int kTcRotBytes = 14 * 4 * 128;  // 7 KB
 constexpr int kTcFHalf = 8 * kTcFRow + 64;  // rows of one ring element; +64 B skews banks
 constexpr int kTcFSlot = 2 * kTcFHalf;
-constexpr int kTcWSlots = 4, kTcRotSlots = 2;
+// (at most 4 rotation slots: the builders wait on the 4-slot mma_done ring)
+constexpr int kTcWSlots = 4, kTcRotSlots = 4;
 constexpr int kTcOffRot = kTcWSlots * kTcWBytes;
-constexpr int kTcOffF = kTcOffRot + kTcRotSlots * 2 * kTcRotBytes;
+constexpr int kTcOffF = kTcOffRot + kTcRotSlots * 4 * kTcRotBytes;  // slot: 2 limbs x 2 ring elements
 constexpr int kTcOffBar = kTcOffF + kTcWSlots * kTcFSlot;
 constexpr size_t kTcSmem = 1024 + kTcOffBar + 256;
 constexpr int kTcThreads = 320;
@@ -78,6 +90,17 @@ LC_D uint64_t umma_desc_sw128(uint32_t saddr) {
   d |= (uint64_t)(1024 >> 4) << 32;         // stride byte offset
   d |= (uint64_t)1 << 46;                   // descriptor version
   d |= (uint64_t)2 << 61;                   // layout: 128-byte swizzle
+  return d;
+}
+
+// K-major operand without swizzle: 8-row x 16-byte core matrices, `lbo`
+// bytes to the next one along K, `sbo` bytes to the next 8-row group.
+LC_D uint64_t umma_desc_noswz(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version; layout 0: no swizzle
   return d;
 }
 
@@ -179,9 +202,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   uint64_t* bars = reinterpret_cast<uint64_t*>(base + kTcOffBar);
   uint64_t* loaded = bars;         // [4] W + F of a stage landed (tx bytes)
   uint64_t* mma_done = bars + 4;   // [4] tcgen05.commit of a stage
-  uint64_t* built = bars + 8;      // [2] 8 builder-warp arrivals
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 10);
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 11);
+  uint64_t* built = bars + 8;      // [kTcRotSlots] 8 builder-warp arrivals
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 8 + kTcRotSlots);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 9 + kTcRotSlots);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t lp = blockIdx.x, g = blockIdx.y;
@@ -195,8 +218,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       mbar_init(&loaded[s], 1);
       mbar_init(&mma_done[s], 1);
     }
-    mbar_init(&built[0], 8);
-    mbar_init(&built[1], 8);
+    for (int r = 0; r < kTcRotSlots; ++r) mbar_init(&built[r], 8);
     *abort_flag = 0;
     fence_mbar_init();
   }
@@ -211,7 +233,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   const uint32_t tmem = *tmem_slot;
 
   auto w_slot = [&](int s) { return base + (s & 3) * kTcWBytes; };
-  auto rot_slot = [&](int s, int ll) { return base + kTcOffRot + ((s & 1) * 2 + ll) * kTcRotBytes; };
+  auto rot_slot = [&](int s, int ll, int jj) {
+    return base + kTcOffRot + (((s % kTcRotSlots) * 2 + ll) * 2 + jj) * kTcRotBytes;
+  };
   auto f_slot = [&](int s) { return base + kTcOffF + (s & 3) * kTcFSlot; };
   auto fail = [&]() {
     record_error(p.err, LC_DEVERR_TIMEOUT);
@@ -242,7 +266,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     // ---------------- MMA issuer
     if (lane == 0) {
       for (int s = 0; s < nst && !*abort_flag; ++s) {
-        if (!mbar_wait(&loaded[s & 3], (s >> 2) & 1) || !mbar_wait(&built[s & 1], (s >> 1) & 1)) {
+        if (!mbar_wait(&loaded[s & 3], (s >> 2) & 1) ||
+            !mbar_wait(&built[s % kTcRotSlots], (uint32_t)((s / kTcRotSlots) & 1))) {
           fail();
           break;
         }
@@ -250,11 +275,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const uint32_t wa = smem_u32(w_slot(s));
 #pragma unroll
         for (int ll = 0; ll < 2; ++ll) {
-          const uint32_t ra = smem_u32(rot_slot(s, ll));
 #pragma unroll
-          for (int ks = 0; ks < 4; ++ks)
-            mma_i8(tmem + ll * 256, umma_desc_sw128(wa + 32 * ks), umma_desc_sw128(ra + 32 * ks),
+          for (int ks = 0; ks < 4; ++ks) {
+            // K step ks: ring element ks / 2, its 16-byte chunks 2 (ks % 2) and 2 (ks % 2) + 1
+            const uint32_t ra = smem_u32(rot_slot(s, ll, ks >> 1)) + 2 * (ks & 1) * 1024;
+            mma_i8(tmem + ll * 256, umma_desc_sw128(wa + 32 * ks), umma_desc_noswz(ra, 1024, 128),
                    TcIdesc<S8>::value, (s > 0 || ks > 0) ? 1u : 0u);
+          }
         }
         mma_commit(&mma_done[s & 3]);
         last_mma = s;
@@ -262,42 +289,44 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
   } else {
     // ---------------- builders
-    // lane: c_lo = 16-byte chunk within the ring element's 64 bytes, q_lo =
-    // low two bits of the 4-row group q, jj = ring element of the stage.
-    const uint32_t c_lo = lane & 3, q_lo = (lane >> 2) & 3, jj = lane >> 4;
+    // Warp-round (2 per stage) = one (limb ll, ring element jj, row i); lane
+    // 2u + h (< 28) writes rows 4h .. 4h + 3 of C_u from 5 aligned words of
+    // the F row.  Row order rho = (t + u) & 3 per store keeps the 8 lanes of a
+    // quarter-warp on 8 distinct 16-byte bank groups; the loads (one F row per
+    // warp, 28 distinct words) are conflict free.
+    const uint32_t u = lane >> 1, h = lane & 1;
     for (int s = 0; s < nst; ++s) {
       bool ok = true;
-      if (s >= 2) ok = mbar_wait(&mma_done[(s - 2) & 3], ((s - 2) >> 2) & 1);  // rotation slot free
+      if (s >= kTcRotSlots)  // rotation slot free: the MMAs of stage s - kTcRotSlots are done
+        ok = mbar_wait(&mma_done[(s - kTcRotSlots) & 3], (uint32_t)(((s - kTcRotSlots) >> 2) & 1));
       ok = ok && mbar_wait(&loaded[s & 3], (s >> 2) & 1);
       if (!ok) fail();
       // warp-uniform: the loop below synchronises the warp
       if (__any_sync(0xffffffffu, *abort_flag)) break;
-      const unsigned char* fbase = f_slot(s) + jj * kTcFHalf;
 #pragma unroll
-      for (int it = 0; it < 4; ++it) {
-        // wc: bits 0-1 = q_hi, 2-3 = ii, 4 = ll
-        const uint32_t wc = warp * 4 + it;
-        const uint32_t q = (wc & 3) * 4 + q_lo, ii = (wc >> 2) & 3, ll = wc >> 4;
-        const unsigned char* frow = fbase + (ll * 4 + ii) * kTcFRow;
-        const uint32_t off = 60 - 4 * q + 16 * c_lo;  // window of row 4q+3, 4-byte aligned
-        uint32_t w[5];
+      for (int rd = 0; rd < 2; ++rd) {
+        const uint32_t combo = 2 * warp + rd;  // bits: 0-1 row i, 2 ring element jj, 3 limb ll
+        const uint32_t ii = combo & 3, jj = (combo >> 2) & 1, ll = combo >> 3;
+        if (lane < 28) {
+          const uint32_t* frow =
+              reinterpret_cast<const uint32_t*>(f_slot(s) + jj * kTcFHalf + (ll * 4 + ii) * kTcFRow);
+          uint32_t w[5];
 #pragma unroll
-        for (int e = 0; e < 5; ++e) w[e] = *reinterpret_cast<const uint32_t*>(frow + off + 4 * e);
-        unsigned char* tile = rot_slot(s, ll);
-        const uint32_t c = jj * 4 + c_lo;
+          for (int e = 0; e < 5; ++e) w[e] = frow[2 * u + h + e];  // word 2u + h + 4 <= 31
+          unsigned char* blk = rot_slot(s, (int)ll, (int)jj) + (4 * u + ii) * 128;
 #pragma unroll
-        for (int rho = 0; rho < 4; ++rho) {
-          const int delta = 3 - rho;  // row 4q+rho starts delta bytes later
-          uint32_t o[4];
+          for (int t = 0; t < 4; ++t) {
+            const uint32_t rho = (t + u) & 3, x = 4 * h + rho;
+            uint32_t o[4];
 #pragma unroll
-          for (int t = 0; t < 4; ++t) o[t] = delta == 0 ? w[t] : __funnelshift_r(w[t], w[t + 1], 8 * delta);
-          const uint32_t n = ii * 64 + 4 * q + rho;
-          *reinterpret_cast<uint4*>(tile + n * 128 + ((c ^ (n & 7)) << 4)) = make_uint4(o[0], o[1], o[2], o[3]);
+            for (int q = 0; q < 4; ++q) o[q] = __funnelshift_r(w[q], w[q + 1], 8 * rho);
+            *reinterpret_cast<uint4*>(blk + 16 * x) = make_uint4(o[0], o[1], o[2], o[3]);
+          }
         }
       }
       fence_proxy_async_smem();
       __syncwarp();
-      if (lane == 0) mbar_arrive(&built[s & 1]);
+      if (lane == 0) mbar_arrive(&built[s % kTcRotSlots]);
     }
   }
 
@@ -321,8 +350,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         tmem_ld16(tmem + (lane_base << 16) + 256 + col, d1);
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-        for (int u = 0; u < 16; ++u)
-          out[(size_t)(col + u) * 128 + b_local] = (int64_t)(int32_t)d0[u] + 256 * (int64_t)(int32_t)d1[u];
+        for (int u = 0; u < 16; ++u) {
+          // operand row n = 8 (4g + i) + x holds row i, coefficient r = 63 - (8g + x)
+          const uint32_t n = col + u;
+          const uint32_t nr = ((n >> 3) & 3) * 64 + 63 - (8 * (n >> 5) + (n & 7));
+          out[(size_t)nr * 128 + b_local] = (int64_t)(int32_t)d0[u] + 256 * (int64_t)(int32_t)d1[u];
+        }
       }
     }
   }
