@@ -305,8 +305,16 @@ def bench_commit(args, rank, max_over_ranks, barrier, world):
     outs = {}
     res = {"workload": C_WORKLOAD, "unit": "ring-elems/s",
            "alg_mul_adds_per_batch": C_KAPPA * C_M * C_D * C_B}
-    for name, engine in (("plain", GoldilocksAjtaiKey.ENGINE_NTT), ("tensor", GoldilocksAjtaiKey.ENGINE_TENSOR_I8)):
+    # plain: the cached-NTT engine with 160-bit integer products on the CUDA cores;
+    # tensor: the coefficient-domain limb-split engine, rot(A) . W on the INT8 tensor
+    # cores; ntt_tensor_products: the cached-NTT engine with its per-slot products as
+    # byte-limb GEMMs on the INT8 tensor cores (the NTT engine's default)
+    for name, engine, products in (("plain", GoldilocksAjtaiKey.ENGINE_NTT, GoldilocksAjtaiKey.PRODUCTS_INT64),
+                                   ("tensor", GoldilocksAjtaiKey.ENGINE_TENSOR_I8, GoldilocksAjtaiKey.PRODUCTS_TENSOR),
+                                   ("ntt_tensor_products", GoldilocksAjtaiKey.ENGINE_NTT,
+                                    GoldilocksAjtaiKey.PRODUCTS_TENSOR)):
         key.engine = engine
+        key.slot_products = products
         out = torch.empty((C_B, C_KAPPA, C_D), dtype=torch.int64, device="cuda")
         op = C.c_void_p(out.data_ptr())
         for _ in range(3):
@@ -340,6 +348,7 @@ def bench_commit(args, rank, max_over_ranks, barrier, world):
                              "h2d_bytes_per_step": C_B * C_M * C_D,
                              "d2h_bytes_per_step": C_B * C_KAPPA * C_D * 8}}
     assert torch.equal(outs["plain"], outs["tensor"]), "tensor engine differs from the NTT engine"
+    assert torch.equal(outs["plain"], outs["ntt_tensor_products"]), "tensor slot products differ"
     # tensor engine: 8 byte-limb GEMMs of B x (kappa*64) x (m*64) int8 multiply-adds
     ops = 2 * 8 * C_B * (C_KAPPA * C_D) * (C_M * C_D)
     bf16, kind = bf16_peak()
@@ -359,6 +368,12 @@ def bench_commit(args, rank, max_over_ranks, barrier, world):
                                  "frac_of_2x_bf16": ach / (2 * bf16),
                                  "bf16_source": f"{kind} bf16 burst {bf16} TFLOP/s"}
     res["speedup_tensor_vs_plain"] = res["plain"]["ms_per_batch"] / res["tensor"]["ms_per_batch"]
+    res["speedup_ntt_tensor_products_vs_plain"] = (res["plain"]["ms_per_batch"] /
+                                                   res["ntt_tensor_products"]["ms_per_batch"])
+    # slot products: 8 x 8 byte-limb GEMMs per NTT slot, M = 16 rows x 8 limbs,
+    # N = B witnesses x 8 limbs, K = m ring elements
+    sp_ops = 2 * C_D * (16 * 8) * (8 * C_B) * C_M
+    res["ntt_tensor_products"]["slot_product_int8_ops_per_batch"] = sp_ops
     del W
     if rank == 0 and not args.no_cpu_baseline:
         import oracle
@@ -402,7 +417,13 @@ def bench_fold(args, rank, max_over_ranks, barrier, world):
     crt = NttTables(CRT_SET_30BIT, 6)
     res = {"workload": F_WORKLOAD, "m": m, "unit": "witness ring-elems/s"}
     K = max(1, args.fold_steps)
-    for name, graph in (("eager", False), ("graph", True)):
+    commits = {}
+    # eager / graph: the commits' slot products on the tensor cores (the default);
+    # graph_int64_products: the same step with 160-bit CUDA-core products
+    for name, graph, products in (("eager", False, GoldilocksAjtaiKey.PRODUCTS_TENSOR),
+                                  ("graph", True, GoldilocksAjtaiKey.PRODUCTS_TENSOR),
+                                  ("graph_int64_products", True, GoldilocksAjtaiKey.PRODUCTS_INT64)):
+        key.slot_products = products
         pipe = FoldPipeline(key, crt, use_graph=graph)
         synth.fill_device(pipe.z, "gl", 97 + rank, 1)
         for _ in range(3):
@@ -419,7 +440,8 @@ def bench_fold(args, rank, max_over_ranks, barrier, world):
         pipe.check()
         ms = max_over_ranks(a.elapsed_time(b) / K)
         res[name] = {"ms_per_step": ms, "value": world * m / (ms / 1e3), "steps": K}
-        if graph:
+        commits[name] = pipe.commits.clone()
+        if name == "graph":
             # end to end: z from pinned host memory in, commitments and CRT NTT out
             hz = torch.empty((m, 64), dtype=torch.int64).pin_memory()
             hz.copy_(pipe.z.cpu())
@@ -440,6 +462,10 @@ def bench_fold(args, rank, max_over_ranks, barrier, world):
                                    "h2d_bytes_per_step": m * 64 * 8,
                                    "d2h_bytes_per_step": hc.numel() * 8 + ht.numel() * 4}
         del pipe
+    key.slot_products = GoldilocksAjtaiKey.PRODUCTS_TENSOR
+    assert torch.equal(commits["graph"], commits["graph_int64_products"]), "slot product forms differ"
+    assert torch.equal(commits["eager"], commits["graph"])
+    del commits
     if rank == 0 and not args.no_cpu_baseline:
         import numpy as np
 

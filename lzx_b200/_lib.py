@@ -33,6 +33,8 @@ LC_ERR_GENERATOR_INVALID = 14
 LC_KEY_TENSOR_I8 = 1
 LC_ENGINE_NTT = 0
 LC_ENGINE_TENSOR_I8 = 1
+LC_PRODUCTS_INT64 = 0
+LC_PRODUCTS_TENSOR = 1
 LC_BATCH_GRAPH = 1
 
 
@@ -88,6 +90,8 @@ def _declare(L):
         "lc_ajtai_key_set_fused": (i32, [P, i32]),
         "lc_tc_i8_rate": (i32, [u32, i32, C.POINTER(C.c_double), C.POINTER(C.c_float)]),
         "lc_ajtai_key_get_fused": (i32, [P]),
+        "lc_ajtai_key_set_slot_products": (i32, [P, i32]),
+        "lc_ajtai_key_get_slot_products": (i32, [P]),
         "lc_ajtai_commit_u8": (i32, [P, P, sz, P, P]),
         "lc_ajtai_commit_u8_host": (i32, [P, P, sz, P]),
         "lc_decomp_b": (i32, [P, sz, u32, P, P]),

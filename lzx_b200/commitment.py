@@ -92,6 +92,15 @@ class _DeviceKey:
     def fused(self, value: bool):
         check(_lib.lib().lc_ajtai_key_set_fused(self._h, 1 if value else 0), "lc_ajtai_key_set_fused")
 
+    @property
+    def slot_products(self) -> int:
+        """LC_PRODUCTS_TENSOR or LC_PRODUCTS_INT64 (lc_ajtai_key_set_slot_products)."""
+        return _lib.lib().lc_ajtai_key_get_slot_products(self._h)
+
+    @slot_products.setter
+    def slot_products(self, value: int):
+        check(_lib.lib().lc_ajtai_key_set_slot_products(self._h, int(value)), "lc_ajtai_key_set_slot_products")
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and _lib._lib is not None:
@@ -319,6 +328,19 @@ class GoldilocksAjtaiKey:
     @fused.setter
     def fused(self, value: bool):
         self._dev.fused = value
+
+    PRODUCTS_INT64 = _lib.LC_PRODUCTS_INT64
+    PRODUCTS_TENSOR = _lib.LC_PRODUCTS_TENSOR
+
+    @property
+    def slot_products(self) -> int:
+        """Per-slot products of the NTT engine: PRODUCTS_TENSOR (byte-limb GEMMs on
+        the tensor cores, the default) or PRODUCTS_INT64 (CUDA-core integer MAC)."""
+        return self._dev.slot_products
+
+    @slot_products.setter
+    def slot_products(self, value: int):
+        self._dev.slot_products = value
 
     def commit(self, w, out=None):
         return self._dev.commit_array(w, out)

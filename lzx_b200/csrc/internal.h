@@ -97,6 +97,7 @@ struct lc_ajtai_key {
   size_t fused_bytes = 0;
   bool fused = true;        // small commits as one launch (lc_ajtai_key_set_fused)
   bool last_fused = false;  // the last commit on this key ran as one launch
+  int slot_products = LC_PRODUCTS_TENSOR;  // lc_ajtai_key_set_slot_products
   void* d_in = nullptr;  // host-API staging
   size_t in_bytes = 0;
   void* d_out = nullptr;
@@ -136,4 +137,12 @@ int tc_commit(lc_tc_tables* t, const void* w, bool s8, size_t batch, uint64_t* o
 int tc_ntt_prepare();
 int tc_witness_ntt(const void* w, bool s8, size_t batch, uint32_t m, uint32_t b_pad, uint64_t* what_t,
                    uint32_t* err, cudaStream_t st);
+// Goldilocks per-slot products Chat[b][i][t] = sum_j Ahat_T[t][j][i] What_T[t][j][b]
+// (mod p) as exact byte-limb GEMMs on the INT8 tensor cores (n slots, m ring
+// elements, a_m the key's row stride); scratch grown in *part.
+// LC_ERR_UNSUPPORTED for batch paddings it does not take (8, 16, 32 and
+// multiples of 64 are taken).
+int tc_slot_products(const uint64_t* ahat_t, uint32_t a_m, const uint64_t* what_t, uint32_t m, uint32_t n,
+                     uint32_t kappa, size_t batch, uint32_t b_pad, void** part, size_t* part_bytes,
+                     uint64_t* chat, uint32_t* err, cudaStream_t st);
 }  // namespace lc

@@ -834,6 +834,309 @@ int tc_witness_ntt(const void* w, bool s8, size_t batch, uint32_t m, uint32_t b_
 
 }  // namespace lc
 
+namespace lc {
+
+// ------------------------------------------------------------------ slot products on the tensor cores
+//
+// The NTT engine's per-slot products C_t[i][b] = sum_j Ahat[i][j][t] What[b][j][t]
+// (mod p) as exact unsigned byte GEMMs.  With both residues split into byte
+// limbs, C_t = sum_{la,lw} 2^(8 (la + lw)) D_t[(i,la)][(b,lw)] and
+//   D_t[(i,la)][(b,lw)] = sum_j Ahat_la[i][j][t] * What_lw[b][j][t]   (u8 x u8 -> s32),
+// exact for at most 32768 ring elements j per sum (32768 * 255^2 < 2^31).
+// The cached key Ahat_T[t][j][16] (u64) is, read as bytes, the A operand of
+// slot t in MN-major form: row j (the K index) holds the 128 bytes (i, la),
+// la fastest; What_T[t][j][b_pad] is the B operand the same way, 8 b_pad
+// bytes (b, lw) per row.  3-D TMA maps (x = bytes of a row, y = j < m, z =
+// slot) load 64-row stages with the 128-byte (64-byte for 8 witnesses)
+// swizzle, the MN-major canonical layout of the MMA descriptors (SBO = 8
+// rows, LBO = next 128-byte atom along N); rows past m read as zero.  CTA
+// (slot, N tile of up to 512 bytes, K split): one TMA thread, one MMA thread
+// (M = 128, N <= 256 per accumulator, K = 32), four epilogue warps writing
+// D transposed so that the lanes (rows (i, la)) store contiguously; a second
+// kernel sums the splits and limbs and reduces mod p into Chat[b][i][t].
+constexpr int kSpStages = 4;
+constexpr int kSpRows = 64;          // K rows (ring elements j) per stage
+constexpr uint32_t kSpKSplit = 32768;  // ring elements per exact int32 sum
+constexpr int kSpThreads = 192;      // warp 0 TMA, 1 MMA + TMEM, 2..5 epilogue
+
+template <int NCTA>
+struct SpCfg {
+  static constexpr int SW = NCTA >= 128 ? 128 : 64;  // B swizzle atom (bytes of a row)
+  static constexpr int ATOMS = NCTA / SW;
+  static constexpr int MMA_N = NCTA > 256 ? 256 : NCTA;
+  static constexpr int ACCS = NCTA / MMA_N;
+  static constexpr int A_BYTES = kSpRows * 128;
+  static constexpr int B_ATOM = kSpRows * SW;
+  static constexpr int STAGE = A_BYTES + ATOMS * B_ATOM;
+  static constexpr size_t SMEM = 1024 + (size_t)kSpStages * STAGE + 128;
+  static_assert(STAGE % 1024 == 0 && B_ATOM % 512 == 0, "swizzle atoms stay aligned");
+  static_assert(SMEM <= 227 * 1024, "shared memory");
+};
+
+// MN-major operand: LBO = bytes to the next atom along M/N, SBO = bytes to
+// the next 8-row group along K; layout 2 = 128-byte swizzle, 4 = 64-byte.
+LC_D uint64_t umma_desc_mn(uint32_t saddr, uint32_t lbo, uint32_t sbo, uint32_t layout) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)layout << 61;
+  return d;
+}
+
+// D = s32, A = B = u8, both MN-major (bits 15, 16), M = 128
+template <int N>
+struct SpIdesc {
+  static constexpr uint32_t value =
+      (2u << 4) | (1u << 15) | (1u << 16) | ((uint32_t)(N >> 3) << 17) | ((128u >> 4) << 24);
+};
+
+struct SpParams {
+  int32_t* partial;  // [split][t][ntile][NCTA][128]
+  uint32_t m, nslots, ntiles, splits;
+  uint32_t* err;
+};
+
+template <int NCTA>
+__global__ void __launch_bounds__(kSpThreads, 1)
+    slot_products_kernel(const __grid_constant__ CUtensorMap amap, const __grid_constant__ CUtensorMap wmap,
+                         const __grid_constant__ SpParams p) {
+  using C = SpCfg<NCTA>;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char* base =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + kSpStages * C::STAGE);
+  uint64_t* full = bars;                   // [4] stage landed (tx bytes)
+  uint64_t* empty = bars + kSpStages;      // [4] its MMAs finished
+  uint64_t* done = bars + 2 * kSpStages;   // every MMA finished
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kSpStages + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 2 * kSpStages + 2);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t t = blockIdx.x, nt = blockIdx.y, split = blockIdx.z;
+  const uint32_t j0 = split * kSpKSplit;
+  const uint32_t j1 = min(p.m, j0 + kSpKSplit);
+  const int nst = (int)((j1 - j0 + kSpRows - 1) / kSpRows);
+
+  if (tid == 0) {
+    for (int s = 0; s < kSpStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(NCTA));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  auto stage = [&](int s) { return base + (s % kSpStages) * C::STAGE; };
+  auto fail = [&]() {
+    record_error(p.err, LC_DEVERR_TIMEOUT);
+    *abort_flag = 1;
+  };
+  int last_loaded = -1, last_mma = -1;
+
+  if (warp == 0) {
+    // ---------------- TMA: A rows (i, la) and the B atoms of this N tile
+    if (lane == 0) {
+      for (int s = 0; s < nst && !*abort_flag; ++s) {
+        if (s >= kSpStages && !mbar_wait(&empty[s % kSpStages], (uint32_t)(((s - kSpStages) / kSpStages) & 1))) {
+          fail();
+          break;
+        }
+        unsigned char* st = stage(s);
+        const int y = (int)(j0 + kSpRows * s);
+        mbar_arrive_expect_tx(&full[s % kSpStages], (uint32_t)C::STAGE);
+        tma_load_3d(st, &amap, 0, y, (int)t, &full[s % kSpStages]);
+#pragma unroll
+        for (int a = 0; a < C::ATOMS; ++a)
+          tma_load_3d(st + C::A_BYTES + a * C::B_ATOM, &wmap, (int)(nt * NCTA + a * C::SW), y, (int)t,
+                      &full[s % kSpStages]);
+        last_loaded = s;
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer
+    if (lane == 0) {
+      constexpr uint32_t kBLayout = C::SW == 128 ? 2u : 4u;
+      for (int s = 0; s < nst && !*abort_flag; ++s) {
+        if (!mbar_wait(&full[s % kSpStages], (uint32_t)((s / kSpStages) & 1))) {
+          fail();
+          break;
+        }
+        tc_fence_after();
+        const uint32_t sa = smem_u32(stage(s)), sb = sa + C::A_BYTES;
+#pragma unroll
+        for (int ks = 0; ks < kSpRows / 32; ++ks) {
+#pragma unroll
+          for (int acc = 0; acc < C::ACCS; ++acc) {
+            const uint64_t ad = umma_desc_mn(sa + ks * 32 * 128, C::B_ATOM, 8 * 128, 2u);
+            const uint64_t bd = umma_desc_mn(sb + acc * (C::MMA_N / C::SW) * C::B_ATOM + ks * 32 * C::SW,
+                                             C::B_ATOM, 8 * C::SW, kBLayout);
+            mma_i8(tmem + acc * C::MMA_N, ad, bd, SpIdesc<C::MMA_N>::value, (s > 0 || ks > 0) ? 1u : 0u);
+          }
+        }
+        mma_commit(&empty[s % kSpStages]);
+        last_mma = s;
+      }
+      if (last_mma >= 0) mma_commit(done);
+    }
+  } else {
+    // ---------------- epilogue: lane = row (i, la); column = (b, lw)
+    const bool ok = nst > 0 && !*abort_flag && mbar_wait(done, 0);
+    if (__all_sync(0xffffffffu, ok)) {
+      tc_fence_after();
+      const uint32_t lq = warp & 3, row = 32 * lq + lane;
+      int32_t* out = p.partial + (((size_t)split * p.nslots + t) * p.ntiles + nt) * (size_t)NCTA * 128;
+#pragma unroll 1
+      for (int c0 = 0; c0 < NCTA; c0 += 16) {
+        uint32_t d[16];
+        tmem_ld16(tmem + ((32 * lq) << 16) + c0, d);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int u = 0; u < 16; ++u) out[(size_t)(c0 + u) * 128 + row] = (int32_t)d[u];
+      }
+    } else if (nst > 0 && lane == 0) {
+      fail();
+    }
+  }
+  // ---------------- nothing in flight when TMEM and shared memory go
+  __syncthreads();
+  if (warp == 0 && lane == 0) {
+    for (int s = max(0, last_loaded - (kSpStages - 1)); s <= last_loaded; ++s)
+      mbar_wait(&full[s % kSpStages], (uint32_t)((s / kSpStages) & 1));
+  }
+  if (warp == 1 && lane == 0 && last_mma >= 0) mbar_wait(done, 0);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCTA));
+  }
+}
+
+// Chat[b][i][t] = sum_{la,lw} 2^(8 (la + lw)) sum_split D[split][t][nt][(bl, lw)][(i, la)]  mod p.
+// Pair sums over the splits fit 64 bits (< 2^31 * splits); the 15 sums of equal
+// la + lw = k (< 2^42) are folded with 2^(8k) mod p in 128 bits.
+__global__ void slot_products_reduce_kernel(const int32_t* __restrict__ part, uint64_t* __restrict__ chat,
+                                            uint32_t n, uint32_t kappa, uint32_t batch, uint32_t ncta,
+                                            uint32_t ntiles, uint32_t splits) {
+  const size_t total = (size_t)n * batch * kappa;
+  const uint32_t wpt = ncta / 8;  // witnesses per N tile
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t i = idx % kappa;
+    const uint32_t b = (uint32_t)((idx / kappa) % batch);
+    const uint32_t t = (uint32_t)(idx / ((size_t)kappa * batch));
+    const uint32_t nt = b / wpt, bl = b % wpt;
+    uint64_t tk[15];
+#pragma unroll
+    for (int k = 0; k < 15; ++k) tk[k] = 0;
+    for (uint32_t sp = 0; sp < splits; ++sp) {
+      const int32_t* d = part + (((size_t)sp * n + t) * ntiles + nt) * (size_t)ncta * 128;
+#pragma unroll
+      for (int lw = 0; lw < 8; ++lw) {
+        const int32_t* col = d + (size_t)(bl * 8 + lw) * 128 + i * 8;
+#pragma unroll
+        for (int la = 0; la < 8; ++la) tk[la + lw] += (uint64_t)(uint32_t)col[la];
+      }
+    }
+    unsigned __int128 v = 0;
+    uint64_t c = 1;  // 2^(8k) mod p
+#pragma unroll
+    for (int k = 0; k < 15; ++k) {
+      v += (unsigned __int128)tk[k] * c;
+      c = gl_mul(c, 256);
+    }
+    chat[((size_t)b * kappa + i) * n + t] = gl_canon(gl_reduce128_lazy((uint64_t)(v >> 64), (uint64_t)v));
+  }
+}
+
+template <int NCTA>
+static int launch_slot_products(const CUtensorMap& amap, const CUtensorMap& wmap, const SpParams& prm,
+                                cudaStream_t st) {
+  auto kern = slot_products_kernel<NCTA>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SpCfg<NCTA>::SMEM);
+  if (e != cudaSuccess) return map_cuda(e);
+  kern<<<dim3(prm.nslots, prm.ntiles, prm.splits), kSpThreads, SpCfg<NCTA>::SMEM, st>>>(amap, wmap, prm);
+  return map_cuda(cudaGetLastError());
+}
+
+int tc_slot_products(const uint64_t* ahat_t, uint32_t a_m, const uint64_t* what_t, uint32_t m, uint32_t n,
+                     uint32_t kappa, size_t batch, uint32_t b_pad, void** part, size_t* part_bytes,
+                     uint64_t* chat, uint32_t* err, cudaStream_t st) {
+  if (batch == 0) return LC_OK;
+  EncodeTiledFn enc = encode_fn();
+  if (!enc || kappa > 16 || m == 0) return LC_ERR_UNSUPPORTED;
+  uint32_t ncta;
+  if (b_pad % 64 == 0)
+    ncta = 512;
+  else if (b_pad == 32 || b_pad == 16 || b_pad == 8)
+    ncta = 8 * b_pad;
+  else
+    return LC_ERR_UNSUPPORTED;
+  const uint32_t ntiles = 8 * b_pad / ncta;
+  const uint32_t splits = (m + kSpKSplit - 1) / kSpKSplit;
+  if ((size_t)n * ntiles > 65535 || splits > 65535) return LC_ERR_UNSUPPORTED;
+  const size_t need = (size_t)splits * n * ntiles * ncta * 128 * sizeof(int32_t);
+  if (need > *part_bytes) {
+    if (*part) cudaFree(*part);
+    *part = nullptr;
+    *part_bytes = 0;
+    if (cudaMalloc(part, need) != cudaSuccess) {
+      cudaGetLastError();
+      return LC_ERR_OUT_OF_MEMORY;
+    }
+    *part_bytes = need;
+  }
+  // A: bytes (i, la) of Ahat_T[t][j][16]; B: bytes (b, lw) of What_T[t][j][b_pad]
+  CUtensorMap amap, wmap;
+  const cuuint32_t estr[3] = {1, 1, 1};
+  {
+    const cuuint64_t dims[3] = {128, (cuuint64_t)m, (cuuint64_t)n};
+    const cuuint64_t strides[2] = {128, (cuuint64_t)a_m * 128};
+    const cuuint32_t box[3] = {128, (cuuint32_t)kSpRows, 1};
+    if (enc(&amap, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<uint64_t*>(ahat_t), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return LC_ERR_UNSUPPORTED;
+  }
+  {
+    const cuuint64_t row = (cuuint64_t)b_pad * 8;
+    const cuuint64_t dims[3] = {row, (cuuint64_t)m, (cuuint64_t)n};
+    const cuuint64_t strides[2] = {row, (cuuint64_t)m * row};
+    const cuuint32_t sw = ncta >= 128 ? 128 : 64;
+    const cuuint32_t box[3] = {sw, (cuuint32_t)kSpRows, 1};
+    if (enc(&wmap, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<uint64_t*>(what_t), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, sw == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return LC_ERR_UNSUPPORTED;
+  }
+  const SpParams prm{static_cast<int32_t*>(*part), m, n, ntiles, splits, err};
+  int rc;
+  switch (ncta) {
+    case 512: rc = launch_slot_products<512>(amap, wmap, prm, st); break;
+    case 256: rc = launch_slot_products<256>(amap, wmap, prm, st); break;
+    case 128: rc = launch_slot_products<128>(amap, wmap, prm, st); break;
+    default: rc = launch_slot_products<64>(amap, wmap, prm, st); break;
+  }
+  if (rc) return rc;
+  const size_t total = (size_t)n * batch * kappa;
+  const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, (size_t)device_sm_count() * 16);
+  slot_products_reduce_kernel<<<blocks, 256, 0, st>>>(static_cast<const int32_t*>(*part), chat, n, kappa,
+                                                      (uint32_t)batch, ncta, ntiles, splits);
+  return map_cuda(cudaGetLastError());
+}
+
+}  // namespace lc
+
 // ------------------------------------------------------------------ INT8 tensor rate
 //
 // Measurement kernel for the INT8 tensor roofline: one CTA per SM keeps its
