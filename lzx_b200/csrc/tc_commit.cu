@@ -447,19 +447,21 @@ LC_D void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, ui
       : "memory");
 }
 
-// sum_l 2^(8l) D_l mod p for one output (|D_l| < 2^22)
+// sum_l 2^(8l) D_l mod p for one output (|D_l| < 2^22).  A = D0 + 2^8 D1 +
+// 2^16 D2 + 2^24 D3 and B (limbs 4..7) are exact in int64 (|A|, |B| < 2^47);
+// the value is A + B 2^32 and B 2^32 = lo(B) 2^32 + hi(B) 2^64 with
+// 2^64 == 2^32 - 1 (mod p), |hi(B)| < 2^15.  The offset 2^48 keeps
+// A + hi(B) (2^32 - 1) positive and below 2^49; adding lo(B) 2^32 wraps 2^64
+// at most once, folded as 2^32 - 1; the offset comes off mod p at the end.
 LC_D uint64_t tn_fold(const uint32_t (&d)[8][8], int u) {
-  const int64_t e0 = (int64_t)(int32_t)d[0][u] + (int64_t)(int32_t)d[1][u] * 256 +
-                     (int64_t)(int32_t)d[2][u] * 65536 + (int64_t)(int32_t)d[3][u] * 16777216;
-  const int64_t e1 = (int64_t)(int32_t)d[4][u] + (int64_t)(int32_t)d[5][u] * 256 +
-                     (int64_t)(int32_t)d[6][u] * 65536 + (int64_t)(int32_t)d[7][u] * 16777216;
-  // |e0 + e1 2^32| < 2^79 < p 2^16
-  const __int128 v = (__int128)e1 * ((__int128)1 << 32) + e0 + ((__int128)kGlP << 16);
-  const uint64_t hi = (uint64_t)(v >> 64), lo = (uint64_t)v;  // hi < 2^17
-  const uint64_t t = hi * kGlEps;                              // hi 2^64 == hi (2^32 - 1)
-  uint64_t r = lo + t;
-  if (r < t) r += kGlEps;  // no second carry: lo + t - 2^64 < t < 2^49
-  return gl_canon(r);
+  const int64_t A = (int64_t)(int32_t)d[0][u] + (int64_t)(int32_t)d[1][u] * 256 +
+                    (int64_t)(int32_t)d[2][u] * 65536 + (int64_t)(int32_t)d[3][u] * 16777216;
+  const int64_t B = (int64_t)(int32_t)d[4][u] + (int64_t)(int32_t)d[5][u] * 256 +
+                    (int64_t)(int32_t)d[6][u] * 65536 + (int64_t)(int32_t)d[7][u] * 16777216;
+  const uint64_t t = (uint64_t)(A + (B >> 32) * (int64_t)kGlEps + ((int64_t)1 << 48));  // in (0, 2^49)
+  uint64_t r = t + ((uint64_t)(uint32_t)B << 32);
+  if (r < t) r += kGlEps;  // no second wrap: r < 2^49 after the first
+  return gl_sub(gl_canon(r), (uint64_t)1 << 48);
 }
 
 template <bool S8>
