@@ -55,6 +55,8 @@ def both_products(key, W):
     (6, 3, 777, 32),        # 256
     (6, 16, 513, 64),       # 512
     (6, 7, 257, 200),       # batch padded to 256: two tiles of 512
+    (6, 3, 7, 8),           # fewer ring elements than one 64-row stage
+    (6, 2, 1, 64),          # a single ring element
     (7, 8, 300, 16),
     (8, 2, 129, 64),
 ])
