@@ -763,11 +763,10 @@ static int launch_commit_fused(lc_ajtai_key* key, const S* w, size_t batch, void
     if (rc) return rc;
   }
   auto kern = commit_fused_kernel<A, S, LOG_N, LOG_V>;
-  static bool attr_done = false;
-  if (!attr_done) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+  static std::atomic<uint64_t> attr_done{0};
+  {
+    const cudaError_t e = smem_attr_once(attr_done, kern, C::SMEM);
     if (e != cudaSuccess) return map_cuda(e);
-    attr_done = true;
   }
   // ring elements per CTA: about 16 multiply-adds per thread and at least 8
   // (few atomic additions per product), within one transform pass

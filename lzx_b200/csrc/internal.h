@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "../../include/lattice_cuda.h"
 
 namespace lc {
@@ -114,6 +116,20 @@ struct lc_ajtai_key {
 };
 
 namespace lc {
+// Sets a kernel's dynamic shared-memory limit once per device: `done` keeps
+// one bit per device (the attribute is per device; devices past 63 set it on
+// every call).
+template <class K>
+inline cudaError_t smem_attr_once(std::atomic<uint64_t>& done, K kern, size_t bytes) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return cudaGetLastError();
+  const uint64_t bit = (dev >= 0 && dev < 64) ? (uint64_t)1 << dev : 0;
+  if (bit && (done.load(std::memory_order_relaxed) & bit)) return cudaSuccess;
+  const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_relaxed);
+  return e;
+}
+
 int device_sm_count();
 int map_cuda(cudaError_t e);
 int run_ntt(const lc_ntt_plan* plan, const void* in, void* out, size_t count, bool inverse,

@@ -138,11 +138,10 @@ static int launch_tile_cfg(const NttParams& p, cudaStream_t s) {
   using C = NttKernelCfg<A, LOG_N, LOG_V, NT, IT, STAGES, INV>;
   auto kern = ntt_tile_kernel<A, LOG_N, LOG_V, NT, IT, STAGES, INV, OPT>;
   constexpr size_t smem = C::SMEM;
-  static bool attr_done = false;
-  if (!attr_done) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  static std::atomic<uint64_t> attr_done{0};
+  {
+    const cudaError_t e = smem_attr_once(attr_done, kern, smem);
     if (e != cudaSuccess) return e == cudaErrorInvalidValue ? LC_ERR_UNSUPPORTED : map_cuda(e);
-    attr_done = true;
   }
   int per_sm = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem);
@@ -161,11 +160,10 @@ static int launch_warp_cfg(const NttParams& p, cudaStream_t s) {
   using C = NttWarpCfg<A, LOG_N, LOG_V, WARPS, IT, STAGES, INV>;
   auto kern = ntt_warp_kernel<A, LOG_N, LOG_V, WARPS, IT, STAGES, INV>;
   constexpr size_t smem = C::SMEM;
-  static bool attr_done = false;
-  if (!attr_done) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  static std::atomic<uint64_t> attr_done{0};
+  {
+    const cudaError_t e = smem_attr_once(attr_done, kern, smem);
     if (e != cudaSuccess) return e == cudaErrorInvalidValue ? LC_ERR_UNSUPPORTED : map_cuda(e);
-    attr_done = true;
   }
   int per_sm = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, C::NT, smem);
