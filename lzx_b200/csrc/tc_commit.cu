@@ -595,15 +595,19 @@ __global__ void __launch_bounds__(kTnThreads, 1)
 #pragma unroll
           for (int l = 0; l < 8; ++l) tmem_ld8(tmem + ((32 * q) << 16) + (l >> 2) * 256 + (l & 3) * 64 + t0, d[l]);
           asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          if (tb == 1) {
+            // this warp's accumulator columns are all in registers: the next
+            // ring element's MMAs may overwrite them while the fold runs
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(acc_empty);
+          }
 #pragma unroll
           for (int u = 0; u < 8; ++u) {
             if (valid) *dst = tn_fold(d, u);
             dst += stride;
           }
         }
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(acc_empty);
       }
       if (stop) break;
     }
