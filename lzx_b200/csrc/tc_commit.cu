@@ -1090,7 +1090,7 @@ int tc_slot_products(const uint64_t* ahat_t, uint32_t a_m, const uint64_t* what_
     return LC_ERR_UNSUPPORTED;
   const uint32_t ntiles = 8 * b_pad / ncta;
   const uint32_t splits = (m + kSpKSplit - 1) / kSpKSplit;
-  if ((size_t)n * ntiles > 65535 || splits > 65535) return LC_ERR_UNSUPPORTED;
+  if (ntiles > 65535 || splits > 65535) return LC_ERR_UNSUPPORTED;  // grid y, z
   const size_t need = (size_t)splits * n * ntiles * ncta * 128 * sizeof(int32_t);
   if (need > *part_bytes) {
     if (*part) cudaFree(*part);
