@@ -244,13 +244,14 @@ LC_API int lc_tc_i8_rate(uint32_t iters, int s8, double *ops_per_s, float *ms);
 LC_API int lc_ajtai_key_set_fused(lc_ajtai_key *key, int enable);
 LC_API int lc_ajtai_key_get_fused(const lc_ajtai_key *key);
 
-/* How the NTT engine forms its per-slot products C_t = A_t^T W_t over
- * Goldilocks (staged commits): LC_PRODUCTS_TENSOR (default) as exact byte-limb
- * GEMMs on the INT8 tensor cores -- both residues split into 8 unsigned byte
- * limbs, read in place from the cached NTT(A) and the witness transforms,
- * int32 sums of at most 32768 ring elements, limbs recombined and reduced mod
- * p -- for batch paddings 8, 16, 32 and multiples of 64 (others, and u32
- * keys, use the integer form); LC_PRODUCTS_INT64 with 160-bit integer
+/* How the NTT engine forms its per-slot products C_t = A_t^T W_t (staged
+ * commits): LC_PRODUCTS_TENSOR (default) as exact byte-limb GEMMs on the INT8
+ * tensor cores -- both residues split into unsigned byte limbs (8 for
+ * Goldilocks, 4 for u32 moduli), read in place from the cached NTT(A) and the
+ * witness transforms, int32 sums of at most 32768 ring elements, limbs
+ * recombined and reduced mod q -- whenever a witness row of the transforms
+ * (limbs x padded batch) is 32, 64, 128, 256 or a multiple of 512 bytes (other
+ * paddings use the integer form); LC_PRODUCTS_INT64 with 160-bit integer
  * multiply-accumulates on the CUDA cores.  Identical results.
  * lc_ajtai_key_get_slot_products returns the mode (-1 for a null key). */
 #define LC_PRODUCTS_INT64 0

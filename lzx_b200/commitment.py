@@ -209,6 +209,16 @@ class AjtaiPublicKey:
     def fused(self, value: bool):
         self._dev.fused = value
 
+    @property
+    def slot_products(self) -> int:
+        """Per-slot products of staged commits: LC_PRODUCTS_TENSOR (byte-limb GEMMs
+        on the tensor cores, the default) or LC_PRODUCTS_INT64."""
+        return self._dev.slot_products
+
+    @slot_products.setter
+    def slot_products(self, value: int):
+        self._dev.slot_products = value
+
     def entry(self, i: int, j: int):
         if i < self.params.k and j < self.params.m:
             return RingElement(self.params.ring, self._matrix[i * self.params.m + j].copy())

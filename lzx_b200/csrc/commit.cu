@@ -673,18 +673,14 @@ template <class E>
 static int commit_core(lc_ajtai_key* key, size_t batch, uint32_t b_pad, void* out, cudaStream_t st) {
   const uint32_t n = key->n, m = key->m, kappa = key->k;
   const uint32_t q = key->plan->q[0];
-  if constexpr (std::is_same<E, uint64_t>::value) {
-    // Goldilocks: the per-slot products as byte-limb GEMMs on the tensor cores
-    if (key->slot_products == LC_PRODUCTS_TENSOR) {
-      int rc = grow(&key->d_chat, &key->chat_bytes, (size_t)batch * kappa * n * sizeof(E));
-      if (rc) return rc;
-      uint64_t* chat = reinterpret_cast<uint64_t*>(key->d_chat);
-      rc = tc_slot_products(reinterpret_cast<const uint64_t*>(key->d_ahat_t), key->a_m,
-                            reinterpret_cast<const uint64_t*>(key->d_what_t), m, n, kappa, batch, b_pad,
-                            &key->d_partial, &key->partial_bytes, chat, key->d_err, st);
-      if (rc == LC_OK) return run_ntt(key->plan, chat, out, (size_t)batch * kappa, true, st);
-      if (rc != LC_ERR_UNSUPPORTED) return rc;
-    }
+  // the per-slot products as byte-limb GEMMs on the tensor cores
+  if (key->slot_products == LC_PRODUCTS_TENSOR) {
+    int rc = grow(&key->d_chat, &key->chat_bytes, (size_t)batch * kappa * n * sizeof(E));
+    if (rc) return rc;
+    rc = tc_slot_products(key->d_ahat_t, key->a_m, key->d_what_t, (uint32_t)sizeof(E), q, m, n, kappa, batch,
+                          b_pad, &key->d_partial, &key->partial_bytes, key->d_chat, key->d_err, st);
+    if (rc == LC_OK) return run_ntt(key->plan, key->d_chat, out, (size_t)batch * kappa, true, st);
+    if (rc != LC_ERR_UNSUPPORTED) return rc;
   }
   const bool tiled = b_pad % kBTile == 0;
   const bool quad = !tiled && b_pad % 4 == 0;

@@ -153,12 +153,13 @@ int tc_commit(lc_tc_tables* t, const void* w, bool s8, size_t batch, uint64_t* o
 int tc_ntt_prepare();
 int tc_witness_ntt(const void* w, bool s8, size_t batch, uint32_t m, uint32_t b_pad, uint64_t* what_t,
                    uint32_t* err, cudaStream_t st);
-// Goldilocks per-slot products Chat[b][i][t] = sum_j Ahat_T[t][j][i] What_T[t][j][b]
-// (mod p) as exact byte-limb GEMMs on the INT8 tensor cores (n slots, m ring
-// elements, a_m the key's row stride); scratch grown in *part.
-// LC_ERR_UNSUPPORTED for batch paddings it does not take (8, 16, 32 and
-// multiples of 64 are taken).
-int tc_slot_products(const uint64_t* ahat_t, uint32_t a_m, const uint64_t* what_t, uint32_t m, uint32_t n,
-                     uint32_t kappa, size_t batch, uint32_t b_pad, void** part, size_t* part_bytes,
-                     uint64_t* chat, uint32_t* err, cudaStream_t st);
+// Per-slot products Chat[b][i][t] = sum_j Ahat_T[t][j][i] What_T[t][j][b]
+// (mod q; Goldilocks for elem_bytes 8, the u32 modulus q for elem_bytes 4) as
+// exact byte-limb GEMMs on the INT8 tensor cores (n slots, m ring elements,
+// a_m the key's row stride); scratch grown in *part.  LC_ERR_UNSUPPORTED
+// unless a witness row of What_T (elem_bytes * b_pad bytes) is 32, 64, 128,
+// 256 or a multiple of 512 bytes.
+int tc_slot_products(const void* ahat_t, uint32_t a_m, const void* what_t, uint32_t elem_bytes, uint32_t q,
+                     uint32_t m, uint32_t n, uint32_t kappa, size_t batch, uint32_t b_pad, void** part,
+                     size_t* part_bytes, void* chat, uint32_t* err, cudaStream_t st);
 }  // namespace lc

@@ -845,42 +845,50 @@ namespace lc {
 // ------------------------------------------------------------------ slot products on the tensor cores
 //
 // The NTT engine's per-slot products C_t[i][b] = sum_j Ahat[i][j][t] What[b][j][t]
-// (mod p) as exact unsigned byte GEMMs.  With both residues split into byte
-// limbs, C_t = sum_{la,lw} 2^(8 (la + lw)) D_t[(i,la)][(b,lw)] and
+// (mod q) as exact unsigned byte GEMMs.  With both residues split into L byte
+// limbs (L = 8 for Goldilocks, 4 for u32 moduli),
+// C_t = sum_{la,lw} 2^(8 (la + lw)) D_t[(i,la)][(b,lw)] and
 //   D_t[(i,la)][(b,lw)] = sum_j Ahat_la[i][j][t] * What_lw[b][j][t]   (u8 x u8 -> s32),
 // exact for at most 32768 ring elements j per sum (32768 * 255^2 < 2^31).
-// The cached key Ahat_T[t][j][16] (u64) is, read as bytes, the A operand of
-// slot t in MN-major form: row j (the K index) holds the 128 bytes (i, la),
-// la fastest; What_T[t][j][b_pad] is the B operand the same way, 8 b_pad
-// bytes (b, lw) per row.  3-D TMA maps (x = bytes of a row, y = j < m, z =
-// slot) load 64-row stages with the 128-byte (64-byte for 8 witnesses)
-// swizzle, the MN-major canonical layout of the MMA descriptors (SBO = 8
-// rows, LBO = next 128-byte atom along N); rows past m read as zero.  CTA
-// (slot, N tile of up to 512 bytes, K split): one TMA thread, one MMA thread
-// (M = 128, N <= 256 per accumulator, K = 32), four epilogue warps writing
-// D transposed so that the lanes (rows (i, la)) store contiguously; a second
-// kernel sums the splits and limbs and reduces mod p into Chat[b][i][t].
+// The cached key Ahat_T[t][j][16] is, read as bytes, the A operand of slot t
+// in MN-major form: row j (the K index) holds the 16 L bytes (i, la), la
+// fastest; What_T[t][j][b_pad] is the B operand the same way, L b_pad bytes
+// (b, lw) per row.  3-D TMA maps (x = bytes of a row, y = j < m, z = slot)
+// load 64-row stages with the swizzle of the row width (128, 64 or 32 bytes),
+// the MN-major canonical layout of the MMA descriptors (SBO = 8 rows, LBO =
+// next atom along M/N); rows past m read as zero.  For u32 keys the 64-byte A
+// rows fill half of M = 128: the descriptor's second A atom is a zero tile.
+// CTA (slot, N tile of up to 512 bytes, K split): one TMA thread, one MMA
+// thread (M = 128, N <= 256 per accumulator, K = 32), four epilogue warps
+// writing D transposed so that the lanes (rows (i, la)) store contiguously;
+// a second kernel sums the splits and limbs and reduces into Chat[b][i][t].
 constexpr int kSpStages = 4;
 constexpr int kSpRows = 64;          // K rows (ring elements j) per stage
 constexpr uint32_t kSpKSplit = 32768;  // ring elements per exact int32 sum
 constexpr int kSpThreads = 192;      // warp 0 TMA, 1 MMA + TMEM, 2..5 epilogue
 
-template <int NCTA>
+template <int NCTA, int AW>
 struct SpCfg {
-  static constexpr int SW = NCTA >= 128 ? 128 : 64;  // B swizzle atom (bytes of a row)
+  static constexpr int SW = NCTA >= 128 ? 128 : NCTA;  // B swizzle atom (bytes of a row): 128, 64 or 32
   static constexpr int ATOMS = NCTA / SW;
   static constexpr int MMA_N = NCTA > 256 ? 256 : NCTA;
   static constexpr int ACCS = NCTA / MMA_N;
-  static constexpr int A_BYTES = kSpRows * 128;
+  static constexpr int A_LOAD = kSpRows * AW;    // bytes TMA writes per stage (AW = 128 or 64)
+  static constexpr int A_BYTES = kSpRows * 128;  // A region: for AW = 64 the zero atom follows
   static constexpr int B_ATOM = kSpRows * SW;
   static constexpr int STAGE = A_BYTES + ATOMS * B_ATOM;
   static constexpr size_t SMEM = 1024 + (size_t)kSpStages * STAGE + 128;
-  static_assert(STAGE % 1024 == 0 && B_ATOM % 512 == 0, "swizzle atoms stay aligned");
+  static constexpr uint32_t A_LAYOUT = AW == 128 ? 2u : 4u;
+  static constexpr uint32_t B_LAYOUT = SW == 128 ? 2u : SW == 64 ? 4u : 6u;
+  static_assert(AW == 128 || AW == 64, "row bytes of the key");
+  static_assert(SW == 128 || SW == 64 || SW == 32, "swizzle atom");
+  static_assert(STAGE % 1024 == 0 && B_ATOM % 256 == 0, "swizzle atoms stay aligned");
   static_assert(SMEM <= 227 * 1024, "shared memory");
 };
 
 // MN-major operand: LBO = bytes to the next atom along M/N, SBO = bytes to
-// the next 8-row group along K; layout 2 = 128-byte swizzle, 4 = 64-byte.
+// the next 8-row group along K; layout 2 = 128-byte swizzle, 4 = 64-byte,
+// 6 = 32-byte.
 LC_D uint64_t umma_desc_mn(uint32_t saddr, uint32_t lbo, uint32_t sbo, uint32_t layout) {
   uint64_t d = 0;
   d |= (uint64_t)((saddr >> 4) & 0x3FFF);
@@ -904,11 +912,11 @@ struct SpParams {
   uint32_t* err;
 };
 
-template <int NCTA>
+template <int NCTA, int AW>
 __global__ void __launch_bounds__(kSpThreads, 1)
     slot_products_kernel(const __grid_constant__ CUtensorMap amap, const __grid_constant__ CUtensorMap wmap,
                          const __grid_constant__ SpParams p) {
-  using C = SpCfg<NCTA>;
+  using C = SpCfg<NCTA, AW>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* base =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -933,9 +941,17 @@ __global__ void __launch_bounds__(kSpThreads, 1)
     *abort_flag = 0;
     fence_mbar_init();
   }
+  if constexpr (AW == 64) {
+    // the second A atom of every stage: rows (i, la) 64..127 are zero
+    for (int s = 0; s < kSpStages; ++s) {
+      uint4* z = reinterpret_cast<uint4*>(base + s * C::STAGE + C::A_LOAD);
+      for (int e = tid; e < (C::A_BYTES - C::A_LOAD) / 16; e += kSpThreads) z[e] = make_uint4(0, 0, 0, 0);
+    }
+    fence_proxy_async_smem();
+  }
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(NCTA));
+                 "r"(NCTA < 32 ? 32 : NCTA));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   tc_fence_before();
@@ -959,7 +975,7 @@ __global__ void __launch_bounds__(kSpThreads, 1)
         }
         unsigned char* st = stage(s);
         const int y = (int)(j0 + kSpRows * s);
-        mbar_arrive_expect_tx(&full[s % kSpStages], (uint32_t)C::STAGE);
+        mbar_arrive_expect_tx(&full[s % kSpStages], (uint32_t)(C::A_LOAD + C::ATOMS * C::B_ATOM));
         tma_load_3d(st, &amap, 0, y, (int)t, &full[s % kSpStages]);
 #pragma unroll
         for (int a = 0; a < C::ATOMS; ++a)
@@ -971,7 +987,6 @@ __global__ void __launch_bounds__(kSpThreads, 1)
   } else if (warp == 1) {
     // ---------------- MMA issuer
     if (lane == 0) {
-      constexpr uint32_t kBLayout = C::SW == 128 ? 2u : 4u;
       for (int s = 0; s < nst && !*abort_flag; ++s) {
         if (!mbar_wait(&full[s % kSpStages], (uint32_t)((s / kSpStages) & 1))) {
           fail();
@@ -983,9 +998,10 @@ __global__ void __launch_bounds__(kSpThreads, 1)
         for (int ks = 0; ks < kSpRows / 32; ++ks) {
 #pragma unroll
           for (int acc = 0; acc < C::ACCS; ++acc) {
-            const uint64_t ad = umma_desc_mn(sa + ks * 32 * 128, C::B_ATOM, 8 * 128, 2u);
+            // A: one 128-byte atom, or (AW = 64) the key's atom and the zero atom C::A_LOAD later
+            const uint64_t ad = umma_desc_mn(sa + ks * 32 * AW, C::A_LOAD, 8 * AW, C::A_LAYOUT);
             const uint64_t bd = umma_desc_mn(sb + acc * (C::MMA_N / C::SW) * C::B_ATOM + ks * 32 * C::SW,
-                                             C::B_ATOM, 8 * C::SW, kBLayout);
+                                             C::B_ATOM, 8 * C::SW, C::B_LAYOUT);
             mma_i8(tmem + acc * C::MMA_N, ad, bd, SpIdesc<C::MMA_N>::value, (s > 0 || ks > 0) ? 1u : 0u);
           }
         }
@@ -1024,71 +1040,102 @@ __global__ void __launch_bounds__(kSpThreads, 1)
   __syncthreads();
   if (warp == 1) {
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCTA));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCTA < 32 ? 32 : NCTA));
   }
 }
 
-// Chat[b][i][t] = sum_{la,lw} 2^(8 (la + lw)) sum_split D[split][t][nt][(bl, lw)][(i, la)]  mod p.
-// Pair sums over the splits fit 64 bits (< 2^31 * splits); the 15 sums of equal
-// la + lw = k (< 2^42) are folded with 2^(8k) mod p in 128 bits.
-__global__ void slot_products_reduce_kernel(const int32_t* __restrict__ part, uint64_t* __restrict__ chat,
-                                            uint32_t n, uint32_t kappa, uint32_t batch, uint32_t ncta,
-                                            uint32_t ntiles, uint32_t splits) {
+// Chat[b][i][t] = sum_{la,lw} 2^(8 (la + lw)) sum_split D[split][t][nt][(bl, lw)][(i, la)]  mod q.
+// Pair sums over the splits fit 64 bits (< 2^31 * splits); the 2L - 1 sums of
+// equal la + lw = k are folded with 2^(8k) mod q (128 bits for Goldilocks,
+// 64-bit remainders for u32 q).
+template <class E>
+__global__ void slot_products_reduce_kernel(const int32_t* __restrict__ part, E* __restrict__ chat, uint32_t n,
+                                            uint32_t kappa, uint32_t batch, uint32_t ncta, uint32_t ntiles,
+                                            uint32_t splits, uint32_t q) {
+  constexpr int L = sizeof(E);
   const size_t total = (size_t)n * batch * kappa;
-  const uint32_t wpt = ncta / 8;  // witnesses per N tile
+  const uint32_t wpt = ncta / L;  // witnesses per N tile
   for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
        idx += (size_t)gridDim.x * blockDim.x) {
     const uint32_t i = idx % kappa;
     const uint32_t b = (uint32_t)((idx / kappa) % batch);
     const uint32_t t = (uint32_t)(idx / ((size_t)kappa * batch));
     const uint32_t nt = b / wpt, bl = b % wpt;
-    uint64_t tk[15];
+    uint64_t tk[2 * L - 1];
 #pragma unroll
-    for (int k = 0; k < 15; ++k) tk[k] = 0;
+    for (int k = 0; k < 2 * L - 1; ++k) tk[k] = 0;
     for (uint32_t sp = 0; sp < splits; ++sp) {
       const int32_t* d = part + (((size_t)sp * n + t) * ntiles + nt) * (size_t)ncta * 128;
 #pragma unroll
-      for (int lw = 0; lw < 8; ++lw) {
-        const int32_t* col = d + (size_t)(bl * 8 + lw) * 128 + i * 8;
+      for (int lw = 0; lw < L; ++lw) {
+        const int32_t* col = d + (size_t)(bl * L + lw) * 128 + i * L;
 #pragma unroll
-        for (int la = 0; la < 8; ++la) tk[la + lw] += (uint64_t)(uint32_t)col[la];
+        for (int la = 0; la < L; ++la) tk[la + lw] += (uint64_t)(uint32_t)col[la];
       }
     }
-    unsigned __int128 v = 0;
-    uint64_t c = 1;  // 2^(8k) mod p
+    E res;
+    if constexpr (L == 8) {
+      unsigned __int128 v = 0;
+      uint64_t c = 1;  // 2^(8k) mod p
 #pragma unroll
-    for (int k = 0; k < 15; ++k) {
-      v += (unsigned __int128)tk[k] * c;
-      c = gl_mul(c, 256);
+      for (int k = 0; k < 2 * L - 1; ++k) {
+        v += (unsigned __int128)tk[k] * c;
+        c = gl_mul(c, 256);
+      }
+      res = gl_canon(gl_reduce128_lazy((uint64_t)(v >> 64), (uint64_t)v));
+    } else {
+      uint64_t v = 0, c = 1 % q;  // 2^(8k) mod q
+#pragma unroll
+      for (int k = 0; k < 2 * L - 1; ++k) {
+        v = (v + (tk[k] % q) * c % q) % q;  // each term < q < 2^32 before the sum
+        c = (c << 8) % q;
+      }
+      res = (E)v;
     }
-    chat[((size_t)b * kappa + i) * n + t] = gl_canon(gl_reduce128_lazy((uint64_t)(v >> 64), (uint64_t)v));
+    chat[((size_t)b * kappa + i) * n + t] = res;
   }
 }
 
-template <int NCTA>
+template <int NCTA, int AW>
 static int launch_slot_products(const CUtensorMap& amap, const CUtensorMap& wmap, const SpParams& prm,
                                 cudaStream_t st) {
-  auto kern = slot_products_kernel<NCTA>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SpCfg<NCTA>::SMEM);
+  auto kern = slot_products_kernel<NCTA, AW>;
+  using C = SpCfg<NCTA, AW>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
   if (e != cudaSuccess) return map_cuda(e);
-  kern<<<dim3(prm.nslots, prm.ntiles, prm.splits), kSpThreads, SpCfg<NCTA>::SMEM, st>>>(amap, wmap, prm);
+  kern<<<dim3(prm.nslots, prm.ntiles, prm.splits), kSpThreads, C::SMEM, st>>>(amap, wmap, prm);
   return map_cuda(cudaGetLastError());
 }
 
-int tc_slot_products(const uint64_t* ahat_t, uint32_t a_m, const uint64_t* what_t, uint32_t m, uint32_t n,
-                     uint32_t kappa, size_t batch, uint32_t b_pad, void** part, size_t* part_bytes,
-                     uint64_t* chat, uint32_t* err, cudaStream_t st) {
+template <int AW>
+static int launch_slot_products_n(uint32_t ncta, const CUtensorMap& amap, const CUtensorMap& wmap,
+                                  const SpParams& prm, cudaStream_t st) {
+  switch (ncta) {
+    case 512: return launch_slot_products<512, AW>(amap, wmap, prm, st);
+    case 256: return launch_slot_products<256, AW>(amap, wmap, prm, st);
+    case 128: return launch_slot_products<128, AW>(amap, wmap, prm, st);
+    case 64: return launch_slot_products<64, AW>(amap, wmap, prm, st);
+    case 32: return launch_slot_products<32, AW>(amap, wmap, prm, st);
+    default: return LC_ERR_UNSUPPORTED;
+  }
+}
+
+int tc_slot_products(const void* ahat_t, uint32_t a_m, const void* what_t, uint32_t elem_bytes, uint32_t q,
+                     uint32_t m, uint32_t n, uint32_t kappa, size_t batch, uint32_t b_pad, void** part,
+                     size_t* part_bytes, void* chat, uint32_t* err, cudaStream_t st) {
   if (batch == 0) return LC_OK;
   EncodeTiledFn enc = encode_fn();
-  if (!enc || kappa > 16 || m == 0) return LC_ERR_UNSUPPORTED;
+  if (!enc || kappa > 16 || m == 0 || (elem_bytes != 8 && elem_bytes != 4)) return LC_ERR_UNSUPPORTED;
+  // N tile: 512 bytes, or the whole row when it is 32, 64, 128 or 256 bytes
+  const uint64_t row = (uint64_t)elem_bytes * b_pad;
   uint32_t ncta;
-  if (b_pad % 64 == 0)
+  if (row % 512 == 0)
     ncta = 512;
-  else if (b_pad == 32 || b_pad == 16 || b_pad == 8)
-    ncta = 8 * b_pad;
+  else if (row == 256 || row == 128 || row == 64 || row == 32)
+    ncta = (uint32_t)row;
   else
     return LC_ERR_UNSUPPORTED;
-  const uint32_t ntiles = 8 * b_pad / ncta;
+  const uint64_t ntiles = row / ncta;
   const uint32_t splits = (m + kSpKSplit - 1) / kSpKSplit;
   if (ntiles > 65535 || splits > 65535) return LC_ERR_UNSUPPORTED;  // grid y, z
   const size_t need = (size_t)splits * n * ntiles * ncta * 128 * sizeof(int32_t);
@@ -1103,41 +1150,45 @@ int tc_slot_products(const uint64_t* ahat_t, uint32_t a_m, const uint64_t* what_
     *part_bytes = need;
   }
   // A: bytes (i, la) of Ahat_T[t][j][16]; B: bytes (b, lw) of What_T[t][j][b_pad]
+  const uint32_t aw = 16 * elem_bytes;
   CUtensorMap amap, wmap;
   const cuuint32_t estr[3] = {1, 1, 1};
   {
-    const cuuint64_t dims[3] = {128, (cuuint64_t)m, (cuuint64_t)n};
-    const cuuint64_t strides[2] = {128, (cuuint64_t)a_m * 128};
-    const cuuint32_t box[3] = {128, (cuuint32_t)kSpRows, 1};
-    if (enc(&amap, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<uint64_t*>(ahat_t), dims, strides, box, estr,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-      return LC_ERR_UNSUPPORTED;
-  }
-  {
-    const cuuint64_t row = (cuuint64_t)b_pad * 8;
-    const cuuint64_t dims[3] = {row, (cuuint64_t)m, (cuuint64_t)n};
-    const cuuint64_t strides[2] = {row, (cuuint64_t)m * row};
-    const cuuint32_t sw = ncta >= 128 ? 128 : 64;
-    const cuuint32_t box[3] = {sw, (cuuint32_t)kSpRows, 1};
-    if (enc(&wmap, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<uint64_t*>(what_t), dims, strides, box, estr,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, sw == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+    const cuuint64_t dims[3] = {aw, (cuuint64_t)m, (cuuint64_t)n};
+    const cuuint64_t strides[2] = {aw, (cuuint64_t)a_m * aw};
+    const cuuint32_t box[3] = {aw, (cuuint32_t)kSpRows, 1};
+    if (enc(&amap, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(ahat_t), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, aw == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
       return LC_ERR_UNSUPPORTED;
   }
-  const SpParams prm{static_cast<int32_t*>(*part), m, n, ntiles, splits, err};
-  int rc;
-  switch (ncta) {
-    case 512: rc = launch_slot_products<512>(amap, wmap, prm, st); break;
-    case 256: rc = launch_slot_products<256>(amap, wmap, prm, st); break;
-    case 128: rc = launch_slot_products<128>(amap, wmap, prm, st); break;
-    default: rc = launch_slot_products<64>(amap, wmap, prm, st); break;
+  {
+    const cuuint64_t dims[3] = {row, (cuuint64_t)m, (cuuint64_t)n};
+    const cuuint64_t strides[2] = {row, (cuuint64_t)m * row};
+    const cuuint32_t sw = ncta >= 128 ? 128 : ncta;
+    const cuuint32_t box[3] = {sw, (cuuint32_t)kSpRows, 1};
+    const CUtensorMapSwizzle swz = sw == 128 ? CU_TENSOR_MAP_SWIZZLE_128B
+                                   : sw == 64 ? CU_TENSOR_MAP_SWIZZLE_64B
+                                              : CU_TENSOR_MAP_SWIZZLE_32B;
+    if (enc(&wmap, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(what_t), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return LC_ERR_UNSUPPORTED;
   }
+  const SpParams prm{static_cast<int32_t*>(*part), m, n, (uint32_t)ntiles, splits, err};
+  int rc = aw == 128 ? launch_slot_products_n<128>(ncta, amap, wmap, prm, st)
+                     : launch_slot_products_n<64>(ncta, amap, wmap, prm, st);
   if (rc) return rc;
   const size_t total = (size_t)n * batch * kappa;
   const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, (size_t)device_sm_count() * 16);
-  slot_products_reduce_kernel<<<blocks, 256, 0, st>>>(static_cast<const int32_t*>(*part), chat, n, kappa,
-                                                      (uint32_t)batch, ncta, ntiles, splits);
+  if (elem_bytes == 8)
+    slot_products_reduce_kernel<uint64_t><<<blocks, 256, 0, st>>>(
+        static_cast<const int32_t*>(*part), static_cast<uint64_t*>(chat), n, kappa, (uint32_t)batch, ncta,
+        (uint32_t)ntiles, splits, q);
+  else
+    slot_products_reduce_kernel<uint32_t><<<blocks, 256, 0, st>>>(
+        static_cast<const int32_t*>(*part), static_cast<uint32_t*>(chat), n, kappa, (uint32_t)batch, ncta,
+        (uint32_t)ntiles, splits, q);
   return map_cuda(cudaGetLastError());
 }
 

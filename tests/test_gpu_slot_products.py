@@ -5,10 +5,11 @@ GEMMs on the INT8 tensor cores (lc_ajtai_key_set_slot_products(...,
 LC_PRODUCTS_TENSOR), the default) or with 160-bit integer multiply-adds on the
 CUDA cores (LC_PRODUCTS_INT64).  Both must give the oracle's commitment
 (AjtaiPublicKey::commit, lattice-commitment/src/ajtai.rs:118-153, over
-lattice-core/src/field.rs) bit for bit: every N-tile width (batch paddings 8,
-16, 32, 64 and several tiles of 512 bytes), several K-splits of 32768 ring
-elements, odd ring-element counts, d = 64/128/256, int8, uint8 and residue
-witnesses, and a key view whose row stride differs from its width.
+lattice-core/src/field.rs, and over Modulus32::Q_32 and a 30-bit CRT prime)
+bit for bit: every N-tile width (witness rows of 32, 64, 128, 256 bytes and
+several tiles of 512), several K-splits of 32768 ring elements, odd
+ring-element counts, d = 64/128/256, int8, uint8 and residue witnesses, and a
+key view whose row stride differs from its width.
 """
 import ctypes as C
 
@@ -16,7 +17,8 @@ import numpy as np
 import pytest
 
 import oracle
-from lzx_b200 import GoldilocksAjtaiKey, _lib, synth
+from lzx_b200 import (CRT_SET_30BIT, AjtaiParams, AjtaiPublicKey, GoldilocksAjtaiKey, Modulus32, RingConfig,
+                      _lib, synth)
 from lzx_b200.batch import key_view
 
 pytestmark = pytest.mark.gpu
@@ -59,6 +61,7 @@ def both_products(key, W):
     (6, 2, 1, 64),          # a single ring element
     (7, 8, 300, 16),
     (8, 2, 129, 64),
+    (6, 4, 3000, 4),        # N tile 32 bytes: too long for the single launch
 ])
 @pytest.mark.parametrize("digits", ["i8", "u8", "residue"])
 def test_tensor_products_match_integer_and_oracle(log_d, kappa, m, batch, digits):
@@ -113,6 +116,31 @@ def test_key_view_row_stride():
     torch.cuda.synchronize()
     Av = A.reshape(kappa, m, 64)[:kv, :nv].reshape(-1)
     assert np.array_equal(out.cpu().numpy().view(np.uint64), oracle_commit(Av, log_d, kv, nv, W))
+
+
+@pytest.mark.parametrize("modulus", [Modulus32.Q_32, CRT_SET_30BIT[1]], ids=["q32", "crt30"])
+@pytest.mark.parametrize("log_n,k,m,batch", [
+    (6, 2, 300, 8),      # u32 rows: 32-byte N tile
+    (6, 5, 700, 16),     # 64
+    (7, 16, 129, 32),    # 128
+    (6, 3, 1000, 64),    # 256
+    (8, 2, 257, 128),    # 512
+    (6, 7, 300, 200),    # padded to 256: two tiles of 512
+])
+def test_u32_tensor_products_match_integer_and_oracle(modulus, log_n, k, m, batch):
+    """u32 keys: 4 byte limbs, the key's 64-byte rows fill half of M = 128."""
+    pk = AjtaiPublicKey.from_seed(AjtaiParams(RingConfig(modulus, log_n), k, m, 1 << 20), bytes([log_n + k]) * 32)
+    n, q = 1 << log_n, modulus.q
+    W = synth.synth_mod32(7, m + batch, q, batch * m * n).reshape(batch, m, n)
+    assert pk.slot_products == GoldilocksAjtaiKey.PRODUCTS_TENSOR
+    tensor = pk.commit_batch(W)
+    pk.slot_products = GoldilocksAjtaiKey.PRODUCTS_INT64
+    integer = pk.commit_batch(W)
+    pk.slot_products = GoldilocksAjtaiKey.PRODUCTS_TENSOR
+    assert np.array_equal(tensor, integer)
+    t = oracle.NttTables32(oracle.Modulus32(modulus.q, modulus.two_adicity, modulus.generator), log_n)
+    for b in sorted({0, batch - 1}):
+        assert np.array_equal(tensor[b], oracle.ajtai32_commit_naive(t, pk._matrix, k, m, W[b]))
 
 
 def test_switch_arguments():
