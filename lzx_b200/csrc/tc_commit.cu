@@ -454,10 +454,14 @@ LC_D void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, ui
 // A + hi(B) (2^32 - 1) positive and below 2^49; adding lo(B) 2^32 wraps 2^64
 // at most once, folded as 2^32 - 1; the offset comes off mod p at the end.
 LC_D uint64_t tn_fold(const uint32_t (&d)[8][8], int u) {
-  const int64_t A = (int64_t)(int32_t)d[0][u] + (int64_t)(int32_t)d[1][u] * 256 +
-                    (int64_t)(int32_t)d[2][u] * 65536 + (int64_t)(int32_t)d[3][u] * 16777216;
-  const int64_t B = (int64_t)(int32_t)d[4][u] + (int64_t)(int32_t)d[5][u] * 256 +
-                    (int64_t)(int32_t)d[6][u] * 65536 + (int64_t)(int32_t)d[7][u] * 16777216;
+  // limb pairs in 32 bits: |D| < 2^21 (s8 digits) or 0 <= D < 2^22 (u8), so
+  // D_l + 2^8 D_(l+1) stays inside int32
+  const int32_t p01 = (int32_t)d[0][u] + (int32_t)d[1][u] * 256;
+  const int32_t p23 = (int32_t)d[2][u] + (int32_t)d[3][u] * 256;
+  const int32_t p45 = (int32_t)d[4][u] + (int32_t)d[5][u] * 256;
+  const int32_t p67 = (int32_t)d[6][u] + (int32_t)d[7][u] * 256;
+  const int64_t A = (int64_t)p01 + (int64_t)p23 * 65536;
+  const int64_t B = (int64_t)p45 + (int64_t)p67 * 65536;
   const uint64_t t = (uint64_t)(A + (B >> 32) * (int64_t)kGlEps + ((int64_t)1 << 48));  // in (0, 2^49)
   uint64_t r = t + ((uint64_t)(uint32_t)B << 32);
   if (r < t) r += kGlEps;  // no second wrap: r < 2^49 after the first
