@@ -465,7 +465,10 @@ LC_D uint64_t tn_fold(const uint32_t (&d)[8][8], int u) {
   const uint64_t t = (uint64_t)(A + (B >> 32) * (int64_t)kGlEps + ((int64_t)1 << 48));  // in (0, 2^49)
   uint64_t r = t + ((uint64_t)(uint32_t)B << 32);
   if (r < t) r += kGlEps;  // no second wrap: r < 2^49 after the first
-  return gl_sub(gl_canon(r), (uint64_t)1 << 48);
+  // r - 2^48 is canonical for r >= 2^48 (r - 2^48 < 2^64 - 2^48 < p);
+  // below, adding p once brings it into [0, p)
+  constexpr uint64_t kOff = (uint64_t)1 << 48;
+  return r - kOff + (r < kOff ? kGlP : 0);
 }
 
 template <bool S8>
