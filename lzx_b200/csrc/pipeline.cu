@@ -7,10 +7,12 @@
 // key (AjtaiPublicKey::commit, lattice-commitment/src/ajtai.rs:118-153, batch
 // of 8 witnesses), and z itself is mapped to a CRT set of 30-bit primes
 // (Modulus32::reduce_u64, lattice-ring/src/modulus.rs:65 per prime) and
-// transformed there (NttTables::forward_fast, ntt.rs:118-146).  The object
-// owns fixed device buffers, so after one eager warm-up run (which sizes the
-// key's scratch) the four stages are captured once into a CUDA graph and
-// every later run is one cudaGraphLaunch.
+// transformed there (NttTables::forward_fast, ntt.rs:118-146).  The CRT
+// branch depends only on z, so it runs on a second stream beside the
+// decomposition and the commitments (forked and joined with events; in the
+// graph, two parallel branches).  The object owns fixed device buffers, so
+// after one eager warm-up run (which sizes the key's scratch) the stages are
+// captured once into a CUDA graph and every later run is one cudaGraphLaunch.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -86,6 +88,8 @@ struct lc_fold_pipeline {
   int use_graph = 0;
   bool warmed = false;
   cudaStream_t cap = nullptr;
+  cudaStream_t side = nullptr;    // the CRT branch
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   uint64_t scratch_sig = 0;  // key scratch the graph was captured with
@@ -95,11 +99,20 @@ namespace lc {
 
 static int fold_stages(lc_fold_pipeline* f, cudaStream_t st) {
   const size_t coeffs = (size_t)f->m * 64;
+  // fork: the CRT branch starts after the caller's earlier work on st
+  cudaError_t e = cudaEventRecord(f->ev_fork, st);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(f->side, f->ev_fork, 0);
+  if (e != cudaSuccess) return map_cuda(e);
+  int rc_crt = crt_residues(f->crt, f->z, coeffs, f->crt_out, f->side);
+  if (!rc_crt) rc_crt = lc_ntt_forward(f->crt, f->crt_out, f->crt_out, f->m, f->side);
   int rc = lc_decomp_b(f->z, coeffs, 8, f->digits, st);
   if (!rc) rc = lc_ajtai_commit_u8(f->key, f->digits, 8, f->commits, st);
-  if (!rc) rc = crt_residues(f->crt, f->z, coeffs, f->crt_out, st);
-  if (!rc) rc = lc_ntt_forward(f->crt, f->crt_out, f->crt_out, f->m, st);
-  return rc;
+  // join: st continues after both branches (also closes the side stream's
+  // part of a capture)
+  e = cudaEventRecord(f->ev_join, f->side);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(st, f->ev_join, 0);
+  if (e != cudaSuccess) return map_cuda(e);
+  return rc ? rc : rc_crt;
 }
 
 }  // namespace lc
@@ -126,7 +139,10 @@ LC_API int lc_fold_pipeline_create(lc_ajtai_key* key, const lc_ntt_plan* crt_pla
   const size_t coeffs = (size_t)m * 64;
   if (cudaMalloc(&f->z, coeffs * 8) != cudaSuccess || cudaMalloc(&f->digits, coeffs * 8) != cudaSuccess ||
       cudaMalloc(&f->commits, (size_t)8 * k * 64 * 8) != cudaSuccess ||
-      cudaMalloc(&f->crt_out, coeffs * nm * 4) != cudaSuccess) {
+      cudaMalloc(&f->crt_out, coeffs * nm * 4) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&f->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&f->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&f->ev_join, cudaEventDisableTiming) != cudaSuccess) {
     cudaGetLastError();
     lc_fold_pipeline_destroy(f);
     return LC_ERR_OUT_OF_MEMORY;
@@ -208,6 +224,9 @@ LC_API void lc_fold_pipeline_destroy(lc_fold_pipeline* f) {
   if (f->exec) cudaGraphExecDestroy(f->exec);
   if (f->graph) cudaGraphDestroy(f->graph);
   if (f->cap) cudaStreamDestroy(f->cap);
+  if (f->side) cudaStreamDestroy(f->side);
+  if (f->ev_fork) cudaEventDestroy(f->ev_fork);
+  if (f->ev_join) cudaEventDestroy(f->ev_join);
   for (void* p : {(void*)f->z, (void*)f->digits, (void*)f->commits, (void*)f->crt_out})
     if (p) cudaFree(p);
   delete f;
