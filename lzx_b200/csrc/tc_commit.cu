@@ -408,15 +408,16 @@ __global__ void tc_reduce_kernel(const int64_t* __restrict__ partial, uint64_t* 
 // (the natural-order negacyclic NTT, out[t] = w(psi^(2t+1))).  With the
 // residues V split into 8 byte limbs, D_l[r][t] = sum_c W[r][c] V_l[t][c] is
 // exact in int32 (64 * 128 * 255 < 2^21, u8 digits 64 * 255 * 255 < 2^22) and
-// What = sum_l 2^(8l) D_l (mod p).  An M = 128 tile holds BB witnesses x HB
-// segments of their ring elements (BB * HB = 128, read by a 3-D TMA view of
-// w[b][j][64] with the 128-byte swizzle, two ring elements per 128-byte row);
-// each ring element is four MMAs (two limb groups N = 256, K = 64 as two
-// K-steps) into all 512 TMEM columns.  Sixteen epilogue warps read the limbs
-// back, fold them (int64, then 128-bit plus p*2^16 to make it positive) and
-// reduce mod p, writing What_T[t][j][b] coalesced along b.
+// What = sum_l 2^(8l) D_l (mod p).  An M = 128 tile holds R consecutive ring
+// elements x BB witnesses (R * BB = 128; rows ordered witness fastest, one
+// 64-byte ring element each, read by a 3-D TMA view of w[b][j][64] -- x the
+// digit, y the witness, z the ring element -- with the 64-byte swizzle); a
+// tile is four MMAs (two limb groups N = 256, K = 64 as two K-steps) into all
+// 512 TMEM columns.  Sixteen epilogue warps read the limbs back, fold them
+// mod p and write What_T[t][j][b]: a warp's 32 rows are 32 consecutive
+// entries of one slot.
 constexpr int kTnSlots = 4;
-constexpr int kTnATile = 128 * 128;
+constexpr int kTnATile = 128 * 64;  // 128 rows (ring element, witness) x 64 digit bytes
 constexpr int kTnVTile = 256 * 128;
 constexpr int kTnOffV = kTnSlots * kTnATile;
 constexpr int kTnOffBar = kTnOffV + 2 * kTnVTile;
@@ -428,10 +429,22 @@ static_assert(kTnSmem <= 227 * 1024, "shared memory");
 struct TnParams {
   const uint4* vimg;  // [2][256][128] bytes: the limb tiles in their swizzled shared-memory image
   uint64_t* what_t;   // [64][m][b_pad]
-  uint32_t m, b_pad, batch, L, BB, HB, npairs;
+  uint32_t m, b_pad, batch, BB, R, nblk;  // tile: R ring elements x BB witnesses; nblk ring-element blocks
   uint64_t items;
   uint32_t* err;
 };
+
+// K-major operand, 64-byte swizzle: 64-byte rows, 8-row groups of 512 bytes
+// (SBO), start address advanced by 32 bytes per K step inside the atom.
+LC_D uint64_t umma_desc_sw64(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);  // start address
+  d |= (uint64_t)1 << 16;                   // leading byte offset (unused here)
+  d |= (uint64_t)(512 >> 4) << 32;          // stride byte offset
+  d |= (uint64_t)1 << 46;                   // descriptor version
+  d |= (uint64_t)4 << 61;                   // layout: 64-byte swizzle
+  return d;
+}
 
 LC_D void tmem_ld8(uint32_t addr, uint32_t (&v)[8]) {
   asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
@@ -530,41 +543,35 @@ __global__ void __launch_bounds__(kTnThreads, 1)
           break;
         }
         const uint64_t item = blockIdx.x + i * gridDim.x;
-        const uint32_t jp = (uint32_t)(item % p.npairs), bt = (uint32_t)(item / p.npairs);
+        const uint32_t jb = (uint32_t)(item % p.nblk), bt = (uint32_t)(item / p.nblk);
         mbar_arrive_expect_tx(&loaded[i % kTnSlots], kTnATile);
-        tma_load_3d(a_slot(i), &wmap, (int)(jp * 128), (int)(bt * p.BB), 0, &loaded[i % kTnSlots]);
+        tma_load_3d(a_slot(i), &wmap, 0, (int)(bt * p.BB), (int)(jb * p.R), &loaded[i % kTnSlots]);
         last_loaded = (int64_t)i;
       }
     }
   } else if (warp == kMmaWarp) {
     // ---------------- MMA issuer
     if (lane == 0) {
-      uint64_t e = 0;  // ring elements issued
       for (uint64_t i = 0; i < n_my && !*abort_flag; ++i) {
         if (!mbar_wait(&loaded[i % kTnSlots], (uint32_t)((i / kTnSlots) & 1))) {
           fail();
           break;
         }
-        bool ok = true;
-        for (int jj = 0; jj < 2 && ok; ++jj, ++e) {
-          if (e >= 1 && !mbar_wait(acc_empty, (uint32_t)((e - 1) & 1))) {
-            fail();
-            ok = false;
-            break;
-          }
-          tc_fence_after();
-          const uint32_t aa = smem_u32(a_slot(i)) + 64 * jj;
-#pragma unroll
-          for (int g = 0; g < 2; ++g) {
-            const uint32_t va = smem_u32(base + kTnOffV + g * kTnVTile);
-#pragma unroll
-            for (int ks = 0; ks < 2; ++ks)
-              mma_i8(tmem + g * 256, umma_desc_sw128(aa + 32 * ks), umma_desc_sw128(va + 32 * ks),
-                     TcIdesc<S8>::value, ks > 0 ? 1u : 0u);
-          }
-          mma_commit(acc_full);
+        if (i >= 1 && !mbar_wait(acc_empty, (uint32_t)((i - 1) & 1))) {  // the epilogue read the last item
+          fail();
+          break;
         }
-        if (!ok) break;
+        tc_fence_after();
+        const uint32_t aa = smem_u32(a_slot(i));
+#pragma unroll
+        for (int g = 0; g < 2; ++g) {
+          const uint32_t va = smem_u32(base + kTnOffV + g * kTnVTile);
+#pragma unroll
+          for (int ks = 0; ks < 2; ++ks)
+            mma_i8(tmem + g * 256, umma_desc_sw64(aa + 32 * ks), umma_desc_sw128(va + 32 * ks),
+                   TcIdesc<S8>::value, ks > 0 ? 1u : 0u);
+        }
+        mma_commit(acc_full);
         mma_commit(&freed[i % kTnSlots]);
       }
       mma_commit(all_done);
@@ -572,27 +579,25 @@ __global__ void __launch_bounds__(kTnThreads, 1)
     }
   } else {
     // ---------------- epilogue: warp w reads TMEM lanes 32 (w % 4).., slots 16 (w / 4)..
+    // row = (ring element jl, witness bb), witness fastest: a warp's 32 rows
+    // are 32 consecutive What_T entries of one slot
     const uint32_t q = warp & 3, part = warp >> 2;
     const uint32_t row = 32 * q + lane;
-    const uint32_t hh = row / p.BB, bb = row % p.BB;
-    uint64_t e = 0;
+    const uint32_t jl = row / p.BB, bb = row % p.BB;
     for (uint64_t i = 0; i < n_my; ++i) {
       const uint64_t item = blockIdx.x + i * gridDim.x;
-      const uint32_t jp = (uint32_t)(item % p.npairs), bt = (uint32_t)(item / p.npairs);
+      const uint32_t jb = (uint32_t)(item % p.nblk), bt = (uint32_t)(item / p.nblk);
       const uint32_t b = bt * p.BB + bb;
-      bool stop = false;
-      for (int jj = 0; jj < 2; ++jj, ++e) {
+      {
         // warp-uniform decision: the TMEM loads below are .sync.aligned
-        const bool ok = !*abort_flag && mbar_wait(acc_full, (uint32_t)(e & 1));
+        const bool ok = !*abort_flag && mbar_wait(acc_full, (uint32_t)(i & 1));
         if (!__all_sync(0xffffffffu, ok)) {
           fail();
-          stop = true;
           break;
         }
         tc_fence_after();
-        const uint32_t jl = 2 * jp + jj;
-        const bool valid = b < p.b_pad && jl < p.L;
-        const uint32_t j = hh * p.L + jl;
+        const uint32_t j = jb * p.R + jl;
+        const bool valid = b < p.b_pad && j < p.m;
         const size_t stride = (size_t)p.m * p.b_pad;  // one slot t
         uint64_t* dst = p.what_t + (size_t)(16 * part) * stride + (size_t)j * p.b_pad + b;
 #pragma unroll 1
@@ -604,7 +609,7 @@ __global__ void __launch_bounds__(kTnThreads, 1)
           asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
           if (tb == 1) {
             // this warp's accumulator columns are all in registers: the next
-            // ring element's MMAs may overwrite them while the fold runs
+            // item's MMAs may overwrite them while the fold runs
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(acc_empty);
@@ -616,7 +621,6 @@ __global__ void __launch_bounds__(kTnThreads, 1)
           }
         }
       }
-      if (stop) break;
     }
   }
   // ---------------- nothing in flight when TMEM and shared memory go
@@ -813,7 +817,7 @@ int tc_witness_ntt(const void* w, bool s8, size_t batch, uint32_t m, uint32_t b_
   EncodeTiledFn enc = encode_fn();
   if (!img || !enc || (reinterpret_cast<uintptr_t>(w) & 15)) return LC_ERR_UNSUPPORTED;
   if ((size_t)m * b_pad < ((size_t)1 << 16) || (size_t)m * 64 > 0x7FFFFFFF) return LC_ERR_UNSUPPORTED;
-  // M tile: BB witnesses x HB segments of m / HB ring elements
+  // M tile: R consecutive ring elements x BB witnesses, witness fastest
   uint32_t BB;
   if (b_pad % 128 == 0)
     BB = 128;
@@ -821,25 +825,24 @@ int tc_witness_ntt(const void* w, bool s8, size_t batch, uint32_t m, uint32_t b_
     BB = b_pad;
   else
     return LC_ERR_UNSUPPORTED;
-  const uint32_t HB = 128 / BB;
-  if (m % HB) return LC_ERR_UNSUPPORTED;
-  const uint32_t L = m / HB, npairs = (L + 1) / 2;
-  const uint64_t items = (uint64_t)((b_pad + BB - 1) / BB) * npairs;
-  // w[b][j][64] as a 3-D byte array: x = 64 j_lo + c, y = b, z = segment; the
-  // rows past batch and the bytes past L*64 (odd L) read as zero
+  const uint32_t R = 128 / BB;
+  const uint32_t nblk = (m + R - 1) / R;
+  const uint64_t items = (uint64_t)(b_pad / BB) * nblk;
+  // w[b][j][64] as a 3-D byte array: x = digit c, y = witness b, z = ring
+  // element j; rows past batch or past m read as zero
   CUtensorMap map;
-  const cuuint64_t dims[3] = {(cuuint64_t)L * 64, (cuuint64_t)batch, (cuuint64_t)HB};
-  const cuuint64_t strides[2] = {(cuuint64_t)m * 64, (cuuint64_t)L * 64};
-  const cuuint32_t box[3] = {128, BB, HB};
+  const cuuint64_t dims[3] = {64, (cuuint64_t)batch, (cuuint64_t)m};
+  const cuuint64_t strides[2] = {(cuuint64_t)m * 64, 64};
+  const cuuint32_t box[3] = {64, BB, R};
   const cuuint32_t estr[3] = {1, 1, 1};
   const CUresult cr = enc(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(w), dims, strides, box, estr,
-                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (cr != CUDA_SUCCESS) return LC_ERR_UNSUPPORTED;
   auto kern = s8 ? tc_ntt_kernel<true> : tc_ntt_kernel<false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTnSmem);
   if (e != cudaSuccess) return map_cuda(e);
-  const TnParams prm{img, what_t, m, b_pad, (uint32_t)batch, L, BB, HB, npairs, items, err};
+  const TnParams prm{img, what_t, m, b_pad, (uint32_t)batch, BB, R, nblk, items, err};
   const unsigned grid = (unsigned)std::min<uint64_t>(items, (uint64_t)std::max(1, device_sm_count()));
   kern<<<grid, kTnThreads, kTnSmem, st>>>(map, prm);
   return map_cuda(cudaGetLastError());
