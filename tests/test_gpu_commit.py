@@ -166,8 +166,8 @@ def test_goldilocks_batches_small_and_tiled(batch):
 @pytest.mark.parametrize("digits", ["i8", "u8"])
 def test_goldilocks_byte_digit_transform_shapes(batch, m, digits):
     """Shapes whose d = 64 witness transform runs as INT8 tensor-core products:
-    tiles of BB witnesses x 128/BB segments of their ring elements (BB = 128,
-    32, 16, 8, 4, 1), padded batches, an odd ring-element count per row."""
+    tiles of 128/BB consecutive ring elements x BB witnesses (BB = 128, 32, 16,
+    8, 4, 1), padded batches, an odd ring-element count."""
     kappa = 2
     A, key = gl_key(kappa, m, seed=batch + m)
     if digits == "i8":
