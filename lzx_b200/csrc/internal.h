@@ -16,25 +16,29 @@ enum class PlanKind : int { U32Lazy = 0, U32Mont = 1, Goldilocks = 2 };
 // points; chunk k uses buffer/stream k&1 so copies of one chunk overlap the
 // transform of the other.
 struct HostPipeline {
-  void* buf[2] = {nullptr, nullptr};
+  // kSlots chunks in flight: while one slot's results go back over the link,
+  // the next slots' inputs come in
+  static constexpr int kSlots = 3;
+  void* buf[kSlots] = {};
   size_t bytes = 0;
-  cudaStream_t stream[2] = {nullptr, nullptr};
+  cudaStream_t stream[kSlots] = {};
 
   int ensure(size_t need) {
     if (!stream[0]) {
-      if (cudaStreamCreateWithFlags(&stream[0], cudaStreamNonBlocking) != cudaSuccess ||
-          cudaStreamCreateWithFlags(&stream[1], cudaStreamNonBlocking) != cudaSuccess) {
-        cudaGetLastError();
-        return LC_ERR_CUDA;
+      for (int i = 0; i < kSlots; ++i) {
+        if (cudaStreamCreateWithFlags(&stream[i], cudaStreamNonBlocking) != cudaSuccess) {
+          cudaGetLastError();
+          return LC_ERR_CUDA;
+        }
       }
     }
     if (need <= bytes) return LC_OK;
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < kSlots; ++i) {
       if (buf[i]) cudaFree(buf[i]);
       buf[i] = nullptr;
     }
     bytes = 0;
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < kSlots; ++i) {
       if (cudaMalloc(&buf[i], need) != cudaSuccess) {
         cudaGetLastError();
         return LC_ERR_OUT_OF_MEMORY;
@@ -43,8 +47,18 @@ struct HostPipeline {
     bytes = need;
     return LC_OK;
   }
+  // first error of the slots' streams (all of them are waited for)
+  cudaError_t sync() {
+    cudaError_t first = cudaSuccess;
+    for (int i = 0; i < kSlots; ++i) {
+      if (!stream[i]) continue;
+      const cudaError_t e = cudaStreamSynchronize(stream[i]);
+      if (first == cudaSuccess) first = e;
+    }
+    return first;
+  }
   void release() {
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < kSlots; ++i) {
       if (buf[i]) cudaFree(buf[i]);
       if (stream[i]) cudaStreamDestroy(stream[i]);
       buf[i] = nullptr;

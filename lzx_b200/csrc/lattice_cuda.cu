@@ -491,8 +491,8 @@ static int ntt_host(lc_ntt_plan* plan, const void* in, void* out, size_t count, 
   if (count == 0) return LC_OK;
   const size_t eb = plan->kind == PlanKind::Goldilocks ? 8 : 4;
   const size_t poly_bytes = ((size_t)1 << plan->log_n) * eb;
-  // chunk so that one chunk (all moduli) is about 32 MiB
-  size_t chunk = std::max<size_t>(1, ((size_t)32 << 20) / (poly_bytes * plan->num_moduli));
+  // chunk so that one chunk (all moduli) is about 16 MiB
+  size_t chunk = std::max<size_t>(1, ((size_t)16 << 20) / (poly_bytes * plan->num_moduli));
   chunk = std::min(chunk, count);
   HostPipeline& hp = plan->staging;
   int rc = hp.ensure(chunk * poly_bytes * plan->num_moduli);
@@ -503,8 +503,8 @@ static int ntt_host(lc_ntt_plan* plan, const void* in, void* out, size_t count, 
   int k = 0;
   while (done < count) {
     const size_t c = std::min(chunk, count - done);
-    cudaStream_t s = hp.stream[k & 1];
-    char* dbuf = static_cast<char*>(hp.buf[k & 1]);
+    cudaStream_t s = hp.stream[k % HostPipeline::kSlots];
+    char* dbuf = static_cast<char*>(hp.buf[k % HostPipeline::kSlots]);
     // the buffer of this stream is free once its previous D2H has finished (stream order)
     for (uint32_t m = 0; m < plan->num_moduli; ++m) {
       cudaMemcpyAsync(dbuf + m * c * poly_bytes, src + (m * count + done) * poly_bytes,
@@ -520,11 +520,9 @@ static int ntt_host(lc_ntt_plan* plan, const void* in, void* out, size_t count, 
     done += c;
     ++k;
   }
-  cudaError_t e1 = cudaStreamSynchronize(hp.stream[0]);
-  cudaError_t e2 = cudaStreamSynchronize(hp.stream[1]);
+  const cudaError_t e = hp.sync();
   if (rc) return rc;
-  if (e1 != cudaSuccess) return map_cuda(e1);
-  if (e2 != cudaSuccess) return map_cuda(e2);
+  if (e != cudaSuccess) return map_cuda(e);
   return lc_ntt_plan_check(plan, nullptr);
 }
 

@@ -432,8 +432,8 @@ LC_API int lc_quad50_mul_host(lc_quad50_plan* plan, const uint64_t* a, const uin
   int k = 0;
   while (done < count) {
     const size_t c = std::min(chunk, count - done);
-    cudaStream_t s = hp.stream[k & 1];
-    uint64_t* da = static_cast<uint64_t*>(hp.buf[k & 1]);
+    cudaStream_t s = hp.stream[k % HostPipeline::kSlots];
+    uint64_t* da = static_cast<uint64_t*>(hp.buf[k % HostPipeline::kSlots]);
     uint64_t* db = da + chunk * n;
     uint64_t* dout = db + chunk * n;
     cudaMemcpyAsync(da, a + done * n, c * pb, cudaMemcpyHostToDevice, s);
@@ -444,11 +444,9 @@ LC_API int lc_quad50_mul_host(lc_quad50_plan* plan, const uint64_t* a, const uin
     done += c;
     ++k;
   }
-  cudaError_t e1 = cudaStreamSynchronize(hp.stream[0]);
-  cudaError_t e2 = cudaStreamSynchronize(hp.stream[1]);
+  const cudaError_t e = hp.sync();
   if (rc) return rc;
-  if (e1 != cudaSuccess) return map_cuda(e1);
-  return map_cuda(e2);
+  return map_cuda(e);
 }
 
 }  // extern "C"
