@@ -72,3 +72,13 @@ def test_header_cites_reference_interfaces():
     src = open(os.path.join(ROOT, "include", "lattice_cuda.h")).read()
     for cite in ("ntt.rs:46-106", "ntt.rs:118-146", "ntt.rs:187-216", "ntt.rs:38-42"):
         assert cite in src
+
+
+def test_integration_binding_declares_every_entry_point():
+    """The Rust FFI module given in INTEGRATION.md declares every entry point
+    of the header, so a maintainer who copies it reaches the whole ABI."""
+    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    blocks = re.findall(r"```rust\n(.*?)\n```", doc, re.S)
+    declared_rust = {f for b in blocks if 'extern "C"' in b for f in re.findall(r"pub fn (lc_\w+)\(", b)}
+    missing = [f for f in _lib.declared_functions() if f not in declared_rust]
+    assert not missing, missing
