@@ -82,3 +82,43 @@ def test_integration_binding_declares_every_entry_point():
     declared_rust = {f for b in blocks if 'extern "C"' in b for f in re.findall(r"pub fn (lc_\w+)\(", b)}
     missing = [f for f in _lib.declared_functions() if f not in declared_rust]
     assert not missing, missing
+
+
+def test_null_handles_are_rejected():
+    """Every entry point that takes a plan, key, batch, pipeline or output
+    pointer rejects null with LC_ERR_INVALID_ARGUMENT (the getters with -1)
+    before touching a device, like the reference's Result errors."""
+    L = _lib.lib()
+    bad = _lib.LC_ERR_INVALID_ARGUMENT
+    calls = {
+        "lc_ajtai_key_set_fused": (L.lc_ajtai_key_set_fused, (None, 1)),
+        "lc_ajtai_key_set_slot_products": (L.lc_ajtai_key_set_slot_products, (None, 0)),
+        "lc_ajtai_key_set_engine": (L.lc_ajtai_key_set_engine, (None, 0)),
+        "lc_ajtai_key_info": (L.lc_ajtai_key_info, (None, None, None, None)),
+        "lc_ajtai_commit": (L.lc_ajtai_commit, (None, None, 1, None, None)),
+        "lc_ajtai_commit_i8": (L.lc_ajtai_commit_i8, (None, None, 1, None, None)),
+        "lc_ajtai_commit_u8": (L.lc_ajtai_commit_u8, (None, None, 1, None, None)),
+        "lc_ajtai_commit_host": (L.lc_ajtai_commit_host, (None, None, 1, None)),
+        "lc_ajtai_commit_noalloc": (L.lc_ajtai_commit_noalloc, (None, None, 1, None, None)),
+        "lc_ajtai_key_check": (L.lc_ajtai_key_check, (None, None)),
+        "lc_ajtai_key_view": (L.lc_ajtai_key_view, (None, 1, 1, None)),
+        "lc_ntt_inverse": (L.lc_ntt_inverse, (None, None, None, 1, None)),
+        "lc_ntt_forward_host": (L.lc_ntt_forward_host, (None, None, None, 1)),
+        "lc_ntt_plan_info": (L.lc_ntt_plan_info, (None, None, None, None)),
+        "lc_ntt_plan_set_variant": (L.lc_ntt_plan_set_variant, (None, 0)),
+        "lc_ntt_plan_check": (L.lc_ntt_plan_check, (None, None)),
+        "lc_batch_run": (L.lc_batch_run, (None, None)),
+        "lc_batch_info": (L.lc_batch_info, (None, None, None, None, None)),
+        "lc_batch_set_config": (L.lc_batch_set_config, (None, 1, 1, 1)),
+        "lc_fold_pipeline_run": (L.lc_fold_pipeline_run, (None, None)),
+        "lc_fold_pipeline_buffers": (L.lc_fold_pipeline_buffers, (None, None, None, None, None)),
+        "lc_quad50_mul_host": (L.lc_quad50_mul_host, (None, None, None, None, 1)),
+        "lc_quad50_plan_info": (L.lc_quad50_plan_info, (None, None, None)),
+        "lc_lb_commit_host": (L.lc_lb_commit_host, (None, None, 1, None, None, None)),
+        "lc_lb_key_info": (L.lc_lb_key_info, (None, None, None, None, None)),
+        "lc_tc_i8_rate": (L.lc_tc_i8_rate, (1, 1, None, None)),
+    }
+    for name, (fn, args) in calls.items():
+        assert fn(*args) == bad, name
+    for getter in (L.lc_ajtai_key_get_fused, L.lc_ajtai_key_get_slot_products, L.lc_ajtai_key_get_engine):
+        assert getter(None) == -1
