@@ -706,11 +706,10 @@ static int commit_core(lc_ajtai_key* key, size_t batch, uint32_t b_pad, void* ou
     constexpr int JB = sizeof(E) == 8 ? 16 : 32;
     using MC = MacCfg<E, JB>;
     auto kern = mac_tiled_kernel<E, JB>;
-    static bool attr = false;
-    if (!attr) {
-      if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MC::SMEM) != cudaSuccess)
-        return map_cuda(cudaGetLastError());
-      attr = true;
+    static std::atomic<uint64_t> attr_done{0};
+    {
+      const cudaError_t e = smem_attr_once(attr_done, kern, MC::SMEM);
+      if (e != cudaSuccess) return map_cuda(e);
     }
     kern<<<dim3(n, btiles, splits), MC::NT, MC::SMEM, st>>>(ahat, key->a_m, what, part, m, b_pad, n, splits, q,
                                                            key->d_err);
