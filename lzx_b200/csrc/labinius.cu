@@ -197,16 +197,23 @@ static void build_limb(uint32_t q, LbLimb& L) {
   }
 }
 
-static std::once_flag g_maps_once;
-static int g_maps_rc = LC_OK;
+// c_lb_maps is constant memory of each device: uploaded once per device (one
+// bit per device; devices past 63 upload on every call).
+static std::mutex g_maps_mu;
+static uint64_t g_maps_done = 0;
 
 static int ensure_maps() {
-  std::call_once(g_maps_once, [] {
-    LbMaps m;
-    build_maps(m);
-    g_maps_rc = map_cuda(cudaMemcpyToSymbol(c_lb_maps, &m, sizeof(m)));
-  });
-  return g_maps_rc;
+  int dev = 0;
+  const cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return map_cuda(e);
+  const uint64_t bit = (dev >= 0 && dev < 64) ? (uint64_t)1 << dev : 0;
+  std::lock_guard<std::mutex> lk(g_maps_mu);
+  if (bit && (g_maps_done & bit)) return LC_OK;
+  LbMaps m;
+  build_maps(m);
+  const int rc = map_cuda(cudaMemcpyToSymbol(c_lb_maps, &m, sizeof(m)));
+  if (rc == LC_OK) g_maps_done |= bit;
+  return rc;
 }
 
 // ------------------------------------------------------------------ device arithmetic
