@@ -24,12 +24,12 @@ struct HostPipeline {
   cudaStream_t stream[kSlots] = {};
 
   int ensure(size_t need) {
-    if (!stream[0]) {
-      for (int i = 0; i < kSlots; ++i) {
-        if (cudaStreamCreateWithFlags(&stream[i], cudaStreamNonBlocking) != cudaSuccess) {
-          cudaGetLastError();
-          return LC_ERR_CUDA;
-        }
+    // any stream missing (first call, or an earlier creation that failed)
+    for (int i = 0; i < kSlots; ++i) {
+      if (!stream[i] && cudaStreamCreateWithFlags(&stream[i], cudaStreamNonBlocking) != cudaSuccess) {
+        stream[i] = nullptr;
+        cudaGetLastError();
+        return LC_ERR_CUDA;
       }
     }
     if (need <= bytes) return LC_OK;
