@@ -1217,12 +1217,21 @@ static int commit_host(lc_ajtai_key* key, const void* s, size_t in_elem, size_t 
   rc = in_elem == 1 ? (i8 ? lc_ajtai_commit_i8(key, (const int8_t*)key->d_in, batch, key->d_out, st)
                           : lc_ajtai_commit_u8(key, (const uint8_t*)key->d_in, batch, key->d_out, st))
                     : lc_ajtai_commit(key, key->d_in, batch, key->d_out, st);
-  if (rc) return rc;
+  if (rc) {
+    // the input copy may still be reading the caller's (pinned) buffer
+    cudaStreamSynchronize(st);
+    cudaGetLastError();
+    return rc;
+  }
   // the single-launch kernel has no bounded waits and never sets an error word
   const bool flags = !key->last_fused;
   if (cudaMemcpyAsync(stage_out ? key->h_stage_out : out, key->d_out, out_bytes, cudaMemcpyDeviceToHost, st) !=
-      cudaSuccess)
-    return map_cuda(cudaGetLastError());
+      cudaSuccess) {
+    const int err = map_cuda(cudaGetLastError());
+    cudaStreamSynchronize(st);  // nothing queued may still read the caller's input
+    cudaGetLastError();
+    return err;
+  }
   // both error words come back with the result: one synchronisation per call
   if (flags) {
     cudaMemcpyAsync(key->h_flags, key->d_err, 4, cudaMemcpyDeviceToHost, st);
