@@ -122,3 +122,29 @@ def test_null_handles_are_rejected():
         assert fn(*args) == bad, name
     for getter in (L.lc_ajtai_key_get_fused, L.lc_ajtai_key_get_slot_products, L.lc_ajtai_key_get_engine):
         assert getter(None) == -1
+
+
+def test_every_status_has_a_message_and_maps_to_an_error():
+    """Each lc_status of the header has its own message; the Python layer
+    turns LC_ERR_DIMENSION_MISMATCH into AjtaiError::DimensionMismatch
+    (ajtai.rs:44-49) and every other failure into LatticeCudaError."""
+    from lzx_b200.commitment import AjtaiError, _map_status
+    src = open(os.path.join(ROOT, "include", "lattice_cuda.h")).read()
+    codes = {name: int(v) for name, v in re.findall(r"\b(LC_(?:OK|ERR_\w+))\s*=\s*(\d+)", src)}
+    assert codes["LC_OK"] == 0 and len(codes) >= 10
+    L = _lib.lib()
+    msgs = {c: L.lc_status_string(v) for c, v in codes.items()}
+    assert all(m and m != b"unknown status" for m in msgs.values()), msgs
+    assert len(set(msgs.values())) == len(msgs)
+    _map_status(0, "ok")
+    for name, v in codes.items():
+        if v == 0:
+            continue
+        if name == "LC_ERR_DIMENSION_MISMATCH":
+            with pytest.raises(AjtaiError) as e:
+                _map_status(v, "commit")
+            assert e.value.kind == "DimensionMismatch"
+        else:
+            with pytest.raises(_lib.LatticeCudaError) as e:
+                _map_status(v, "commit")
+            assert e.value.status == v and "commit" in str(e.value)
