@@ -374,22 +374,31 @@ def bench_commit(args, rank, max_over_ranks, barrier, world):
     # N = B witnesses x 8 limbs, K = m ring elements
     sp_ops = 2 * C_D * (16 * 8) * (8 * C_B) * C_M
     res["ntt_tensor_products"]["slot_product_int8_ops_per_batch"] = sp_ops
-    del W
+    res["bit_exact"] = True  # the three forms agree (asserted above)
+    outs_host = (outs["plain"][:4].cpu().numpy().view("uint64") if rank == 0 and not args.no_cpu_baseline
+                 else None)
+    del W, outs
     if rank == 0 and not args.no_cpu_baseline:
         import oracle
         oracle.prefer_native(True)
         nt = host_threads()
         t = oracle.NttTablesGl(6)
-        a_host = synth.synth_gl(4321, 0, C_KAPPA * C_M * C_D)
+        a_host = synth.synth_gl(4321 + rank, 0, C_KAPPA * C_M * C_D)
         a_ntt = t.forward_batch(a_host, nthreads=nt)
-        wb = synth.synth_i8(4321, 1, 4 * C_M * C_D).reshape(4, C_M, C_D)
+        wb = synth.synth_i8(4321 + rank, 1, 4 * C_M * C_D).reshape(4, C_M, C_D)
         t0 = time.perf_counter()
-        oracle.ajtaigl_commit_batch(t, a_ntt, C_KAPPA, C_M, wb, nthreads=nt, simd=True, native=True)
+        got = oracle.ajtaigl_commit_batch(t, a_ntt, C_KAPPA, C_M, wb, nthreads=nt, simd=True, native=True)
         dt = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        oracle.ajtaigl_commit_batch(t, a_ntt, C_KAPPA, C_M, wb[:1], nthreads=1, simd=True, native=True)
+        dt1 = time.perf_counter() - t0
+        res["bit_exact_vs_oracle_sample"] = bool((got == outs_host[:4]).all()) if outs_host is not None else None
         res["cpu_baseline"] = {"value": 4 * C_M / dt, "unit": "ring-elems/s", "cores": nt,
                                "kind": "port",
                                "sample": f"4 of the 128 witnesses, full n=2^16, {nt} threads, "
-                                         "AVX-512 Goldilocks MAC where available"}
+                                         "AVX-512 Goldilocks MAC where available",
+                               "single_thread": {"value": C_M / dt1, "cores": 1,
+                                                 "sample": "1 of the 128 witnesses, full n=2^16"}}
     return res
 
 
@@ -465,6 +474,7 @@ def bench_fold(args, rank, max_over_ranks, barrier, world):
     key.slot_products = GoldilocksAjtaiKey.PRODUCTS_TENSOR
     assert torch.equal(commits["graph"], commits["graph_int64_products"]), "slot product forms differ"
     assert torch.equal(commits["eager"], commits["graph"])
+    res["forms_agree"] = True  # eager, graph and integer-product commits are identical (asserted)
     del commits
     if rank == 0 and not args.no_cpu_baseline:
         import numpy as np
@@ -478,16 +488,20 @@ def bench_fold(args, rank, max_over_ranks, barrier, world):
         a_ntt = t.forward_batch(a_host, nthreads=nt)
         z = synth.synth_gl(97, 1, ms_ * 64)
         tabs = [oracle.NttTables32(oracle.Modulus32(*q), 6) for q in oracle.CRT_PRIMES]
-        t0 = time.perf_counter()
-        digits = oracle.decomp_b(z, 8)
-        oracle.ajtaigl_commit_batch(t, a_ntt, F_KAPPA, ms_, digits.reshape(8, ms_, 64), nthreads=nt,
-                                    simd=True, native=True)
-        for tb, (q, _, _) in zip(tabs, oracle.CRT_PRIMES):
-            tb.forward_batch((z % np.uint64(q)).astype(np.uint32), nthreads=nt)
-        dt = time.perf_counter() - t0
+        def step(threads):
+            t0 = time.perf_counter()
+            digits = oracle.decomp_b(z, 8)
+            oracle.ajtaigl_commit_batch(t, a_ntt, F_KAPPA, ms_, digits.reshape(8, ms_, 64), nthreads=threads,
+                                        simd=True, native=True)
+            for tb, (q, _, _) in zip(tabs, oracle.CRT_PRIMES):
+                tb.forward_batch((z % np.uint64(q)).astype(np.uint32), nthreads=threads)
+            return time.perf_counter() - t0
+        dt = step(nt)
+        dt1 = step(1)
         res["cpu_baseline"] = {"value": ms_ / dt, "unit": "witness ring-elems/s", "cores": nt, "kind": "port",
                                "sample": f"one folding step at m={ms_} (decomp_b, 8 digit commits with the "
-                                         f"AVX-512 MAC where available, 4-prime CRT NTT), {nt} threads"}
+                                         f"AVX-512 MAC where available, 4-prime CRT NTT), {nt} threads",
+                               "single_thread": {"value": ms_ / dt1, "cores": 1}}
     return res
 
 
@@ -498,17 +512,19 @@ U_WORKLOAD = ("uneven commit jobs: d in {64,128,256}, n log-uniform in [2^10, 2^
               "work-queue launches, CUDA graph, autotuned) vs the same jobs one commit call at a time")
 
 
-def bench_uneven(args, rank, max_over_ranks, barrier, world):
-    """Total committed ring elements/s (sum of n over the jobs)."""
+def uneven_workload(rank: int, nj: int = 512, lmax: int = 18):
+    """The uneven batch: six key classes (d in {64,128,256} x Goldilocks or the
+    4-prime CRT set; kappa = 16, m = 2^lmax; keys from seeded device streams)
+    and nj jobs (class, n log-uniform in [2^10, 2^lmax], kappa in {8,16},
+    int8 witnesses in one device buffer, outputs in one buffer per element
+    type).  Returns a dict of everything the bench leg and the parity test use."""
     import numpy as np
     import torch
 
-    from lzx_b200 import CRT_SET_30BIT, GoldilocksAjtaiKey, synth, tune
-    from lzx_b200.batch import CommitBatch, CommitJob, U32AjtaiKey, key_view
+    from lzx_b200 import CRT_SET_30BIT, GoldilocksAjtaiKey, synth
+    from lzx_b200.batch import CommitJob, U32AjtaiKey
     rng = np.random.default_rng(2024 + rank)
-    nj, lmax = args.uneven_jobs, args.uneven_log_nmax
     m = 1 << lmax
-    # classes: (log_d, Goldilocks?) with one kappa=16, m=2^lmax key (or one per CRT prime)
     specs = [(ld, gl) for gl in (True, False) for ld in (6, 7, 8)]
     classes = []
     for ci, (ld, gl) in enumerate(specs):
@@ -525,7 +541,6 @@ def bench_uneven(args, rank, max_over_ranks, barrier, world):
                 keys.append(U32AjtaiKey(mod, ld, 16, m, A))
             classes.append(keys)
         del A
-    # jobs: witnesses in one device buffer, outputs in one buffer per element type
     cls_of = rng.integers(len(specs), size=nj)
     ns = np.floor(2.0 ** (10 + (lmax - 10) * rng.random(nj))).astype(np.int64)
     kappas = rng.choice([8, 16], size=nj)
@@ -554,6 +569,24 @@ def bench_uneven(args, rank, max_over_ranks, barrier, world):
         out = (OG[gofs[i]:gofs[i] + k * d].view(1, k, d) if gl
                else OU[uofs[i]:uofs[i] + 4 * k * d].view(4, k, d))
         jobs.append(CommitJob(int(cls_of[i]), k, n, w, out))
+    return {"m": m, "specs": specs, "classes": classes, "cls_of": cls_of, "ns": ns, "kappas": kappas,
+            "W": W, "OG": OG, "OU": OU, "gofs": gofs, "uofs": uofs, "wtot": wtot, "jobs": jobs,
+            "key_seeds": [300 + ci for ci in range(len(specs))]}
+
+
+def bench_uneven(args, rank, max_over_ranks, barrier, world):
+    """Total committed ring elements/s (sum of n over the jobs)."""
+    import numpy as np
+    import torch
+
+    from lzx_b200 import synth, tune
+    from lzx_b200.batch import CommitBatch, key_view
+    nj, lmax = args.uneven_jobs, args.uneven_log_nmax
+    wl = uneven_workload(rank, nj, lmax)
+    specs, classes, jobs = wl["specs"], wl["classes"], wl["jobs"]
+    cls_of, ns, kappas = wl["cls_of"], wl["ns"], wl["kappas"]
+    W, OG, OU, gofs, uofs, wtot = wl["W"], wl["OG"], wl["OU"], wl["gofs"], wl["uofs"], wl["wtot"]
+    del wl
     total_elems = int(ns.sum())
     res = {"workload": U_WORKLOAD.replace("LOG", str(lmax)), "jobs": nj, "sum_n": total_elems,
            "unit": "committed ring-elems/s"}
@@ -630,37 +663,58 @@ def bench_uneven(args, rank, max_over_ranks, barrier, world):
         raise RuntimeError("batch outputs differ from the one-by-one commits")
     del batch
     if rank == 0 and not args.no_cpu_baseline:
+        from concurrent.futures import ThreadPoolExecutor
+
         import oracle
         oracle.prefer_native(True)
         nt = host_threads()
         sample = [i for i in range(nj) if ns[i] <= 8192][:12]
-        t_cpu, elems = 0.0, 0
+        # inputs and cached NTT(A) prepared outside the timed region; the timed
+        # part is the reference's commit per job (MAC + witness NTTs + inverse)
+        work = []
         for i in sample:
             ld, gl = specs[cls_of[i]]
             d, n, k = 1 << ld, int(ns[i]), int(kappas[i])
             wv = jobs[i].w.cpu().numpy()
             if gl:
-                a_h = synth.synth_gl(7, i, k * n * d)
                 t = oracle.NttTablesGl(ld)
-                a_ntt = t.forward_batch(a_h, nthreads=nt)
-                t0 = time.perf_counter()
-                oracle.ajtaigl_commit_batch(t, a_ntt, k, n, wv.reshape(1, n, d), nthreads=nt, simd=True,
-                                            native=True)
-                t_cpu += time.perf_counter() - t0
+                work.append(("gl", t, t.forward_batch(synth.synth_gl(7, i, k * n * d), nthreads=nt), k, n,
+                             wv.reshape(1, n, d)))
             else:
                 for pi, mod in enumerate(oracle.CRT_PRIMES):
                     t = oracle.NttTables32(oracle.Modulus32(*mod), ld)
-                    a_h = synth.synth_mod32(7, i * 4 + pi, mod[0], k * n * d)
-                    a_ntt = t.forward_batch(a_h.reshape(-1, d), nthreads=nt)
+                    a_ntt = t.forward_batch(synth.synth_mod32(7, i * 4 + pi, mod[0], k * n * d).reshape(-1, d),
+                                            nthreads=nt)
                     s_res = np.where(wv < 0, mod[0] - np.abs(wv.astype(np.int64)), wv).astype(np.uint32)
-                    t0 = time.perf_counter()
-                    oracle.ajtai32_commit(t, a_ntt, k, n, s_res)
-                    t_cpu += time.perf_counter() - t0
-            elems += n
-        res["cpu_baseline"] = {"value": elems / t_cpu, "unit": "committed ring-elems/s", "cores": nt,
+                    work.append(("u32", t, a_ntt, k, n, s_res))
+        elems = sum(int(ns[i]) for i in sample)
+
+        def one(w, threads):
+            kind, t, a_ntt, k, n, wv = w
+            if kind == "gl":
+                oracle.ajtaigl_commit_batch(t, a_ntt, k, n, wv, nthreads=threads, simd=True, native=True)
+            else:
+                oracle.ajtai32_commit(t, a_ntt, k, n, wv)
+
+        t0 = time.perf_counter()
+        for w in work:
+            one(w, 1)
+        t_one = time.perf_counter() - t0
+        # all cores: Goldilocks jobs spread their MAC over the threads; the
+        # single-threaded u32 commits (one per job and prime) run side by side
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(nt) as ex:
+            list(ex.map(lambda w: one(w, 1), [w for w in work if w[0] == "u32"]))
+        for w in work:
+            if w[0] == "gl":
+                one(w, nt)
+        t_all = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": elems / t_all, "unit": "committed ring-elems/s", "cores": nt,
                                "kind": "port",
                                "sample": f"{len(sample)} of the jobs with n <= 8192 (oracle cached-NTT commit "
-                                         f"per job; Goldilocks MAC on {nt} threads, u32 commits 1 thread)"}
+                                         f"per job; Goldilocks MAC on {nt} threads, u32 commits per job and "
+                                         f"prime side by side)",
+                               "single_thread": {"value": elems / t_one, "cores": 1}}
     return res
 
 
@@ -1124,16 +1178,104 @@ def run_ours(args):
                 "steps": KE, "api": "lc_ntt_forward_host + lc_ntt_inverse_host, pinned host memory"},
         "gpu_launches": 2 * K,
         "clocks": clocks,
-        "commit": commit,
-        "fold": fold,
-        "uneven_batch": uneven,
-        "key_from_seed": keygen,
-        "single_commit": single,
-        "quad_slot_mul": quad50,
-        "labinius_commit": labinius,
+        # full records of every leg first; the short summaries of configs 1,
+        # 3, 4 and 5 close the line, so that the last ~1.5 kB carry them
+        "detail": {"commit": commit, "fold": fold, "uneven_batch": uneven, "single_commit": single,
+                   "key_from_seed": keygen, "quad_slot_mul": quad50, "labinius_commit": labinius},
+        "single_commit": compact_single(single),
+        "uneven_batch": compact_uneven(uneven),
+        "fold": compact_fold(fold),
+        "commit": compact_commit(commit),
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+# ------------------------------------------------------------------ compact summaries
+
+def _sig(x, n: int = 4):
+    """x rounded to n significant digits (floats only), for the short summaries."""
+    import math
+    if isinstance(x, bool) or not isinstance(x, float) or x == 0 or not math.isfinite(x):
+        return x
+    return float(f"{x:.{n}g}")
+
+
+def _get(d, *path):
+    for p in path:
+        if not isinstance(d, dict) or p not in d:
+            return None
+        d = d[p]
+    return d
+
+
+def _cpu_short(cb):
+    if not cb:
+        return None
+    return {"all": _sig(cb.get("value")), "1t": _sig(_get(cb, "single_thread", "value")), "cores": cb.get("cores"),
+            "kind": cb.get("kind")}
+
+
+def compact_commit(c):
+    """Config 3 in a few hundred characters: ms and committed ring elements/s of
+    the three forms on the same inputs, the INT8 roofline of the tensor engine,
+    end to end, CPU (1 thread and all cores) and the exactness flags."""
+    if not c:
+        return None
+    out = {"cfg": "GL d64 k16 n2^16 B128 int8", "unit": "ring-elems/s", "bit_exact": c.get("bit_exact"),
+           "oracle_sample_exact": c.get("bit_exact_vs_oracle_sample")}
+    for name, short in (("plain", "plain"), ("tensor", "tensor"), ("ntt_tensor_products", "ntt_tensor")):
+        r = c.get(name) or {}
+        out[short] = {"ms": _sig(r.get("ms_per_batch")), "v": _sig(r.get("value")),
+                      "e2e": _sig(_get(r, "e2e", "value"))}
+    out["tensor_vs_plain"] = _sig(c.get("speedup_tensor_vs_plain"), 3)
+    out["ntt_tensor_vs_plain"] = _sig(c.get("speedup_ntt_tensor_products_vs_plain"), 3)
+    rf = _get(c, "tensor", "roofline") or {}
+    out["int8_roofline"] = {"frac": _sig(rf.get("frac"), 3), "tops": _sig(rf.get("achieved")),
+                            "peak": _sig(rf.get("peak")), "src": "measured"}
+    e = _get(c, "plain", "e2e") or {}
+    out["e2e_bytes"] = {"h2d": e.get("h2d_bytes_per_step"), "d2h": e.get("d2h_bytes_per_step")}
+    out["cpu"] = _cpu_short(c.get("cpu_baseline"))
+    return out
+
+
+def compact_fold(f):
+    """Config 5: the graph-captured folding step."""
+    if not f:
+        return None
+    g = f.get("graph") or {}
+    e = g.get("e2e") or {}
+    return {"cfg": f"m={f.get('m')} GL d64 k16 + CRT NTT", "unit": "witness ring-elems/s",
+            "ms": _sig(g.get("ms_per_step")), "v": _sig(g.get("value")),
+            "int64_products_ms": _sig(_get(f, "graph_int64_products", "ms_per_step")),
+            "eager_ms": _sig(_get(f, "eager", "ms_per_step")), "forms_agree": f.get("forms_agree"),
+            "e2e": {"v": _sig(e.get("value")), "h2d": e.get("h2d_bytes_per_step"),
+                    "d2h": e.get("d2h_bytes_per_step")},
+            "cpu": _cpu_short(f.get("cpu_baseline"))}
+
+
+def compact_uneven(u):
+    """Config 4: the batch against the same jobs one commit call at a time."""
+    if not u:
+        return None
+    b = u.get("batch") or {}
+    e = b.get("e2e") or {}
+    return {"jobs": u.get("jobs"), "sum_n": u.get("sum_n"), "unit": "committed ring-elems/s",
+            "batch_ms": _sig(b.get("ms")), "v": _sig(b.get("value")),
+            "one_by_one_ms": _sig(_get(u, "one_by_one", "ms")),
+            "speedup": _sig(u.get("speedup_batch_vs_one_by_one"), 3),
+            "bit_exact": b.get("bit_exact_vs_one_by_one"),
+            "e2e": {"v": _sig(e.get("value")), "h2d": e.get("h2d_bytes_per_step"),
+                    "d2h": e.get("d2h_bytes_per_step")},
+            "cpu": _cpu_short(u.get("cpu_baseline"))}
+
+
+def compact_single(s):
+    """Config 1: one commitment's latency."""
+    if not s:
+        return None
+    return {"device_us": _sig(s.get("device_us_per_commit"), 3), "e2e_us": _sig(s.get("e2e_us_per_commit"), 3),
+            "cpu_1t_us": _sig(_get(s, "cpu_baseline", "value"), 3)}
 
 
 def run_only(args, which):

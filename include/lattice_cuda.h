@@ -170,7 +170,10 @@ LC_API int lc_ajtai_commit_u8(lc_ajtai_key *key, const uint8_t *s, size_t batch,
 LC_API int lc_ajtai_commit_host(lc_ajtai_key *key, const void *s, size_t batch, void *out);
 LC_API int lc_ajtai_commit_i8_host(lc_ajtai_key *key, const int8_t *s, size_t batch, void *out);
 LC_API int lc_ajtai_commit_u8_host(lc_ajtai_key *key, const uint8_t *s, size_t batch, void *out);
-/* Wait for `stream` and report device-side errors of this key's kernels. */
+/* Wait for `stream` and report device-side errors of this key's kernels
+ * (LC_ERR_TIMEOUT).  The error word is cleared by the report, except when a
+ * timed-out kernel could not confirm that its own copies had landed: that
+ * state stays set and every later check reports it. */
 LC_API int lc_ajtai_key_check(lc_ajtai_key *key, lc_stream stream);
 
 /* A view of the first k rows and m columns of `parent`'s A: commits through
@@ -261,17 +264,20 @@ LC_API int lc_ajtai_key_get_slot_products(const lc_ajtai_key *key);
 
 /* Commit without allocating any device memory.  No counterpart in the
  * reference: it exists for callers that cannot call cudaMalloc while they
- * commit -- code that records work into a CUDA graph, processes whose device
- * memory is already handed out by another allocator under a fixed budget, and
- * latency-critical verifiers that cannot afford cudaMalloc's implicit device
- * synchronisation.  It computes exactly what lc_ajtai_commit computes for the
- * same key and residues (device pointers s = [batch][m][n], out =
- * [batch][k][n]), but its scratch is one fixed 16 MiB array compiled into this
- * library, which every GPU that loads the library keeps for the life of the
- * process.  The key (created beforehand, which does allocate) is only read.
- * Limits: log_n 6..8, and n*m*b_pad + batch*k*n + n*16*b_pad elements must fit
- * in 16 MiB (b_pad = batch below 64, else batch rounded up to 128); a larger
- * request returns LC_ERR_INVALID_ARGUMENT without touching the GPU.
+ * commit -- processes whose device memory is already handed out by another
+ * allocator under a fixed budget, and latency-critical verifiers that cannot
+ * afford cudaMalloc's implicit device synchronisation.  It computes exactly
+ * what lc_ajtai_commit computes for the same key and residues (device
+ * pointers s = [batch][m][n], out = [batch][k][n]), but its scratch is one
+ * fixed 16 MiB array compiled into this library, which every GPU that loads
+ * the library keeps for the life of the process.  The key (created
+ * beforehand, which does allocate) is only read.
+ * Limits: log_n 6..8, and three regions must fit in 16 MiB together: the
+ * witness transforms (n*m*b_pad elements) and the summed rows (batch*k*n
+ * elements), each rounded up to a multiple of 256 bytes, plus one K-split of
+ * partial sums (n*16*b_pad elements); b_pad = batch below 64, else batch
+ * rounded up to 128.  A larger request returns LC_ERR_INVALID_ARGUMENT
+ * without touching the GPU.
  * The first call on each device looks up the array's device address; make that
  * first call before any stream capture.  All calls share the one array, so
  * calls whose kernels overlap on the GPU (different streams, or different host

@@ -11,8 +11,8 @@ Same names, argument meaning and error behaviour as idrees2516/lzx's
 * :class:`GoldilocksAjtaiKey`: the same cached-NTT commitment over Goldilocks
   for batches of witnesses given as residues or int8 digits.
 
-The seed expansion (SHAKE-256) runs on the host; the cached NTT(A) lives on
-the GPU and every commit runs there (``lc_ajtai_*`` of the C ABI).
+The seed expansion (SHAKE-256, ``lc_uniform_from_seed``), the cached NTT(A)
+and every commit run on the GPU (``lc_ajtai_*`` of the C ABI).
 """
 from __future__ import annotations
 

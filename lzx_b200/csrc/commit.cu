@@ -283,11 +283,17 @@ __global__ void __launch_bounds__(256)
   if (failed) {
     if (tid == 0) {
       record_error(err, LC_DEVERR_TIMEOUT);
-      // the prefetch of the following block may still be landing (bounded wait)
+      // Copies that may still be landing must finish before the CTA exits:
+      // the block whose wait expired (its phase is the one before the
+      // toggle) and the prefetch of the following block.  Bounded waits; if
+      // either expires again, the error word is marked poisoned.
+      const int f = failed_blk & 1;
+      bool landed = mbar_wait(&bar[f], ((parity >> f) & 1u) ^ 1u);
       if (failed_blk + 1 < nblk) {
-        const int o = (failed_blk & 1) ^ 1;
-        mbar_wait(&bar[o], (parity >> o) & 1u);
+        const int o = f ^ 1;
+        landed = mbar_wait(&bar[o], (parity >> o) & 1u) && landed;
       }
+      if (!landed) record_poisoned(err);
     }
     return;
   }
@@ -1241,7 +1247,7 @@ static int commit_host(lc_ajtai_key* key, const void* s, size_t in_elem, size_t 
   if (e != cudaSuccess) return map_cuda(e);
   if (stage_out) std::memcpy(out, key->h_stage_out, out_bytes);
   if (flags && (key->h_flags[0] | key->h_flags[1])) {
-    cudaMemsetAsync(key->d_err, 0, 4, st);
+    if (key->h_flags[0] != LC_DEVERR_POISONED) cudaMemsetAsync(key->d_err, 0, 4, st);
     cudaMemsetAsync(key->plan->d_err, 0, 4, st);
     cudaStreamSynchronize(st);
     return LC_ERR_TIMEOUT;
@@ -1269,7 +1275,7 @@ LC_API int lc_ajtai_key_check(lc_ajtai_key* key, lc_stream stream) {
   if (cudaMemcpy(&flag, key->d_err, 4, cudaMemcpyDeviceToHost) != cudaSuccess)
     return map_cuda(cudaGetLastError());
   if (flag) {
-    cudaMemset(key->d_err, 0, 4);
+    if (flag != LC_DEVERR_POISONED) cudaMemset(key->d_err, 0, 4);  // a poisoned word stays set
     return LC_ERR_TIMEOUT;
   }
   return lc_ntt_plan_check(key->plan, stream);

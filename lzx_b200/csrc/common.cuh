@@ -17,9 +17,13 @@
 // LC_DEVERR_TIMEOUT in the plan's device error word and returns.
 constexpr uint32_t kSpinLimit = 1u << 26;
 
+// LC_DEVERR_POISONED: after a timeout, a bulk copy of the timed-out kernel
+// did not land within a second bounded wait either, so it may still write
+// into shared memory that a later CTA owns; the word stays set (sticky).
 enum : uint32_t {
   LC_DEVERR_NONE = 0,
   LC_DEVERR_TIMEOUT = 1,
+  LC_DEVERR_POISONED = 2,
 };
 
 namespace lc {
@@ -98,6 +102,10 @@ LC_D void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta
 
 LC_D void record_error(uint32_t* err, uint32_t code) {
   if (err) atomicCAS(err, 0u, code);
+}
+
+LC_D void record_poisoned(uint32_t* err) {
+  if (err) atomicMax(err, (uint32_t)LC_DEVERR_POISONED);
 }
 
 }  // namespace lc

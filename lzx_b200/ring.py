@@ -293,23 +293,12 @@ class RingConfig:
         return RingElement(self, (b.astype(np.uint64) % self.modulus.q).astype(np.uint32))
 
     def uniform_from_seed(self, domain: bytes, seed: bytes, index: int):
-        """``RingConfig::uniform_from_seed`` (ring.rs:102-180)."""
-        n, q = self.n(), self.modulus.q
-        salt = domain + seed + struct.pack("<Q", index)
-        limit = (1 << 32) - ((1 << 32) % q)
-        slack = max(n, 16)
-        stream = _xof(b"uniform", salt, 8 + 4 * (n + slack))
-        cand = np.frombuffer(stream[8:], dtype="<u4").astype(np.uint64)
-        ok = cand[cand < limit][:n]
-        coeffs = list((ok % q).astype(np.uint32))
-        counter = (len(stream) - 8) // 4
-        while len(coeffs) < n:  # ring.rs:155-175
-            b = _xof(b"uniform", salt, 8 + counter * 4 + 4)
-            c = struct.unpack_from("<I", b, len(b) - 4)[0]
-            if c < limit:
-                coeffs.append(c % q)
-            counter += 1
-        return RingElement(self, np.array(coeffs, dtype=np.uint32))
+        """``RingConfig::uniform_from_seed`` (ring.rs:102-180): one element,
+        expanded on the GPU by ``lc_uniform_from_seed`` with count 1."""
+        import torch
+        out = self.uniform_from_seed_batch(domain, seed, index, 1)
+        torch.cuda.synchronize()
+        return RingElement(self, out[0].cpu().numpy().view(np.uint32).copy())
 
     def uniform_from_seed_batch(self, domain: bytes, seed: bytes, index0: int, count: int, out=None):
         """``uniform_from_seed`` for indices index0 .. index0+count-1 on the GPU

@@ -1307,6 +1307,7 @@ uint64_t orc_synth_u64(uint64_t seed, uint64_t stream, uint64_t index) {
 void orc_synth_mod32(uint64_t seed, uint64_t stream, uint32_t q, uint32_t *out, size_t count,
                      size_t offset) {
   uint64_t limit = ((uint64_t)1 << 32) - (((uint64_t)1 << 32) % q);
+#pragma omp parallel for schedule(static)
   for (size_t i = 0; i < count; i++) {
     for (uint64_t r = 0;; r++) {
       uint64_t c = orc_synth_u64(seed, stream + (r << 40), offset + i) & 0xFFFFFFFFull;
@@ -1319,6 +1320,7 @@ void orc_synth_mod32(uint64_t seed, uint64_t stream, uint32_t q, uint32_t *out, 
 }
 
 void orc_synth_gl(uint64_t seed, uint64_t stream, uint64_t *out, size_t count, size_t offset) {
+#pragma omp parallel for schedule(static)
   for (size_t i = 0; i < count; i++) {
     for (uint64_t r = 0;; r++) {
       uint64_t c = orc_synth_u64(seed, stream + (r << 40), offset + i);

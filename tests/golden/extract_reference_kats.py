@@ -9,8 +9,8 @@ run) and writes ``reference_kats.json`` beside this script:
   (``sha3_256_kat`` / ``shake256_kat``),
 * the Modulus32 constants, ``crates/lattice-ring/src/modulus.rs``.
 
-Usage: python tests/golden/extract_reference_kats.py [REFERENCE_ROOT]
-(default REFERENCE_ROOT is /root/reference, the read-only checkout).
+Usage: python tests/golden/extract_reference_kats.py REFERENCE_ROOT
+(or with the REFERENCE_ROOT environment variable set to the checkout).
 """
 from __future__ import annotations
 
@@ -85,7 +85,9 @@ def modulus_constants(root: str) -> dict:
 
 
 def main() -> None:
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: extract_reference_kats.py REFERENCE_ROOT (or set REFERENCE_ROOT)")
     data = {
         "reference": "idrees2516/lzx",
         "goldilocks": goldilocks_kats(root),

@@ -42,3 +42,35 @@ def test_reference_arm_other_ranks_do_no_work():
                           "--warmup", "1", "--gpus", "2"], capture_output=True, text=True, cwd=ROOT, env=env,
                          timeout=300, check=True).stdout
     assert not [l for l in out.splitlines() if l.startswith("{")]
+
+
+def test_short_summaries_fit_the_kept_tail():
+    """The JSON line ends with the short summaries of configs 1, 3, 4 and 5;
+    with full-precision inputs they must fit well inside the last 1500
+    characters of the line, which is what a log tail keeps."""
+    sys.path.insert(0, ROOT)
+    import json as _json
+
+    import bench
+    f = 1234567.891234567
+    e2e = {"value": f, "unit": "u", "h2d_bytes_per_step": 536870912, "d2h_bytes_per_step": 268435456}
+    cpu = {"value": f, "unit": "u", "cores": 128, "kind": "port", "sample": "x" * 200,
+           "single_thread": {"value": f, "cores": 1, "sample": "y" * 100}}
+    commit = {"bit_exact": True, "bit_exact_vs_oracle_sample": True,
+              "speedup_tensor_vs_plain": f, "speedup_ntt_tensor_products_vs_plain": f, "cpu_baseline": cpu,
+              **{k: {"ms_per_batch": f, "value": f, "e2e": e2e} for k in ("plain", "tensor", "ntt_tensor_products")}}
+    commit["tensor"]["roofline"] = {"frac": f, "achieved": f, "peak": f}
+    fold = {"m": 1048576, "forms_agree": True, "cpu_baseline": cpu,
+            "graph": {"ms_per_step": f, "value": f, "e2e": e2e}, "eager": {"ms_per_step": f},
+            "graph_int64_products": {"ms_per_step": f}}
+    uneven = {"jobs": 512, "sum_n": 24000000, "speedup_batch_vs_one_by_one": f, "cpu_baseline": cpu,
+              "one_by_one": {"ms": f}, "batch": {"ms": f, "value": f, "bit_exact_vs_one_by_one": True, "e2e": e2e}}
+    single = {"device_us_per_commit": f, "e2e_us_per_commit": f, "cpu_baseline": {"value": f}}
+    tail = {"single_commit": bench.compact_single(single), "uneven_batch": bench.compact_uneven(uneven),
+            "fold": bench.compact_fold(fold), "commit": bench.compact_commit(commit)}
+    s = _json.dumps(tail)
+    assert len(s) < 1400, len(s)
+    c = tail["commit"]
+    assert c["plain"]["v"] == 1235000.0 and c["int8_roofline"]["frac"] == 1230000.0
+    assert c["cpu"]["1t"] and c["cpu"]["all"] and tail["fold"]["cpu"]["1t"] and tail["uneven_batch"]["cpu"]["1t"]
+    assert bench.compact_commit(None) is None and bench.compact_fold({}) is None

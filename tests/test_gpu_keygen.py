@@ -5,7 +5,8 @@ device against the golden vectors and the oracle -- every modulus family,
 every ring degree, domains long enough to need several SHAKE blocks, the
 three padding edges of the absorbed message, indices near 2^64 -- and
 AjtaiPublicKey::from_seed (lattice-commitment/src/ajtai.rs:87-103) on the
-device against the host expansion: same matrix, same commitments.
+device against the oracle's expansion: same matrix, same commitments.  A
+single-element uniform_from_seed runs on the device too.
 """
 import numpy as np
 import pytest
@@ -76,24 +77,39 @@ def test_uniform_rejects_oversize_and_goldilocks():
     assert st == _lib.LC_ERR_UNSUPPORTED
 
 
+def oracle_key(params, seed):
+    """The oracle's AjtaiPublicKey::from_seed (ajtai.rs:87-103) as a key over its matrix."""
+    t = oracle.NttTables32(omod(params.ring.modulus), params.ring.log_n)
+    mat, _ = oracle.ajtai32_from_seed(t, params.k, params.m, seed)
+    return AjtaiPublicKey(params, seed, mat.reshape(params.k * params.m, params.ring.n()))
+
+
 @pytest.mark.parametrize("log_n,k,m", [(6, 2, 64), (8, 2, 300), (4, 3, 17)])
-def test_key_from_seed_matches_host_expansion(log_n, k, m):
+def test_key_from_seed_matches_oracle_expansion(log_n, k, m):
     params = AjtaiParams(RingConfig(Modulus32.Q_32, log_n), k, m, 1 << 20)
     seed = bytes([0xAB]) * 32
     dev = AjtaiPublicKey.from_seed(params, seed)
-    host = AjtaiPublicKey.from_seed_host(params, seed)
-    assert np.array_equal(dev._matrix, host._matrix)
+    want = oracle_key(params, seed)
+    assert np.array_equal(dev._matrix, want._matrix)
     s = sample_small_secret(params.ring, m, 1 << 12, b"kg")
-    assert dev.commit(s) == host.commit(s)
+    assert dev.commit(s) == want.commit(s)
+
+
+def test_single_element_uniform_from_seed_runs_on_device():
+    ring = RingConfig(Modulus32.Q_32, 6)
+    seed = bytes([0x5A]) * 32
+    for idx in (0, 1, 12345):
+        got = ring.uniform_from_seed(b"ajtai-A", seed, idx).coeffs()
+        assert np.array_equal(got, oracle.uniform_from_seed(omod(Modulus32.Q_32), 6, b"ajtai-A", seed, idx))
 
 
 def test_c_abi_key_from_seed():
     """lc_ajtai_key_from_seed builds the same key as a key created from the
-    host-expanded matrix."""
+    oracle-expanded matrix."""
     import ctypes as C
     params = AjtaiParams(RingConfig(Modulus32.Q_32, 6), 2, 40, 1 << 20)
     seed = bytes(range(100, 132))
-    host = AjtaiPublicKey.from_seed_host(params, seed)
+    host = oracle_key(params, seed)
     h = C.c_void_p()
     L = _lib.lib()
     _lib.check(L.lc_ajtai_key_from_seed(params.ring.tables.handle, 2, 40, seed, C.byref(h)), "from_seed")

@@ -1,13 +1,14 @@
 """The commit entry point that allocates no device memory.
 
 lc_ajtai_commit_noalloc serves callers that cannot call cudaMalloc while they
-commit: work recorded into a CUDA graph, processes whose device memory is
-already owned by another allocator, latency-critical verifiers that cannot
-take cudaMalloc's implicit synchronisation.  Its scratch is a fixed 16 MiB
-array inside the library.  These tests call it through the C ABI, twice in a
-row with different witnesses, and require exactly the residues that the
-ordinary lc_ajtai_commit returns for the same key and input; a request larger
-than the fixed scratch must be refused without running.
+commit: processes whose device memory is already owned by another allocator,
+latency-critical verifiers that cannot take cudaMalloc's implicit
+synchronisation.  Its scratch is a fixed 16 MiB array inside the library.
+These tests call it through the C ABI, twice in a row with different
+witnesses, and require exactly the residues that the ordinary
+lc_ajtai_commit returns for the same key and input (Goldilocks and Q_32
+keys, a key view, a key made for the tensor engine); a request larger than
+the fixed scratch must be refused without running.
 
 This file is collected last on purpose, so that a run that stops at the first
 failure has already run every other test; it also passes alone in a fresh
@@ -70,6 +71,21 @@ def test_q32_noalloc_matches_commit_twice():
         s = synth.synth_mod32(70 + call, 1, Modulus32.Q_32.q, 3 * 16 * 256).reshape(3, 16, 256)
         got, want = _both(pk._dev.handle, _dev(s), 3, 2, 256, np.uint32)
         assert np.array_equal(got, want), f"call {call}"
+
+
+def test_noalloc_on_a_key_view_and_a_tensor_engine_key():
+    """A view (its rows of A are a_m = 300 apart while it commits m = 200) and
+    a key created for the tensor engine both give lc_ajtai_commit's residues."""
+    from lzx_b200.batch import key_view
+    d = 64
+    A = synth.synth_gl(21, 0, 16 * 300 * d).reshape(16, 300, d)
+    parent = GoldilocksAjtaiKey(6, 16, 300, A, tensor_cores=True)
+    view = key_view(parent, 8, 200)
+    for handle, k, m in ((parent.handle, 16, 300), (view.handle, 8, 200)):
+        for call in range(2):
+            W = synth.synth_gl(22 + call, m, 3 * m * d).reshape(3, m, d)
+            got, want = _both(handle, _dev(W), 3, k, d, np.uint64)
+            assert np.array_equal(got, want), (k, m, call)
 
 
 def test_noalloc_refuses_requests_beyond_its_scratch():
