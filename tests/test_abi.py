@@ -84,6 +84,21 @@ def test_integration_binding_declares_every_entry_point():
     assert not missing, missing
 
 
+def test_rust_hooks_call_only_header_entry_points():
+    """The hook code for the two hot-path crates (NttTables dispatch,
+    AjtaiPublicKey::commit / commit_batch) calls only functions the header
+    declares, and the hooks cover the reference methods they replace."""
+    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    blocks = re.findall(r"```rust\n(.*?)\n```", doc, re.S)
+    called = {f for b in blocks for f in re.findall(r"ffi::(lc_\w+)\(", b)}
+    declared = set(_lib.declared_functions())
+    assert called and not (called - declared), sorted(called - declared)
+    code = "\n".join(blocks)
+    for hook in ("fn with_gpu", "fn forward_fast", "fn inverse_fast", "fn forward_batch", "fn inverse_batch",
+                 "fn from_seed_gpu", "fn commit(", "fn commit_batch", "AjtaiError::DimensionMismatch"):
+        assert hook in code, hook
+
+
 def test_null_handles_are_rejected():
     """Every entry point that takes a plan, key, batch, pipeline or output
     pointer rejects null with LC_ERR_INVALID_ARGUMENT (the getters with -1)
