@@ -638,9 +638,33 @@ def bench_uneven(args, rank, max_over_ranks, barrier, world):
     batch.check()
     ms = max_over_ranks(a.elapsed_time(b) / K)
     exact = bool(torch.equal(OG, ref_g) and torch.equal(OU, ref_u))
+    # the same batch with its products on the CUDA cores (160-/64-bit multiply-accumulates),
+    # tuned for that form
+    batch.products = CommitBatch.PRODUCTS_INT64
+    best_i64, _ = tune.tune_batch(batch)
+    batch.run()
+    torch.cuda.synchronize()
+    barrier()
+    a.record()
+    for _ in range(K):
+        batch.run()
+    b.record()
+    torch.cuda.synchronize()
+    batch.check()
+    ms_i64 = max_over_ranks(a.elapsed_time(b) / K)
+    exact = exact and bool(torch.equal(OG, ref_g) and torch.equal(OU, ref_u))
+    batch.products = CommitBatch.PRODUCTS_TENSOR
+    batch.set_config(*best)
+    batch.run()
+    torch.cuda.synchronize()
     res["batch"] = {"ms": ms, "value": world * total_elems / (ms / 1e3), "steps": K,
+                    "products": "tensor cores (byte-limb GEMMs)",
                     "config": {"chunk": best[0], "ctas_per_sm": best[1], "claim": best[2]},
                     "tuning_ms": timings, "items": batch.info, "bit_exact_vs_one_by_one": exact}
+    res["batch_int64_products"] = {"ms": ms_i64, "value": world * total_elems / (ms_i64 / 1e3),
+                                   "products": "CUDA cores (160-/64-bit multiply-accumulates)",
+                                   "config": {"chunk": best_i64[0], "ctas_per_sm": best_i64[1],
+                                              "claim": best_i64[2]}}
     res["speedup_batch_vs_one_by_one"] = obo_ms / ms
     # ---- end to end: witnesses in from pinned host memory, commitments out
     hw = torch.empty(wtot, dtype=torch.int8).pin_memory()
@@ -1262,6 +1286,7 @@ def compact_uneven(u):
     e = b.get("e2e") or {}
     return {"jobs": u.get("jobs"), "sum_n": u.get("sum_n"), "unit": "committed ring-elems/s",
             "batch_ms": _sig(b.get("ms")), "v": _sig(b.get("value")),
+            "int64_products_ms": _sig(_get(u, "batch_int64_products", "ms")),
             "one_by_one_ms": _sig(_get(u, "one_by_one", "ms")),
             "speedup": _sig(u.get("speedup_batch_vs_one_by_one"), 3),
             "bit_exact": b.get("bit_exact_vs_one_by_one"),

@@ -372,10 +372,11 @@ typedef struct lc_commit_job {
 typedef struct lc_batch lc_batch;
 
 /* Plan a batch: jobs of one key are grouped into lanes of at most 128 jobs
- * sorted by n, so the key's cached NTT(A) is read once per lane, not once
- * per job.  Three persistent kernels, each fed by a device work counter, run
- * it: the witness NTTs, the products (one work item per NTT slot and chunk
- * of ring elements), and per job the sum over chunks plus the inverse NTT.
+ * sorted by n, so the key's cached NTT(A) is read once per block of jobs of a
+ * lane, not once per job.  Three launches run it: the witness NTTs
+ * (persistent, fed by a device work counter), the products (see
+ * lc_batch_set_products), and per job the sum over chunks plus the inverse
+ * NTT.
  * flags: LC_BATCH_GRAPH captures the three launches into a CUDA graph on
  * the second run and replays it afterwards.  The keys must outlive the batch;
  * runs of one batch must not overlap on the GPU. */
@@ -387,6 +388,19 @@ LC_API int lc_batch_create(const lc_commit_class *classes, uint32_t num_classes,
  * claimed per counter increment (1..16).  Results do not depend on them. */
 LC_API int lc_batch_set_config(lc_batch *batch, uint32_t chunk, uint32_t ctas_per_sm, uint32_t claim);
 LC_API int lc_batch_get_config(const lc_batch *batch, uint32_t *chunk, uint32_t *ctas_per_sm, uint32_t *claim);
+/* How the products run (the same per-slot sums as the keys' commits,
+ * ajtai.rs:139-148): LC_PRODUCTS_TENSOR (the default wherever it can run) as
+ * exact byte-limb GEMMs on the INT8 tensor cores -- one work item per lane,
+ * NTT slot, block of 32 jobs and chunk of at most 32768 ring elements, the
+ * staircase of transformed witnesses gathered with its inactive jobs as
+ * zeros -- or LC_PRODUCTS_INT64 with 160-bit / 64-bit multiply-accumulates on
+ * the CUDA cores (one item per slot, chunk and 16-job block; `chunk` of
+ * lc_batch_set_config applies to this form only).  Identical results.
+ * lc_batch_set_products returns LC_ERR_UNSUPPORTED when the tensor form
+ * cannot run (no tensor-map encoder in the driver); lc_batch_get_products
+ * returns the mode (-1 for a null batch). */
+LC_API int lc_batch_set_products(lc_batch *batch, int mode);
+LC_API int lc_batch_get_products(const lc_batch *batch);
 /* Work items of the three launches, and the lanes of the plan. */
 LC_API int lc_batch_info(const lc_batch *batch, uint64_t *items_ntt, uint64_t *items_product,
                          uint64_t *items_finish, uint32_t *lanes);

@@ -111,6 +111,8 @@ def _declare(L):
         "lc_batch_create": (i32, [P, u32, P, u32, u32, C.POINTER(P)]),
         "lc_batch_set_config": (i32, [P, u32, u32, u32]),
         "lc_batch_get_config": (i32, [P, U32P, U32P, U32P]),
+        "lc_batch_set_products": (i32, [P, i32]),
+        "lc_batch_get_products": (i32, [P]),
         "lc_batch_info": (i32, [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), U32P]),
         "lc_batch_run": (i32, [P, P]),
         "lc_batch_check": (i32, [P, P]),

@@ -119,6 +119,18 @@ class CommitBatch:
         _lib.check(_lib.lib().lc_batch_get_config(self._h, C.byref(a), C.byref(b), C.byref(c)), "lc_batch_get_config")
         return a.value, b.value, c.value
 
+    PRODUCTS_INT64 = 0   # LC_PRODUCTS_INT64: multiply-accumulates on the CUDA cores
+    PRODUCTS_TENSOR = 1  # LC_PRODUCTS_TENSOR: byte-limb GEMMs on the INT8 tensor cores
+
+    @property
+    def products(self) -> int:
+        """How the per-slot products run (``lc_batch_set_products``); identical results."""
+        return _lib.lib().lc_batch_get_products(self._h)
+
+    @products.setter
+    def products(self, mode: int):
+        _lib.check(_lib.lib().lc_batch_set_products(self._h, mode), "lc_batch_set_products")
+
     @property
     def info(self):
         a, b, c, d = C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_uint32()

@@ -32,11 +32,16 @@
 #include "internal.h"
 #include "mac.cuh"
 #include "ntt_kernels.cuh"
+#include "tcgen05.cuh"
 
 namespace lc {
 
 constexpr int kBatchThreads = 256;
 constexpr uint32_t kLaneJobs = 128;
+// tensor-core products: jobs per block (MMA N = 32 limbs-bytes per job) and
+// ring elements per exact int32 sum (32768 * 255^2 < 2^31)
+constexpr int kTpJobs = 32;
+constexpr uint32_t kTpChunk = 32768;
 constexpr uint32_t kMinChunk = 1024;
 
 // Slot strides (odd, >= N + T) that keep the transposed reads of the
@@ -77,6 +82,8 @@ struct LaneDesc {
   const uint64_t* citem;   // [nchunks + 1]: first product item of each chunk (lane-relative)
   const uint8_t* cblk;     // [nchunks]: 16-job blocks with jobs active at the chunk's start
   uint64_t item0[3];       // first item of the lane in each launch
+  int32_t* tpart;          // tensor-core products: limb-pair sums of the lane (null: CUDA-core partials)
+  const uint32_t* tchunk0; // [blocks + 1]: first K chunk of each 32-job block in tpart
 };
 
 struct SubJob {
@@ -334,12 +341,57 @@ LC_D void finish_item(const LaneDesc& L, const SubJob* __restrict__ subs, uint32
   const uint32_t nch = (J.n + chunk - 1) / chunk;
   for (int i = tid; i < Geo<LOG_N, LOG_V>::inv_entries(); i += kBatchThreads)
     tw[i] = reinterpret_cast<const Tw*>(L.tw_inv)[i];
-  const T* P = reinterpret_cast<const T*>(L.partial);
-  for (uint32_t e = tid; e < J.kappa * N; e += kBatchThreads) {
-    const uint32_t i = e / N, tt = e % N;
-    T s = 0;
-    for (uint32_t c = 0; c < nch; ++c) s = add_mod(s, P[(((size_t)c * N + tt) * kIPad + i) * L.nb + b], L.q);
-    slots[i * SS + tt] = s;
+  if (L.tpart) {
+    // tensor-core partials: D[(b, lw)][(i, la)] per (chunk, slot) of the
+    // job's 32-job block; the 2L - 1 sums of equal la + lw over the chunks
+    // fit 64 bits (< 2^31 * L * chunks) and are folded with 2^(8k) mod q.
+    // Consecutive threads take consecutive rows i, i.e. adjacent words.
+    constexpr int LL = sizeof(T);
+    const uint32_t blk = (uint32_t)b / kTpJobs, bl = (uint32_t)b % kTpJobs;
+    const uint32_t c0 = L.tchunk0[blk], nchk = L.tchunk0[blk + 1] - c0;
+    const size_t tile = (size_t)kTpJobs * LL * 128;
+    for (uint32_t e = tid; e < J.kappa * N; e += kBatchThreads) {
+      const uint32_t i = e % J.kappa, tt = e / J.kappa;
+      uint64_t tk[2 * LL - 1];
+#pragma unroll
+      for (int k = 0; k < 2 * LL - 1; ++k) tk[k] = 0;
+      for (uint32_t c = 0; c < nchk; ++c) {
+        const int32_t* D = L.tpart + ((size_t)(c0 + c) * N + tt) * tile + (size_t)bl * LL * 128 + i * LL;
+#pragma unroll
+        for (int lw = 0; lw < LL; ++lw)
+#pragma unroll
+          for (int la = 0; la < LL; ++la) tk[la + lw] += (uint32_t)__ldg(D + (size_t)lw * 128 + la);
+      }
+      T res;
+      if constexpr (LL == 8) {
+        unsigned __int128 v = 0;
+        uint64_t cw = 1;  // 2^(8k) mod p
+#pragma unroll
+        for (int k = 0; k < 2 * LL - 1; ++k) {
+          v += (unsigned __int128)tk[k] * cw;
+          cw = gl_mul(cw, 256);
+        }
+        res = (T)gl_canon(gl_reduce128_lazy((uint64_t)(v >> 64), (uint64_t)v));
+      } else {
+        const uint64_t q = L.q;
+        uint64_t v = 0, cw = 1 % q;  // 2^(8k) mod q
+#pragma unroll
+        for (int k = 0; k < 2 * LL - 1; ++k) {
+          v = (v + (tk[k] % q) * cw % q) % q;
+          cw = (cw << 8) % q;
+        }
+        res = (T)v;
+      }
+      slots[i * SS + tt] = res;
+    }
+  } else {
+    const T* P = reinterpret_cast<const T*>(L.partial);
+    for (uint32_t e = tid; e < J.kappa * N; e += kBatchThreads) {
+      const uint32_t i = e / N, tt = e % N;
+      T s = 0;
+      for (uint32_t c = 0; c < nch; ++c) s = add_mod(s, P[(((size_t)c * N + tt) * kIPad + i) * L.nb + b], L.q);
+      slots[i * SS + tt] = s;
+    }
   }
   __syncthreads();
   const A ar = make_arith_q<A>(L.q, L.qinv);
@@ -429,6 +481,241 @@ __global__ void __launch_bounds__(kBatchThreads, sizeof(E) == 8 ? 2 : 3)
   }
 }
 
+// ---- launch 2 on the tensor cores: lane products as exact byte-limb GEMMs
+//
+// C_t[i][b] = sum_j Ahat[t][j][i] * What[t][j][b] over j < n_b, with both
+// residues split into L byte limbs (L = 8 Goldilocks, 4 for u32 moduli):
+// C_t = sum_{la,lw} 2^(8 (la + lw)) D_t and
+//   D_t[(i,la)][(b,lw)] = sum_j Ahat_la[t][j][i] * What_lw[t][j][b]   (u8 x u8 -> s32),
+// exact for at most 32768 ring elements j per sum (32768 * 255^2 < 2^31).
+// An item is (lane, slot t, block of 32 jobs, chunk of 32768 ring elements):
+// M = 128 (the key row's 16 x L bytes (i, la); u32 keys fill half and the
+// second A atom is a zero tile), N = 32 L bytes (b, lw), K = the chunk.  The
+// key rows Ahat[t][j][16] arrive by TMA (a 3-D map per lane: row bytes,
+// j < a_m, slot); the witness rows come from the staircase, where row j of
+// the block is the 32 L contiguous bytes at what[t S + R[j] + 32 blk] of
+// which only the first cnt(j) - 32 blk jobs are active: four gather warps
+// copy them with zero-filling cp.async straight into the 128-byte-swizzled
+// MN-major layout the MMA descriptor reads (chunk c of row r at c ^ (r & 7)),
+// so the shorter jobs of a block contribute zeros and nothing outside the
+// staircase is read.  The epilogue (the same four warps) writes D, one
+// [32 L columns][128 rows] int32 tile per item; the finish launch folds the
+// limb pairs over the block's chunks.
+constexpr int kTpRows = 64;            // ring elements per stage
+constexpr int kTpStages = 4;
+constexpr int kTpLag = 2;              // gather stages in flight before a stage is handed to the MMA
+constexpr int kTpThreads = 192;        // warp 0 TMA, 1 MMA + TMEM, 2..5 gather + epilogue
+
+struct TpItem {
+  uint32_t lane, t, blk, chunk;
+};
+
+template <int EB>
+struct TpCfg {
+  static constexpr int NB = kTpJobs * EB;        // B row bytes = MMA N (256 or 128)
+  static constexpr int AW = 16 * EB;             // key row bytes (128 or 64)
+  static constexpr int A_LOAD = kTpRows * AW;    // bytes the TMA writes per stage
+  static constexpr int A_BYTES = kTpRows * 128;  // A region (for AW = 64 the zero atom follows)
+  static constexpr int B_ATOM = kTpRows * 128;   // one 128-byte swizzle atom along N, all K rows
+  static constexpr int ATOMS = NB / 128;
+  static constexpr int STAGE = A_BYTES + ATOMS * B_ATOM;
+  static constexpr size_t SMEM = 1024 + (size_t)kTpStages * STAGE + 128;
+  static constexpr uint32_t A_LAYOUT = AW == 128 ? 2u : 4u;  // 128- or 64-byte swizzle
+  static_assert(STAGE % 1024 == 0, "swizzle atoms stay aligned");
+  static_assert(SMEM <= 227 * 1024, "shared memory");
+};
+
+// D = s32, A = B = u8, both MN-major, N, M = 128
+template <int N>
+struct TpIdesc {
+  static constexpr uint32_t value =
+      (2u << 4) | (1u << 15) | (1u << 16) | ((uint32_t)(N >> 3) << 17) | ((128u >> 4) << 24);
+};
+
+template <int EB>
+LC_D void cp_async_zfill(uint32_t dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(dst), "l"(src), "n"(EB), "r"(bytes)
+               : "memory");
+}
+LC_D void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+LC_D void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <int EB>
+__global__ void __launch_bounds__(kTpThreads, 1)
+    lane_products_tc_kernel(const TpItem* __restrict__ items, const LaneDesc* __restrict__ lanes,
+                            const SubJob* __restrict__ subs, const CUtensorMap* __restrict__ amaps, uint32_t* err) {
+  using C = TpCfg<EB>;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char* base =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + kTpStages * C::STAGE);
+  uint64_t* full = bars;                  // [4] key rows landed (tx) and 128 gather threads arrived
+  uint64_t* empty = bars + kTpStages;     // [4] the stage's MMAs finished
+  uint64_t* done = bars + 2 * kTpStages;  // every MMA finished
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kTpStages + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 2 * kTpStages + 2);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const TpItem it = items[blockIdx.x];
+  const LaneDesc& L = lanes[it.lane];
+  const uint32_t d = 1u << L.log_n;
+  const uint32_t nblk = subs[L.sub0 + kTpJobs * it.blk].n;  // the block's longest job
+  const uint32_t j0 = it.chunk * kTpChunk;
+  const uint32_t j1 = min(nblk, j0 + kTpChunk);
+  const int nst = (int)((j1 - j0 + kTpRows - 1) / kTpRows);
+
+  if (tid == 0) {
+    for (int s = 0; s < kTpStages; ++s) {
+      mbar_init(&full[s], 1 + 128);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if constexpr (C::AW == 64) {
+    // the second A atom of every stage: rows (i, la) 64..127 are zero
+    for (int s = 0; s < kTpStages; ++s) {
+      uint4* z = reinterpret_cast<uint4*>(base + s * C::STAGE + C::A_LOAD);
+      for (int e = tid; e < (C::A_BYTES - C::A_LOAD) / 16; e += kTpThreads) z[e] = make_uint4(0, 0, 0, 0);
+    }
+    fence_proxy_async_smem();
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(C::NB));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  auto stage = [&](int s) { return base + (s % kTpStages) * C::STAGE; };
+  auto fail = [&]() {
+    record_error(err, LC_DEVERR_TIMEOUT);
+    *abort_flag = 1;
+  };
+  int last_loaded = -1, last_mma = -1;
+
+  if (warp == 0) {
+    // ---------------- TMA: key rows (i, la) of slot t
+    if (lane == 0) {
+      const CUtensorMap* amap = amaps + it.lane;
+      for (int s = 0; s < nst && !*abort_flag; ++s) {
+        if (s >= kTpStages && !mbar_wait(&empty[s % kTpStages], (uint32_t)(((s - kTpStages) / kTpStages) & 1))) {
+          fail();
+          break;
+        }
+        mbar_arrive_expect_tx(&full[s % kTpStages], (uint32_t)C::A_LOAD);
+        tma_load_3d(stage(s), amap, 0, (int)(j0 + kTpRows * s), (int)it.t, &full[s % kTpStages]);
+        last_loaded = s;
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer
+    if (lane == 0) {
+      for (int s = 0; s < nst && !*abort_flag; ++s) {
+        if (!mbar_wait(&full[s % kTpStages], (uint32_t)((s / kTpStages) & 1))) {
+          fail();
+          break;
+        }
+        tc_fence_after();
+        const uint32_t sa = smem_u32(stage(s)), sb = sa + C::A_BYTES;
+#pragma unroll
+        for (int ks = 0; ks < kTpRows / 32; ++ks) {
+          const uint64_t ad = umma_desc_mn(sa + ks * 32 * C::AW, C::A_LOAD, 8 * C::AW, C::A_LAYOUT);
+          const uint64_t bd = umma_desc_mn(sb + ks * 32 * 128, C::B_ATOM, 8 * 128, 2);
+          mma_i8(tmem, ad, bd, TpIdesc<C::NB>::value, (s > 0 || ks > 0) ? 1u : 0u);
+        }
+        mma_commit(&empty[s % kTpStages]);
+        last_mma = s;
+      }
+      if (last_mma >= 0) mma_commit(done);
+    }
+  } else {
+    // ---------------- gather: warp g = warp - 2 fills rows 16 g .. 16 g + 15 of
+    // every stage, lane l the entry of job 32 blk + l (EB bytes)
+    const int g = warp - 2;
+    using E = typename std::conditional<EB == 8, uint64_t, uint32_t>::type;
+    const E* W = reinterpret_cast<const E*>(L.what) + (size_t)it.t * L.S + (size_t)kTpJobs * it.blk + lane;
+    const uint32_t bx = (uint32_t)lane * EB;  // byte of the entry in the N row
+    const uint32_t boff = (bx >> 7) * C::B_ATOM + (bx & 15);
+    const uint32_t bchunk = (bx & 127) >> 4;
+    const uint32_t act0 = kTpJobs * it.blk;   // jobs before the block
+    int issued = 0;
+    bool ok = true;
+    for (int s = 0; s < nst; ++s) {
+      if (*abort_flag) {
+        ok = false;
+        break;
+      }
+      if (s >= kTpStages && !mbar_wait(&empty[s % kTpStages], (uint32_t)(((s - kTpStages) / kTpStages) & 1))) {
+        fail();
+        ok = false;
+        break;
+      }
+      const uint32_t jb = j0 + kTpRows * s + 16 * g;
+      // R[jb .. jb + 16]: the rows' staircase offsets and job counts
+      const uint64_t rl = (lane <= 16 && jb + lane <= L.n_max) ? __ldg(L.R + jb + lane) : 0;
+      const uint32_t sb = smem_u32(stage(s)) + C::A_BYTES + boff;
+#pragma unroll 4
+      for (int r = 0; r < 16; ++r) {
+        const uint64_t r0 = __shfl_sync(0xffffffffu, rl, r);
+        const uint64_t r1 = __shfl_sync(0xffffffffu, rl, r + 1);
+        const uint32_t j = jb + r, row = 16 * g + r;
+        const uint32_t cnt = (uint32_t)(r1 - r0);
+        const bool live = j < j1 && cnt > act0 + (uint32_t)lane;
+        const uint32_t dst = sb + row * 128 + ((bchunk ^ (row & 7)) << 4);
+        cp_async_zfill<EB>(dst, live ? (const void*)(W + r0) : L.what, live ? EB : 0);
+      }
+      cp_async_commit();
+      ++issued;
+      if (s >= kTpLag) {
+        cp_async_wait<kTpLag>();
+        fence_proxy_async_smem();
+        mbar_arrive(&full[(s - kTpLag) % kTpStages]);
+      }
+    }
+    cp_async_wait<0>();
+    fence_proxy_async_smem();
+    if (ok)
+      for (int s = max(0, nst - kTpLag); s < nst; ++s) mbar_arrive(&full[s % kTpStages]);
+    (void)issued;
+    // ---------------- epilogue: lane = row (i, la); column = (b, lw)
+    const bool fin = ok && nst > 0 && !*abort_flag && mbar_wait(done, 0);
+    if (__all_sync(0xffffffffu, fin)) {
+      tc_fence_after();
+      const uint32_t lq = warp & 3, row = 32 * lq + lane;
+      int32_t* out = L.tpart + ((size_t)(L.tchunk0[it.blk] + it.chunk) * d + it.t) * (size_t)C::NB * 128;
+#pragma unroll 1
+      for (int c0 = 0; c0 < C::NB; c0 += 16) {
+        uint32_t v[16];
+        tmem_ld16(tmem + ((32 * lq) << 16) + c0, v);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int u = 0; u < 16; ++u) out[(size_t)(c0 + u) * 128 + row] = (int32_t)v[u];
+      }
+    } else if (nst > 0 && lane == 0) {
+      fail();
+    }
+  }
+  // ---------------- nothing in flight when TMEM and shared memory go
+  __syncthreads();
+  if (warp == 0 && lane == 0) {
+    for (int s = max(0, last_loaded - (kTpStages - 1)); s <= last_loaded; ++s)
+      mbar_wait(&full[s % kTpStages], (uint32_t)((s / kTpStages) & 1));
+  }
+  if (warp == 1 && lane == 0 && last_mma >= 0) mbar_wait(done, 0);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(C::NB));
+  }
+}
+
 template <class A, int LOG_N, int LOG_V>
 static void smem_need(size_t& s1, size_t& s3, uint32_t& pb) {
   using C = BCfg<A, LOG_N, LOG_V>;
@@ -480,6 +767,18 @@ struct lc_batch {
   size_t smem[3] = {0, 0, 0};
   uint32_t chunk = 4096, ctas = 2, claim = 1;
   uint32_t flags = 0;
+  // tensor-core products (lane_products_tc_kernel)
+  int products = LC_PRODUCTS_INT64;
+  bool tensor_ok = false;
+  std::vector<uint32_t> h_nfirst;        // per lane: n of each 32-job block's first job, concatenated
+  std::vector<size_t> nfirst_off;
+  int32_t* d_tpart = nullptr;
+  uint32_t* d_tchunk0 = nullptr;
+  CUtensorMap* d_amaps = nullptr;
+  lc::TpItem* d_titems = nullptr;
+  uint64_t titems[2] = {0, 0};           // Goldilocks items, then u32 items
+  std::vector<int32_t*> lane_tpart;
+  std::vector<const uint32_t*> lane_tchunk0;
   bool warmed = false, dirty = true;
   cudaStream_t cap = nullptr;
   cudaGraph_t graph = nullptr;
@@ -494,9 +793,88 @@ static void batch_free(lc_batch* b) {
   if (b->cap) cudaStreamDestroy(b->cap);
   for (void* p : {(void*)b->d_lanes, (void*)b->d_subs, (void*)b->d_R, (void*)b->d_itemj, (void*)b->d_what,
                   (void*)b->d_partial, (void*)b->d_counters, (void*)b->d_err, (void*)b->d_citem,
-                  (void*)b->d_cblk})
+                  (void*)b->d_cblk, (void*)b->d_tpart, (void*)b->d_tchunk0, (void*)b->d_amaps,
+                  (void*)b->d_titems})
     if (p) cudaFree(p);
   delete b;
+}
+
+// Tensor-core products: per lane a TMA map of its key rows, per 32-job block
+// the K chunks, the items (longest first, Goldilocks lanes then u32 lanes)
+// and the partial tiles.  Leaves tensor_ok false when a lane cannot run
+// there (no tensor-map encoder, or an element width other than 8 / 4 bytes).
+static int batch_tensor_setup(lc_batch* b) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc || b->lanes.empty()) return LC_OK;
+  const size_t nl = b->lanes.size();
+  std::vector<CUtensorMap> maps(nl);
+  std::vector<uint32_t> tchunk0;
+  std::vector<size_t> tc_off(nl), part_off(nl);
+  std::vector<std::pair<uint32_t, TpItem>> items[2];  // (rows, item)
+  size_t part_elems = 0;
+  for (size_t l = 0; l < nl; ++l) {
+    const LaneDesc& L = b->lanes[l];
+    const uint32_t eb = L.kind == (uint32_t)PlanKind::Goldilocks ? 8 : 4;
+    const uint32_t d = 1u << L.log_n, aw = 16 * eb;
+    const cuuint64_t dims[3] = {aw, (cuuint64_t)L.a_m, (cuuint64_t)d};
+    const cuuint64_t strides[2] = {aw, (cuuint64_t)L.a_m * aw};
+    const cuuint32_t box[3] = {aw, (cuuint32_t)kTpRows, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    if (enc(&maps[l], CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(L.ahat), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, aw == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return LC_OK;
+    tc_off[l] = tchunk0.size();
+    part_off[l] = part_elems;
+    const uint32_t nblk = (L.nb + kTpJobs - 1) / kTpJobs;
+    uint32_t acc = 0;
+    for (uint32_t blk = 0; blk < nblk; ++blk) {
+      const uint32_t nfirst = b->h_nfirst[b->nfirst_off[l] + blk];
+      const uint32_t chunks = (nfirst + kTpChunk - 1) / kTpChunk;
+      tchunk0.push_back(acc);
+      for (uint32_t c = 0; c < chunks; ++c) {
+        const uint32_t rows = std::min(nfirst, (c + 1) * kTpChunk) - c * kTpChunk;
+        for (uint32_t t = 0; t < d; ++t) items[eb == 8 ? 0 : 1].push_back({rows, TpItem{(uint32_t)l, t, blk, c}});
+      }
+      acc += chunks;
+    }
+    tchunk0.push_back(acc);
+    part_elems += (size_t)acc * d * kTpJobs * eb * 128;
+  }
+  for (auto& v : items)
+    std::stable_sort(v.begin(), v.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+  std::vector<TpItem> flat;
+  for (auto& v : items)
+    for (auto& x : v) flat.push_back(x.second);
+  if (cudaMalloc(&b->d_amaps, nl * sizeof(CUtensorMap)) != cudaSuccess ||
+      cudaMalloc(&b->d_tchunk0, tchunk0.size() * 4) != cudaSuccess ||
+      cudaMalloc(&b->d_titems, std::max<size_t>(1, flat.size()) * sizeof(TpItem)) != cudaSuccess ||
+      cudaMalloc(&b->d_tpart, std::max<size_t>(256, part_elems * 4)) != cudaSuccess) {
+    cudaGetLastError();
+    return LC_ERR_OUT_OF_MEMORY;
+  }
+  cudaMemcpy(b->d_amaps, maps.data(), nl * sizeof(CUtensorMap), cudaMemcpyHostToDevice);
+  cudaMemcpy(b->d_tchunk0, tchunk0.data(), tchunk0.size() * 4, cudaMemcpyHostToDevice);
+  if (!flat.empty()) cudaMemcpy(b->d_titems, flat.data(), flat.size() * sizeof(TpItem), cudaMemcpyHostToDevice);
+  b->titems[0] = items[0].size();
+  b->titems[1] = items[1].size();
+  b->lane_tpart.resize(nl);
+  b->lane_tchunk0.resize(nl);
+  for (size_t l = 0; l < nl; ++l) {
+    b->lane_tpart[l] = b->d_tpart + part_off[l];
+    b->lane_tchunk0[l] = b->d_tchunk0 + tc_off[l];
+  }
+  b->tensor_ok = true;
+  return map_cuda(cudaGetLastError());
+}
+
+// The lanes' partial pointers for the current product mode.
+static void batch_apply_products(lc_batch* b) {
+  for (size_t l = 0; l < b->lanes.size(); ++l) {
+    const bool tc = b->products == LC_PRODUCTS_TENSOR && b->tensor_ok;
+    b->lanes[l].tpart = tc ? b->lane_tpart[l] : nullptr;
+    b->lanes[l].tchunk0 = tc ? b->lane_tchunk0[l] : nullptr;
+  }
 }
 
 // chunk-dependent fields, item bases and the device copy of the lanes
@@ -583,8 +961,22 @@ static int batch_launch(lc_batch* b, cudaStream_t st) {
     if (e != cudaSuccess) return map_cuda(e);
   }
   batch_kernel<0><<<grid, kBatchThreads, b->smem[0], st>>>(p);
-  product_kernel<uint64_t><<<grid, kBatchThreads, 0, st>>>(p);
-  product_kernel<uint32_t><<<grid, kBatchThreads, 0, st>>>(p);
+  if (b->products == LC_PRODUCTS_TENSOR && b->tensor_ok) {
+    static std::atomic<uint64_t> attr8{0}, attr4{0};
+    e = smem_attr_once(attr8, lane_products_tc_kernel<8>, TpCfg<8>::SMEM);
+    if (e == cudaSuccess) e = smem_attr_once(attr4, lane_products_tc_kernel<4>, TpCfg<4>::SMEM);
+    if (e != cudaSuccess) return map_cuda(e);
+    // one CTA per item; grids above 2^31 - 1 items are refused at creation
+    if (b->titems[0])
+      lane_products_tc_kernel<8><<<(unsigned)b->titems[0], kTpThreads, TpCfg<8>::SMEM, st>>>(
+          b->d_titems, b->d_lanes, b->d_subs, b->d_amaps, b->d_err);
+    if (b->titems[1])
+      lane_products_tc_kernel<4><<<(unsigned)b->titems[1], kTpThreads, TpCfg<4>::SMEM, st>>>(
+          b->d_titems + b->titems[0], b->d_lanes, b->d_subs, b->d_amaps, b->d_err);
+  } else {
+    product_kernel<uint64_t><<<grid, kBatchThreads, 0, st>>>(p);
+    product_kernel<uint32_t><<<grid, kBatchThreads, 0, st>>>(p);
+  }
   batch_kernel<2><<<grid, kBatchThreads, b->smem[2], st>>>(p);
   return map_cuda(cudaGetLastError());
 }
@@ -671,6 +1063,8 @@ LC_API int lc_batch_create(const lc_commit_class* classes, uint32_t num_classes,
           subs.push_back(sj);
         }
         L.n_max = jobs[idx[g0]].n;
+        b->nfirst_off.push_back(b->h_nfirst.size());
+        for (size_t g = g0; g < g1; g += kTpJobs) b->h_nfirst.push_back(jobs[idx[g]].n);
         // staircase offsets R[j] and the witness items' first ring elements
         r_off.push_back(Rall.size());
         std::vector<uint64_t> R(L.n_max + 1);
@@ -727,7 +1121,16 @@ LC_API int lc_batch_create(const lc_commit_class* classes, uint32_t num_classes,
     L.what = b->d_what + what_off[l];
     L.partial = b->d_partial + part_off[l];
   }
-  const int rc = batch_layout(b);
+  // products on the tensor cores by default, where every lane can run there
+  int rc = batch_tensor_setup(b);
+  if (rc) {
+    batch_free(b);
+    return rc;
+  }
+  if (b->titems[0] > 0x7FFFFFFFull || b->titems[1] > 0x7FFFFFFFull) b->tensor_ok = false;
+  b->products = b->tensor_ok ? LC_PRODUCTS_TENSOR : LC_PRODUCTS_INT64;
+  batch_apply_products(b);
+  rc = batch_layout(b);
   if (rc) {
     batch_free(b);
     return rc;
@@ -747,6 +1150,17 @@ LC_API int lc_batch_set_config(lc_batch* b, uint32_t chunk, uint32_t ctas_per_sm
   return batch_layout(b);
 }
 
+LC_API int lc_batch_set_products(lc_batch* b, int mode) {
+  using namespace lc;
+  if (!b || (mode != LC_PRODUCTS_TENSOR && mode != LC_PRODUCTS_INT64)) return LC_ERR_INVALID_ARGUMENT;
+  if (mode == LC_PRODUCTS_TENSOR && !b->tensor_ok) return LC_ERR_UNSUPPORTED;
+  b->products = mode;
+  batch_apply_products(b);
+  return batch_layout(b);
+}
+
+LC_API int lc_batch_get_products(const lc_batch* b) { return b ? b->products : -1; }
+
 LC_API int lc_batch_get_config(const lc_batch* b, uint32_t* chunk, uint32_t* ctas_per_sm, uint32_t* claim) {
   if (!b) return LC_ERR_INVALID_ARGUMENT;
   if (chunk) *chunk = b->chunk;
@@ -759,7 +1173,8 @@ LC_API int lc_batch_info(const lc_batch* b, uint64_t* items_ntt, uint64_t* items
                          uint32_t* lanes) {
   if (!b) return LC_ERR_INVALID_ARGUMENT;
   if (items_ntt) *items_ntt = b->total[0];
-  if (items_product) *items_product = b->total[1];
+  if (items_product)
+    *items_product = b->products == LC_PRODUCTS_TENSOR && b->tensor_ok ? b->titems[0] + b->titems[1] : b->total[1];
   if (items_finish) *items_finish = b->total[2];
   if (lanes) *lanes = (uint32_t)b->lanes.size();
   return LC_OK;

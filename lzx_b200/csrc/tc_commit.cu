@@ -49,6 +49,7 @@
 #include "arith.cuh"
 #include "common.cuh"
 #include "internal.h"
+#include "tcgen05.cuh"
 
 namespace lc {
 
@@ -81,68 +82,12 @@ static_assert(kTcSmem <= 227 * 1024, "shared memory");
 
 // ------------------------------------------------------------------ device helpers
 
-// K-major operand, 128-byte swizzle: 8-row groups of 1024 bytes (SBO), start
-// address advanced by 32 bytes per K step inside the swizzle atom.
-LC_D uint64_t umma_desc_sw128(uint32_t saddr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFF);  // start address
-  d |= (uint64_t)1 << 16;                   // leading byte offset (unused here)
-  d |= (uint64_t)(1024 >> 4) << 32;         // stride byte offset
-  d |= (uint64_t)1 << 46;                   // descriptor version
-  d |= (uint64_t)2 << 61;                   // layout: 128-byte swizzle
-  return d;
-}
-
-// K-major operand without swizzle: 8-row x 16-byte core matrices, `lbo`
-// bytes to the next one along K, `sbo` bytes to the next 8-row group.
-LC_D uint64_t umma_desc_noswz(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
-  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
-  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
-  d |= (uint64_t)1 << 46;  // descriptor version; layout 0: no swizzle
-  return d;
-}
-
 // D = s32 (4), A = s8 or u8 (7), B = u8 (10), both K-major, N = 256 (17), M = 128 (24)
 template <bool S8>
 struct TcIdesc {
   static constexpr uint32_t value =
       (2u << 4) | ((S8 ? 1u : 0u) << 7) | (0u << 10) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
 };
-
-LC_D void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-          smem_u32(dst)),
-      "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
-      : "memory");
-}
-
-LC_D void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
-}
-
-LC_D void mma_commit(uint64_t* bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                   smem_u32(bar))
-               : "memory");
-}
-
-LC_D void tmem_ld16(uint32_t addr, uint32_t (&v)[16]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
-        "=r"(v[15])
-      : "r"(addr));
-}
-
-LC_D void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-LC_D void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
 // ------------------------------------------------------------------ key tables
 
@@ -434,32 +379,6 @@ struct TnParams {
   uint32_t* err;
 };
 
-// K-major operand, 64-byte swizzle: 64-byte rows, 8-row groups of 512 bytes
-// (SBO), start address advanced by 32 bytes per K step inside the atom.
-LC_D uint64_t umma_desc_sw64(uint32_t saddr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFF);  // start address
-  d |= (uint64_t)1 << 16;                   // leading byte offset (unused here)
-  d |= (uint64_t)(512 >> 4) << 32;          // stride byte offset
-  d |= (uint64_t)1 << 46;                   // descriptor version
-  d |= (uint64_t)4 << 61;                   // layout: 64-byte swizzle
-  return d;
-}
-
-LC_D void tmem_ld8(uint32_t addr, uint32_t (&v)[8]) {
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
-               : "r"(addr));
-}
-
-LC_D void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
-          smem_u32(dst)),
-      "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
-      : "memory");
-}
-
 // sum_l 2^(8l) D_l mod p for one output (|D_l| < 2^22).  A = D0 + 2^8 D1 +
 // 2^16 D2 + 2^24 D3 and B (limbs 4..7) are exact in int64 (|A|, |B| < 2^47);
 // the value is A + B 2^32 and B 2^32 = lo(B) 2^32 + hi(B) 2^64 with
@@ -638,24 +557,6 @@ __global__ void __launch_bounds__(kTnThreads, 1)
 }
 
 // ------------------------------------------------------------------ host side
-
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-static EncodeTiledFn encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void* ptr = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiledFn>(ptr);
-    cudaGetLastError();
-  });
-  return fn;
-}
 
 }  // namespace lc
 
@@ -895,19 +796,6 @@ struct SpCfg {
   static_assert(STAGE % 1024 == 0 && B_ATOM % 256 == 0, "swizzle atoms stay aligned");
   static_assert(SMEM <= 227 * 1024, "shared memory");
 };
-
-// MN-major operand: LBO = bytes to the next atom along M/N, SBO = bytes to
-// the next 8-row group along K; layout 2 = 128-byte swizzle, 4 = 64-byte,
-// 6 = 32-byte.
-LC_D uint64_t umma_desc_mn(uint32_t saddr, uint32_t lbo, uint32_t sbo, uint32_t layout) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
-  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
-  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
-  d |= (uint64_t)1 << 46;
-  d |= (uint64_t)layout << 61;
-  return d;
-}
 
 // D = s32, A = B = u8, both MN-major (bits 15, 16), M = 128
 template <int N>

@@ -89,9 +89,10 @@ def _time_batch(batch, reps: int) -> float:
 
 
 def tune_batch(batch, reps: int = 2):
-    """Pick the product chunk, the CTAs per SM of the persistent launches and
-    the work items per claim for this batch: a coordinate search (chunk at
-    2 CTAs/SM, then CTAs/SM, then the claim size) timed with CUDA events.
+    """Pick the product chunk (CUDA-core products only), the CTAs per SM of
+    the persistent launches and the work items per claim for this batch: a
+    coordinate search (chunk at 2 CTAs/SM, then CTAs/SM, then the claim
+    size) timed with CUDA events.
     Leaves the best configuration on ``batch``; returns (config, timings)."""
     timings = {}
 
@@ -101,7 +102,10 @@ def tune_batch(batch, reps: int = 2):
             timings[cfg] = _time_batch(batch, reps)
         return timings[cfg]
 
-    best = min(((c, 2, 1) for c in BATCH_CHUNKS), key=t)
+    # the chunk only shapes the CUDA-core products; the tensor-core form
+    # splits its items at the exact-int32 bound instead
+    chunks = BATCH_CHUNKS if batch.products == batch.PRODUCTS_INT64 else (batch.config[0],)
+    best = min(((c, 2, 1) for c in chunks), key=t)
     best = min(((best[0], n, 1) for n in BATCH_CTAS), key=t)
     best = min(((best[0], best[1], k) for k in BATCH_CLAIMS), key=t)
     batch.set_config(*best)

@@ -5,7 +5,9 @@ Every job of a mixed batch (ring degrees 64/128/256; Goldilocks, the 4-prime
 equal the same job committed one by one through a key view
 (lc_ajtai_key_view + lc_ajtai_commit_i8), and sampled jobs the oracle's
 AjtaiPublicKey::commit (lattice-commitment/src/ajtai.rs:118-153) on the key's
-first kappa rows and n columns.  Also: lanes split at 128 jobs, every tuning
+first kappa rows and n columns -- with the products on the tensor cores (the
+default) and on the CUDA cores.  Also: jobs longer than one exact int32
+chunk of the tensor products, lanes split at 128 jobs, every tuning
 configuration, graph replay after the witnesses change in place, and the
 argument checks.
 """
@@ -114,10 +116,14 @@ def test_key_view_matches_submatrix_key(mixed_classes):
         key_view(cl["keys"][0], 8, 301)
 
 
-@pytest.mark.parametrize("graph", [False, True])
-def test_batch_mixed_jobs(mixed_classes, graph):
+@pytest.mark.parametrize("graph,products", [(False, CommitBatch.PRODUCTS_TENSOR), (True, CommitBatch.PRODUCTS_TENSOR),
+                                            (True, CommitBatch.PRODUCTS_INT64)])
+def test_batch_mixed_jobs(mixed_classes, graph, products):
     jobs = make_jobs(mixed_classes, 60, 7)
     batch = CommitBatch([c["keys"] for c in mixed_classes], jobs, graph=graph)
+    assert batch.products == CommitBatch.PRODUCTS_TENSOR  # the default
+    batch.products = products
+    assert batch.products == products
     for _ in range(3):  # eager, capture + launch, replay
         batch.run()
         batch.check()
@@ -158,6 +164,40 @@ def test_batch_lane_split_and_replay(mixed_classes):
         assert torch.equal(j.out, one_by_one(cls, j))
 
 
+def test_batch_tensor_products_over_several_chunks():
+    """Jobs longer than one exact int32 chunk (32768 ring elements) and blocks
+    whose jobs end at different ring elements: tensor products = CUDA-core
+    products = one-by-one commits = the oracle, after switching modes back
+    and forth under a captured graph."""
+    m = 70000
+    classes = [gl_class(6, m, 41), u32_class(CRT_SET_30BIT[:1], 6, m, 42)]
+    lens = [70000, 69999, 40000, 32769, 32768, 100, 1]
+    jobs = []
+    for c in range(2):
+        for k, n in enumerate(lens + [int(x) for x in np.random.default_rng(c).integers(1, m, 30)]):
+            w = torch.empty(n * 64, dtype=torch.int8, device="cuda")
+            synth.fill_device(w, "i8", 43 + c, k)
+            dt = torch.int64 if c == 0 else torch.int32
+            out = torch.full((1, 16 if k % 2 else 8, 64), -1, dtype=dt, device="cuda")
+            jobs.append(CommitJob(c, out.shape[1], n, w.view(n, 64), out))
+    batch = CommitBatch([c["keys"] for c in classes], jobs, graph=True)
+    outs = {}
+    for mode in (CommitBatch.PRODUCTS_TENSOR, CommitBatch.PRODUCTS_INT64, CommitBatch.PRODUCTS_TENSOR):
+        batch.products = mode
+        for _ in range(2):
+            batch.run()
+        batch.check()
+        outs.setdefault(mode, []).append([j.out.clone() for j in jobs])
+    for a, b in zip(outs[CommitBatch.PRODUCTS_TENSOR][0], outs[CommitBatch.PRODUCTS_INT64][0]):
+        assert torch.equal(a, b)
+    for a, b in zip(outs[CommitBatch.PRODUCTS_TENSOR][0], outs[CommitBatch.PRODUCTS_TENSOR][1]):
+        assert torch.equal(a, b)
+    for j in jobs:
+        assert torch.equal(j.out, one_by_one(classes, j)), (j.cls, j.kappa, j.n)
+    for j in (jobs[0], jobs[3], jobs[len(lens)], jobs[len(lens) + 2]):
+        assert np.array_equal(as_u(j.out), oracle_job(classes[j.cls], j)), (j.cls, j.kappa, j.n)
+
+
 def test_batch_argument_checks(mixed_classes):
     cl = mixed_classes[0]
     keys = [cl["keys"]]
@@ -174,3 +214,5 @@ def test_batch_argument_checks(mixed_classes):
     empty = CommitBatch(keys, [])
     empty.run()
     empty.check()
+    with pytest.raises(LatticeCudaError):  # no such product mode
+        empty.products = 7
