@@ -65,6 +65,8 @@ def parse():
                     default=None,
                     help="run only one secondary measurement (1 GPU) and print its JSON object")
     ap.add_argument("--no-fold", action="store_true", help="skip the folding-step measurement")
+    ap.add_argument("--ntt-only", action="store_true",
+                    help="only the headline NTT round trip (for profiling its kernels)")
     ap.add_argument("--fold-m", type=int, default=1 << 20, help="ring elements of the folding-step witness")
     ap.add_argument("--fold-steps", type=int, default=5)
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch measurement")
@@ -1136,18 +1138,19 @@ def run_ours(args):
     # since the library allocates its keys and scratch with cudaMalloc
     del x, y, z
     torch.cuda.empty_cache()
-    commit = None if args.no_commit else bench_commit(args, rank, max_over_ranks, barrier, world)
+    legs = not args.ntt_only
+    commit = bench_commit(args, rank, max_over_ranks, barrier, world) if legs and not args.no_commit else None
     torch.cuda.empty_cache()
-    fold = None if args.no_fold else bench_fold(args, rank, max_over_ranks, barrier, world)
+    fold = bench_fold(args, rank, max_over_ranks, barrier, world) if legs and not args.no_fold else None
     torch.cuda.empty_cache()
-    uneven = None if args.no_uneven else bench_uneven(args, rank, max_over_ranks, barrier, world)
+    uneven = bench_uneven(args, rank, max_over_ranks, barrier, world) if legs and not args.no_uneven else None
     torch.cuda.empty_cache()
-    single = bench_single(args, rank, max_over_ranks, barrier, world)
-    keygen = bench_keygen(args, rank, max_over_ranks, barrier, world)
+    single = bench_single(args, rank, max_over_ranks, barrier, world) if legs else None
+    keygen = bench_keygen(args, rank, max_over_ranks, barrier, world) if legs else None
     torch.cuda.empty_cache()
-    quad50 = bench_quad50(args, rank, max_over_ranks, barrier, world)
+    quad50 = bench_quad50(args, rank, max_over_ranks, barrier, world) if legs else None
     torch.cuda.empty_cache()
-    labinius = bench_labinius(args, rank, max_over_ranks, barrier, world)
+    labinius = bench_labinius(args, rank, max_over_ranks, barrier, world) if legs else None
     torch.cuda.empty_cache()
 
     ctx.close()
@@ -1158,14 +1161,17 @@ def run_ours(args):
     fwd_avg = statistics.mean(fwd_ms)
     inv_avg = statistics.mean(inv_ms)
     achieved = ALG_BYTES_PER_LAUNCH / (fwd_avg / 1e3) / 1e9
-    traffic = None
+    # DRAM bytes of one forward launch from an ncu capture of the variant the
+    # tuner picked (null when no capture of that variant is recorded)
+    traffic, traffic_variant = None, tuning.get("variant")
     tpath = os.path.join(ROOT, "profiles", "ntt_crt4_d256_traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            traffic = json.load(f).get("forward_bytes_per_launch")
+            rec = json.load(f).get("forward_bytes_per_launch", {})
+        traffic = rec.get(str(traffic_variant)) if isinstance(rec, dict) else None
     roofline = {
         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-        "frac": achieved / peak, "traffic": traffic,
+        "frac": achieved / peak, "traffic": traffic, "traffic_variant": traffic_variant,
         "kernel": "NTT forward, ShoupLazy, log_n=8, log_v=4 (tuned variant)",
         "tuning": tuning,
         "peak_source": peak_kind,

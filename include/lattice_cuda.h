@@ -241,9 +241,17 @@ LC_API int lc_tc_i8_rate(uint32_t iters, int s8, double *ops_per_s, float *ms);
  * witness forward transforms, the pointwise products against the cached
  * NTT(A), their sum over the whole witness and the row inverse transforms,
  * i.e. the whole body of AjtaiPublicKey::commit (ajtai.rs:118-153) -- rather
- * than the staged launches.  Identical results; enable = 0 turns it off for
- * this key (every commit then runs staged), 1 turns it back on.
- * lc_ajtai_key_get_fused returns 1 or 0 (-1 for a null key). */
+ * than the staged launches.  Larger commits whose per-slot products run on
+ * the CUDA cores (LC_PRODUCTS_INT64), log_n 6..8, can run their products,
+ * the modular sum of the K splits and the row inverse transforms as one
+ * cooperative launch after the witness transforms (grid barriers between the
+ * three phases; ajtai.rs:139-150).  enable = 1 (the default) uses the one-
+ * launch forms where they measured faster -- the single launch above and,
+ * for batches of at most 3 witnesses, the one-launch products + inverse
+ * NTT; enable = 2 uses the one-launch products + inverse NTT for every
+ * batch shape as well; enable = 0 runs every commit staged (products, split
+ * sum, inverse NTT as separate launches).  Identical results.
+ * lc_ajtai_key_get_fused returns 0, 1 or 2 (-1 for a null key). */
 LC_API int lc_ajtai_key_set_fused(lc_ajtai_key *key, int enable);
 LC_API int lc_ajtai_key_get_fused(const lc_ajtai_key *key);
 

@@ -84,13 +84,15 @@ class _DeviceKey:
         check(_lib.lib().lc_ajtai_key_set_engine(self._h, int(value)), "lc_ajtai_key_set_engine")
 
     @property
-    def fused(self) -> bool:
-        """Whether small commitments run as one launch (lc_ajtai_key_set_fused)."""
-        return _lib.lib().lc_ajtai_key_get_fused(self._h) == 1
+    def fused(self) -> int:
+        """One-launch forms (lc_ajtai_key_set_fused): 0 never, 1 where they are
+        faster (the default), 2 for every batch shape; truthy unless 0."""
+        return _lib.lib().lc_ajtai_key_get_fused(self._h)
 
     @fused.setter
-    def fused(self, value: bool):
-        check(_lib.lib().lc_ajtai_key_set_fused(self._h, 1 if value else 0), "lc_ajtai_key_set_fused")
+    def fused(self, value):
+        level = value if isinstance(value, int) and not isinstance(value, bool) else (1 if value else 0)
+        check(_lib.lib().lc_ajtai_key_set_fused(self._h, level), "lc_ajtai_key_set_fused")
 
     @property
     def slot_products(self) -> int:

@@ -6,8 +6,10 @@
 // of its class's key(s).  Jobs that share a key form lanes of at most 128
 // jobs, sorted by n (longest first).  At ring element j only the jobs with
 // n_b > j take part, so a lane's transformed witnesses are stored as a
-// staircase: slot t, ring element j, job b at  what[t*S + R[j] + b],  where
-// R[j] = sum over j' < j of the number of jobs longer than j', S = sum n_b.
+// staircase: slot t, ring element j, job b at  what[t*Sp + Rp[j] + b],  where
+// R[j] = sum over j' < j of the number of jobs longer than j' (S = sum n_b),
+// Rp[j] the same with every row of active jobs padded to 16 bytes (so each
+// row starts 16-byte aligned) and Sp = Rp[n_max] the entries per slot.
 //   1. witness NTT: an item is PB consecutive staircase polynomials; their
 //      (j, b) come from a per-item start table and a short walk over R;
 //   2. product: a warp's item is (chunk of ring elements, slot t, block of 16
@@ -73,7 +75,9 @@ struct LaneDesc {
   uint32_t n_max;   // longest job
   uint32_t nchunks;
   uint64_t S;       // staircase polynomials
-  const uint64_t* R;       // [n_max + 1]
+  const uint64_t* R;       // [n_max + 1]: jobs longer than j' summed over j' < j
+  const uint64_t* Rp;      // [n_max + 1]: the same with every row padded to 16 bytes (where row j starts)
+  uint64_t Sp;             // entries per slot of `what` (16-byte rows, 16-byte slots)
   const uint32_t* item_j;  // witness items: ring element of the first polynomial
   uint32_t sub0;           // first job of the lane in the sub-job table
   uint32_t pb;             // polynomials per witness item
@@ -122,7 +126,7 @@ struct BCfg {
   static constexpr int PB = GROUPS * IT;  // polynomials per witness item
   static constexpr int TWE = G::fwd_entries() > G::inv_entries() ? G::fwd_entries() : G::inv_entries();
   static constexpr size_t TWB = ((size_t)TWE * sizeof(Tw) + 15) / 16 * 16;
-  static constexpr size_t SMEM1 = TWB + (size_t)PB * SS * sizeof(T) + (size_t)PB * 8 + (size_t)(PB + 2) * 8;
+  static constexpr size_t SMEM1 = TWB + (size_t)PB * SS * sizeof(T) + (size_t)PB * 16 + (size_t)(PB + 2) * 16;
   static constexpr size_t SMEM3 = TWB + (size_t)16 * SS * sizeof(T);
   static_assert(SS >= Slots<A, LOG_N, LOG_V>::S, "slot stride");
 };
@@ -153,9 +157,10 @@ LC_D void witness_item(const LaneDesc& L, const SubJob* __restrict__ subs, uint6
   constexpr int N = C::N, PB = C::PB, SS = C::SS;
   Tw* tw = reinterpret_cast<Tw*>(smem);
   T* slots = reinterpret_cast<T*>(smem + C::TWB);
-  uint32_t* sj = reinterpret_cast<uint32_t*>(slots + PB * SS);
-  uint32_t* sb = sj + PB;
-  uint64_t* sR = reinterpret_cast<uint64_t*>(sb + PB);  // R[j_lo .. j_lo + PB + 1]
+  const int8_t** ssrc = reinterpret_cast<const int8_t**>(slots + PB * SS);  // digits of each polynomial (or null)
+  uint64_t* sdst = reinterpret_cast<uint64_t*>(ssrc + PB);                 // its row offset Rp[j] + b in a slot
+  uint64_t* sR = sdst + PB;                                                // R[j_lo .. j_lo + PB + 1]
+  uint64_t* sRp = sR + PB + 2;                                             // Rp[j_lo .. j_lo + PB + 1]
   __shared__ uint32_t s_jlo;
   const int tid = threadIdx.x;
   const uint64_t p0 = k * PB;
@@ -166,34 +171,66 @@ LC_D void witness_item(const LaneDesc& L, const SubJob* __restrict__ subs, uint6
   // consecutive staircase polynomials advance the ring element by at most one,
   // so the item's PB polynomials lie in ring elements j_lo .. j_lo + PB - 1
   const uint32_t jlo = s_jlo;
-  if (tid < PB + 2) sR[tid] = jlo + tid <= L.n_max ? L.R[jlo + tid] : L.S;
+  if (tid < PB + 2) {
+    sR[tid] = jlo + tid <= L.n_max ? L.R[jlo + tid] : L.S;
+    sRp[tid] = jlo + tid <= L.n_max ? L.Rp[jlo + tid] : L.Sp;
+  }
   __syncthreads();
+  // polynomial p of the staircase: ring element j, job b; its digits and its
+  // place in every slot of `what`, looked up once here
   if (tid < PB) {
     const uint64_t p = p0 + tid;
-    uint32_t jr = 0xFFFFFFFFu, br = 0;
+    const int8_t* src = nullptr;
+    uint64_t dst = 0;
     if (p < L.S) {
       uint32_t x = 0;
       while (sR[x + 1] <= p) ++x;
-      jr = jlo + x;
-      br = (uint32_t)(p - sR[x]);
+      const uint32_t br = (uint32_t)(p - sR[x]);
+      src = subs[L.sub0 + br].w + (size_t)(jlo + x) * N;
+      dst = sRp[x] + br;
     }
-    sj[tid] = jr;
-    sb[tid] = br;
+    ssrc[tid] = src;
+    sdst[tid] = dst;
   }
   __syncthreads();
+  // the item's 16-digit chunks: every load of a thread issued before its
+  // conversions, so several loads are in flight
   constexpr int CH = N / 16;  // 16-digit chunks per polynomial
-  for (int e = tid; e < PB * CH; e += kBatchThreads) {
-    const int s = e / CH, c = e % CH;
-    T* dst = slots + s * SS + c * 16;
-    if (sj[s] != 0xFFFFFFFFu) {
-      const SubJob& J = subs[L.sub0 + sb[s]];
-      const uint4 v = *reinterpret_cast<const uint4*>(J.w + (size_t)sj[s] * N + c * 16);
-      const int8_t* x = reinterpret_cast<const int8_t*>(&v);
+  constexpr int PER = (PB * CH + kBatchThreads - 1) / kBatchThreads;
+  uint4 v[PER];
 #pragma unroll
-      for (int u = 0; u < 16; ++u) dst[u] = digit_residue<T>(x[u], L.q);
-    } else {
+  for (int u = 0; u < PER; ++u) {
+    const int e = tid + u * kBatchThreads;
+    v[u] = make_uint4(0, 0, 0, 0);
+    if (e < PB * CH) {
+      const int8_t* src = ssrc[e / CH];
+      if (src) v[u] = __ldg(reinterpret_cast<const uint4*>(src + (e % CH) * 16));
+    }
+  }
+  // Lanes of a warp hold neighbouring 16-digit chunks 16 words apart; lane l
+  // stores its chunk starting at digit (l % 16), so that one store
+  // instruction of the warp touches 16 distinct banks per polynomial instead
+  // of 2.  The 16 bytes are rotated once (word selects, then byte funnel
+  // shifts), so every digit is then taken from a fixed register position.
+  const uint32_t rot = (uint32_t)tid & 15u;
 #pragma unroll
-      for (int u = 0; u < 16; ++u) dst[u] = 0;
+  for (int u = 0; u < PER; ++u) {
+    const int e = tid + u * kBatchThreads;
+    if (e < PB * CH) {
+      T* dst = slots + (e / CH) * SS + (e % CH) * 16;
+      // byte i of (r0 r1 r2 r3) = byte (i + rot) mod 16 of the chunk
+      const bool w1 = rot & 4u, w2 = rot & 8u;
+      const uint32_t t0 = w1 ? v[u].y : v[u].x, t1 = w1 ? v[u].z : v[u].y;
+      const uint32_t t2 = w1 ? v[u].w : v[u].z, t3 = w1 ? v[u].x : v[u].w;
+      const uint32_t q0 = w2 ? t2 : t0, q1 = w2 ? t3 : t1, q2 = w2 ? t0 : t2, q3 = w2 ? t1 : t3;
+      const uint32_t sh = 8u * (rot & 3u);
+      const uint32_t r[4] = {__funnelshift_r(q0, q1, sh), __funnelshift_r(q1, q2, sh), __funnelshift_r(q2, q3, sh),
+                             __funnelshift_r(q3, q0, sh)};
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int8_t x = (int8_t)(uint8_t)(r[i >> 2] >> (8 * (i & 3)));
+        dst[(i + rot) & 15u] = digit_residue<T>(x, L.q);
+      }
     }
   }
   __syncthreads();
@@ -203,10 +240,17 @@ LC_D void witness_item(const LaneDesc& L, const SubJob* __restrict__ subs, uint6
     transform_slot<A, LOG_N, LOG_V, false>(slots + (it * C::GROUPS + tid / Geo<LOG_N, LOG_V>::T) * SS, tw, ar,
                                            tid % Geo<LOG_N, LOG_V>::T);
   __syncthreads();
-  T* what = reinterpret_cast<T*>(L.what);
-  for (int e = tid; e < PB * N; e += kBatchThreads) {
-    const int tt = e / PB, s = e % PB;
-    if (sj[s] != 0xFFFFFFFFu) what[(size_t)tt * L.S + p0 + s] = slots[s * SS + tt];
+  // PB divides the block, so a thread keeps one polynomial s and walks its
+  // slots tt = tid / PB, + 256 / PB, ...: one slot-strided store each
+  static_assert(kBatchThreads % PB == 0, "a thread keeps its polynomial");
+  {
+    constexpr int TSTEP = kBatchThreads / PB;
+    const int s = tid % PB;
+    if (ssrc[s]) {
+      T* wp = reinterpret_cast<T*>(L.what) + sdst[s] + (size_t)(tid / PB) * L.Sp;
+      const size_t step = (size_t)TSTEP * L.Sp;
+      for (int tt = tid / PB; tt < N; tt += TSTEP, wp += step) *wp = slots[s * SS + tt];
+    }
   }
   __syncthreads();
 }
@@ -221,7 +265,7 @@ LC_D void witness_item(const LaneDesc& L, const SubJob* __restrict__ subs, uint6
 // (ip, g) holds rows 2ip, 2ip+1 of jobs 4(4*blk + g) .. +3 in 160-bit
 // accumulators and streams, two ring elements at a time (loads before the
 // multiply-adds), the key pair Ahat[t][j][2ip..2ip+1] and the witness values
-// what[t*S + R[j] + b] from L2.
+// what[t*Sp + Rp[j] + b] from L2.
 template <class E>
 LC_D void load_pair(const E* p, E& a0, E& a1);
 template <>
@@ -265,8 +309,8 @@ LC_D void product_warp_item(const LaneDesc& L, const SubJob* __restrict__ subs, 
   // other quads' shorter jobs are masked by j < nq[u]
   const uint32_t jend = __shfl_sync(0xffffffffu, min(j1, nq[0]), 0);
   const E* A = reinterpret_cast<const E*>(L.ahat) + (size_t)t * L.a_m * kIPad + 2 * ip;
-  const E* W = reinterpret_cast<const E*>(L.what) + (size_t)t * L.S + 4 * bq;
-  const uint64_t* R = L.R;
+  const E* W = reinterpret_cast<const E*>(L.what) + (size_t)t * L.Sp + 4 * bq;
+  const uint64_t* R = L.Rp;  // where each ring element's row of active jobs starts
   // The staircase offsets of 32 ring elements arrive in one coalesced load and
   // are broadcast by shuffles; the key and witness loads of JU ring elements
   // issue together before their multiply-adds, so a warp keeps several
@@ -493,10 +537,11 @@ __global__ void __launch_bounds__(kBatchThreads, sizeof(E) == 8 ? 2 : 3)
 // second A atom is a zero tile), N = 32 L bytes (b, lw), K = the chunk.  The
 // key rows Ahat[t][j][16] arrive by TMA (a 3-D map per lane: row bytes,
 // j < a_m, slot); the witness rows come from the staircase, where row j of
-// the block is the 32 L contiguous bytes at what[t S + R[j] + 32 blk] of
-// which only the first cnt(j) - 32 blk jobs are active: four gather warps
-// copy them with zero-filling cp.async straight into the 128-byte-swizzled
-// MN-major layout the MMA descriptor reads (chunk c of row r at c ^ (r & 7)),
+// the block is the 32 L contiguous bytes at what[t Sp + Rp[j] + 32 blk]
+// (16-byte aligned) of which only the first cnt(j) - 32 blk jobs are active:
+// four gather warps copy them in 16-byte chunks with zero-filling cp.async
+// straight into the 128-byte-swizzled MN-major layout the MMA descriptor
+// reads (chunk c of row r at c ^ (r & 7)),
 // so the shorter jobs of a block contribute zeros and nothing outside the
 // staircase is read.  The epilogue (the same four warps) writes D, one
 // [32 L columns][128 rows] int32 tile per item; the finish launch folds the
@@ -532,10 +577,10 @@ struct TpIdesc {
       (2u << 4) | (1u << 15) | (1u << 16) | ((uint32_t)(N >> 3) << 17) | ((128u >> 4) << 24);
 };
 
-template <int EB>
-LC_D void cp_async_zfill(uint32_t dst, const void* src, uint32_t bytes) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(dst), "l"(src), "n"(EB), "r"(bytes)
-               : "memory");
+// 16-byte global -> shared copy of `bytes` (0..16) source bytes, the rest zero
+// (src and dst 16-byte aligned; no byte is read when bytes = 0)
+LC_D void cp_async16_zfill(uint32_t dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
 }
 LC_D void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
@@ -636,15 +681,20 @@ __global__ void __launch_bounds__(kTpThreads, 1)
     }
   } else {
     // ---------------- gather: warp g = warp - 2 fills rows 16 g .. 16 g + 15 of
-    // every stage, lane l the entry of job 32 blk + l (EB bytes)
+    // every stage in 16-byte chunks.  Row j of the block starts at
+    // what[t Sp + Rp[j] + 32 blk], 16-byte aligned; chunk k holds jobs
+    // 32 blk + k J .. + J - 1 (J = 16 / EB), of which the first
+    // cnt(j) - 32 blk - k J are active and copied, the rest zero-filled.
+    constexpr int J = 16 / EB;           // jobs per chunk
+    constexpr int CPR = C::NB / 16;      // chunks per row (16 or 8)
+    constexpr int RPI = 32 / CPR;        // rows per warp instruction (2 or 4)
     const int g = warp - 2;
     using E = typename std::conditional<EB == 8, uint64_t, uint32_t>::type;
-    const E* W = reinterpret_cast<const E*>(L.what) + (size_t)it.t * L.S + (size_t)kTpJobs * it.blk + lane;
-    const uint32_t bx = (uint32_t)lane * EB;  // byte of the entry in the N row
-    const uint32_t boff = (bx >> 7) * C::B_ATOM + (bx & 15);
-    const uint32_t bchunk = (bx & 127) >> 4;
-    const uint32_t act0 = kTpJobs * it.blk;   // jobs before the block
-    int issued = 0;
+    const E* W = reinterpret_cast<const E*>(L.what) + (size_t)it.t * L.Sp + (size_t)kTpJobs * it.blk;
+    const uint32_t k = (uint32_t)lane % CPR, rsub = (uint32_t)lane / CPR;
+    const uint32_t boff = (k >> 3) * C::B_ATOM;  // swizzle atom of the chunk
+    const uint32_t kc = k & 7;
+    const int first_job = kTpJobs * (int)it.blk + (int)(k * J);
     bool ok = true;
     for (int s = 0; s < nst; ++s) {
       if (*abort_flag) {
@@ -657,21 +707,24 @@ __global__ void __launch_bounds__(kTpThreads, 1)
         break;
       }
       const uint32_t jb = j0 + kTpRows * s + 16 * g;
-      // R[jb .. jb + 16]: the rows' staircase offsets and job counts
-      const uint64_t rl = (lane <= 16 && jb + lane <= L.n_max) ? __ldg(L.R + jb + lane) : 0;
+      // R[jb .. jb + 16] (job counts) and Rp[jb .. jb + 15] (row starts)
+      const bool in_r = lane <= 16 && jb + lane <= L.n_max;
+      const uint64_t rl = in_r ? __ldg(L.R + jb + lane) : 0;
+      const uint64_t rpl = in_r ? __ldg(L.Rp + jb + lane) : 0;
       const uint32_t sb = smem_u32(stage(s)) + C::A_BYTES + boff;
-#pragma unroll 4
-      for (int r = 0; r < 16; ++r) {
+#pragma unroll
+      for (int rr = 0; rr < 16; rr += RPI) {
+        const int r = rr + (int)rsub;
         const uint64_t r0 = __shfl_sync(0xffffffffu, rl, r);
         const uint64_t r1 = __shfl_sync(0xffffffffu, rl, r + 1);
+        const uint64_t rp = __shfl_sync(0xffffffffu, rpl, r);
         const uint32_t j = jb + r, row = 16 * g + r;
-        const uint32_t cnt = (uint32_t)(r1 - r0);
-        const bool live = j < j1 && cnt > act0 + (uint32_t)lane;
-        const uint32_t dst = sb + row * 128 + ((bchunk ^ (row & 7)) << 4);
-        cp_async_zfill<EB>(dst, live ? (const void*)(W + r0) : L.what, live ? EB : 0);
+        const int act = (j < j1) ? (int)(r1 - r0) - first_job : 0;  // active jobs from this chunk's first
+        const uint32_t bytes = act <= 0 ? 0u : act >= J ? 16u : (uint32_t)act * EB;
+        const uint32_t dst = sb + row * 128 + ((kc ^ (row & 7)) << 4);
+        cp_async16_zfill(dst, bytes ? (const void*)(W + rp + k * J) : L.what, bytes);
       }
       cp_async_commit();
-      ++issued;
       if (s >= kTpLag) {
         cp_async_wait<kTpLag>();
         fence_proxy_async_smem();
@@ -682,7 +735,6 @@ __global__ void __launch_bounds__(kTpThreads, 1)
     fence_proxy_async_smem();
     if (ok)
       for (int s = max(0, nst - kTpLag); s < nst; ++s) mbar_arrive(&full[s % kTpStages]);
-    (void)issued;
     // ---------------- epilogue: lane = row (i, la); column = (b, lw)
     const bool fin = ok && nst > 0 && !*abort_flag && mbar_wait(done, 0);
     if (__all_sync(0xffffffffu, fin)) {
@@ -1077,6 +1129,17 @@ LC_API int lc_batch_create(const lc_commit_class* classes, uint32_t num_classes,
         }
         R[L.n_max] = acc;
         L.S = acc;
+        // the same offsets with each row of active jobs padded to 16 bytes, so
+        // that every row of `what` starts 16-byte aligned
+        const uint64_t pad = 16 / eb;
+        std::vector<uint64_t> Rp(L.n_max + 1);
+        uint64_t accp = 0;
+        for (uint32_t j = 0; j < L.n_max; ++j) {
+          Rp[j] = accp;
+          accp += (R[j + 1] - R[j] + pad - 1) / pad * pad;
+        }
+        Rp[L.n_max] = accp;
+        L.Sp = accp;
         ij_off.push_back(itemj_all.size());
         const uint64_t items = (L.S + pb - 1) / pb;
         uint32_t j = 0;
@@ -1086,9 +1149,10 @@ LC_API int lc_batch_create(const lc_commit_class* classes, uint32_t num_classes,
           itemj_all.push_back(j);
         }
         Rall.insert(Rall.end(), R.begin(), R.end());
+        Rall.insert(Rall.end(), Rp.begin(), Rp.end());
         b->R.push_back(std::move(R));
         what_off.push_back(what_bytes);
-        what_bytes += ((size_t)d * L.S * eb + 255) / 256 * 256;
+        what_bytes += ((size_t)d * L.Sp * eb + 255) / 256 * 256;
         part_off.push_back(partial_bytes);
         partial_bytes += (((size_t)(L.n_max + kMinChunk - 1) / kMinChunk) * d * kIPad * L.nb * eb + 255) / 256 * 256;
         b->lanes.push_back(L);
@@ -1117,6 +1181,7 @@ LC_API int lc_batch_create(const lc_commit_class* classes, uint32_t num_classes,
   for (size_t l = 0; l < b->lanes.size(); ++l) {
     LaneDesc& L = b->lanes[l];
     L.R = b->d_R + r_off[l];
+    L.Rp = L.R + L.n_max + 1;
     L.item_j = b->d_itemj + ij_off[l];
     L.what = b->d_what + what_off[l];
     L.partial = b->d_partial + part_off[l];

@@ -215,25 +215,19 @@ struct MacCfg {
   static constexpr size_t SMEM = 2 * STAGE + 16;
 };
 
+// One product work item (slot t, b-tile bt, K split) of the tiled form.  The
+// caller initialises the two stage barriers once; `parity` carries their
+// phases across the items a CTA runs.  Returns false after a timed-out wait
+// (the error word is set and the CTA's copies have been waited for).
 template <class E, int JB>
-__global__ void __launch_bounds__(256)
-    mac_tiled_kernel(const E* __restrict__ ahat_t, uint32_t am, const E* __restrict__ what_t, E* __restrict__ partial,
-                     uint32_t m, uint32_t b_pad, uint32_t n, uint32_t splits, uint32_t q,
-                     uint32_t* err) {
+LC_D bool mac_tile(const E* __restrict__ ahat_t, uint32_t am, const E* __restrict__ what_t, E* __restrict__ partial,
+                   uint32_t m, uint32_t b_pad, uint32_t n, uint32_t splits, uint32_t q, uint32_t* err, uint32_t t,
+                   uint32_t bt, uint32_t split, unsigned char* smem_raw, uint64_t* bar, uint32_t& parity) {
   using C = MacCfg<E, JB>;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + 2 * C::STAGE);
-  const uint32_t t = blockIdx.x, bt = blockIdx.y, split = blockIdx.z;
   const uint32_t per = (m + splits - 1) / splits;
   const uint32_t j0 = split * per, j1 = min(m, j0 + per);
   const int tid = threadIdx.x;
   const int ti = tid >> 5, tb = tid & 31;
-  if (tid == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
-    fence_mbar_init();
-  }
-  __syncthreads();
   auto stage_a = [&](int s) { return reinterpret_cast<E*>(smem_raw + s * C::STAGE); };
   auto stage_w = [&](int s) { return reinterpret_cast<E*>(smem_raw + s * C::STAGE + C::A_BYTES); };
   auto issue = [&](uint32_t jb, int s) {
@@ -252,7 +246,6 @@ __global__ void __launch_bounds__(256)
   Acc160 acc[2][4];
   const uint32_t nblk = (j1 > j0) ? (j1 - j0 + JB - 1) / JB : 0;
   if (tid == 0 && nblk > 0) issue(j0, 0);
-  uint32_t parity = 0;
   bool failed = false;
   uint32_t failed_blk = 0;
   for (uint32_t k = 0; k < nblk; ++k) {
@@ -283,7 +276,7 @@ __global__ void __launch_bounds__(256)
   if (failed) {
     if (tid == 0) {
       record_error(err, LC_DEVERR_TIMEOUT);
-      // Copies that may still be landing must finish before the CTA exits:
+      // Copies that may still be landing must finish before the CTA moves on:
       // the block whose wait expired (its phase is the one before the
       // toggle) and the prefetch of the following block.  Bounded waits; if
       // either expires again, the error word is marked poisoned.
@@ -295,7 +288,7 @@ __global__ void __launch_bounds__(256)
       }
       if (!landed) record_poisoned(err);
     }
-    return;
+    return false;
   }
   // partial[split][t][i][b]
   for (int ii = 0; ii < 2; ++ii)
@@ -303,6 +296,26 @@ __global__ void __launch_bounds__(256)
       const uint32_t i = 2 * ti + ii, b = bt * kBTile + tb + 32 * u;
       partial[(((size_t)split * n + t) * kIPad + i) * b_pad + b] = acc_reduce<E>(acc[ii][u], q);
     }
+  return true;
+}
+
+template <class E, int JB>
+__global__ void __launch_bounds__(256)
+    mac_tiled_kernel(const E* __restrict__ ahat_t, uint32_t am, const E* __restrict__ what_t, E* __restrict__ partial,
+                     uint32_t m, uint32_t b_pad, uint32_t n, uint32_t splits, uint32_t q,
+                     uint32_t* err) {
+  using C = MacCfg<E, JB>;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + 2 * C::STAGE);
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  uint32_t parity = 0;
+  mac_tile<E, JB>(ahat_t, am, what_t, partial, m, b_pad, n, splits, q, err, blockIdx.x, blockIdx.y, blockIdx.z,
+                  smem_raw, bar, parity);
 }
 
 // Small-batch product for b_pad a multiple of 4: one thread per (split, t,
@@ -312,13 +325,12 @@ __global__ void __launch_bounds__(256)
 // both streams are prefetched into L2 16 ring elements ahead (the loop is
 // otherwise bound by DRAM latency).
 template <class E>
-__global__ void __launch_bounds__(256)
-    mac_quad_kernel(const E* __restrict__ ahat_t, uint32_t am, const E* __restrict__ what_t, E* __restrict__ partial,
-                    uint32_t m, uint32_t b_pad, uint32_t n, uint32_t splits, uint32_t kappa, uint32_t q) {
+LC_D void mac_quad_items(const E* __restrict__ ahat_t, uint32_t am, const E* __restrict__ what_t,
+                         E* __restrict__ partial, uint32_t m, uint32_t b_pad, uint32_t n, uint32_t splits,
+                         uint32_t kappa, uint32_t q, size_t first, size_t stride) {
   const uint32_t npair = (kappa + 1) / 2, nquad = b_pad / 4;
   const size_t total = (size_t)splits * n * nquad * npair;
-  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
-       idx += (size_t)gridDim.x * blockDim.x) {
+  for (size_t idx = first; idx < total; idx += stride) {
     const uint32_t ip = idx % npair;
     const uint32_t bq = (idx / npair) % nquad;
     const uint32_t t = (idx / ((size_t)npair * nquad)) % n;
@@ -354,14 +366,21 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+template <class E>
+__global__ void __launch_bounds__(256)
+    mac_quad_kernel(const E* __restrict__ ahat_t, uint32_t am, const E* __restrict__ what_t, E* __restrict__ partial,
+                    uint32_t m, uint32_t b_pad, uint32_t n, uint32_t splits, uint32_t kappa, uint32_t q) {
+  mac_quad_items<E>(ahat_t, am, what_t, partial, m, b_pad, n, splits, kappa, q,
+                    blockIdx.x * (size_t)blockDim.x + threadIdx.x, (size_t)gridDim.x * blockDim.x);
+}
+
 // Small-batch product: one thread per (split, t, i, b).
 template <class E>
-__global__ void mac_small_kernel(const E* __restrict__ ahat_t, uint32_t am, const E* __restrict__ what_t,
-                                 E* __restrict__ partial, uint32_t m, uint32_t b_pad, uint32_t n,
-                                 uint32_t splits, uint32_t kappa, uint32_t batch, uint32_t q) {
+LC_D void mac_small_items(const E* __restrict__ ahat_t, uint32_t am, const E* __restrict__ what_t,
+                          E* __restrict__ partial, uint32_t m, uint32_t b_pad, uint32_t n, uint32_t splits,
+                          uint32_t kappa, uint32_t batch, uint32_t q, size_t first, size_t stride) {
   const size_t total = (size_t)splits * n * kappa * batch;
-  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
-       idx += (size_t)gridDim.x * blockDim.x) {
+  for (size_t idx = first; idx < total; idx += stride) {
     const uint32_t b = idx % batch;
     const uint32_t i = (idx / batch) % kappa;
     const uint32_t t = (idx / ((size_t)batch * kappa)) % n;
@@ -373,6 +392,14 @@ __global__ void mac_small_kernel(const E* __restrict__ ahat_t, uint32_t am, cons
       mac<E>(acc, ahat_t[((size_t)t * am + j) * kIPad + i], what_t[((size_t)t * m + j) * b_pad + b]);
     partial[(((size_t)split * n + t) * kIPad + i) * b_pad + b] = acc_reduce<E>(acc, q);
   }
+}
+
+template <class E>
+__global__ void mac_small_kernel(const E* __restrict__ ahat_t, uint32_t am, const E* __restrict__ what_t,
+                                 E* __restrict__ partial, uint32_t m, uint32_t b_pad, uint32_t n,
+                                 uint32_t splits, uint32_t kappa, uint32_t batch, uint32_t q) {
+  mac_small_items<E>(ahat_t, am, what_t, partial, m, b_pad, n, splits, kappa, batch, q,
+                     blockIdx.x * (size_t)blockDim.x + threadIdx.x, (size_t)gridDim.x * blockDim.x);
 }
 
 // ------------------------------------------------------------------ single-launch commit
@@ -522,6 +549,168 @@ __global__ void reduce_partials_kernel(const E* __restrict__ partial, E* __restr
     for (uint32_t sp = 0; sp < splits; ++sp)
       s = Field<E>::add(s, partial[(((size_t)sp * n + t) * kIPad + i) * b_pad + b], q);
     chat[idx] = s;
+  }
+}
+
+// ------------------------------------------------------------------ products, split sum and inverse NTT in one launch
+//
+// The staged form's last three launches -- the products with K split across
+// CTAs, the modular sum of the splits, the batched inverse NTT -- as one
+// cooperative kernel, i.e. the whole of ajtai.rs:139-150 after the witness
+// transforms, in three phases separated by grid barriers (bounded spins on a
+// counter zeroed in the stream before the launch; the cooperative launch
+// makes every CTA resident): (1) the product items of the shape's form
+// (tiled, quad or small) over the persistent grid, partial[split][t][i][b];
+// (2) every thread of the grid sums the splits of some outputs into
+// Chat[b][i][t]; (3) groups of 32 rows (b, i) are loaded into shared memory,
+// inverse-transformed there and written straight to out[b][i][..].
+enum : int { kFormTiled = 0, kFormQuad = 1, kFormSmall = 2 };
+constexpr uint32_t kInttRows = 32;  // rows (b, i) per phase-3 item
+
+struct MacInttParams {
+  const void* ahat_t;
+  const void* what_t;
+  void* partial;
+  void* chat;
+  void* out;
+  const void* twi;
+  uint32_t am, m, b_pad, n, splits, kappa, batch, q, qinv, btiles;
+  uint32_t* err;
+  unsigned int* barrier;
+};
+
+template <class A, int LOG_N, int LOG_V, int JB, int FORM>
+struct MacInttCfg {
+  using E = typename A::T;
+  using Tw = typename A::Tw;
+  using G = Geo<LOG_N, LOG_V>;
+  static constexpr int NT = 256;
+  static constexpr size_t PH1 = FORM == kFormTiled ? MacCfg<E, JB>::SMEM : 0;  // stages + barriers
+  static constexpr size_t OFF2 = (PH1 + 127) / 128 * 128;
+  static constexpr size_t TWI = ((size_t)G::inv_entries() * sizeof(Tw) + 15) / 16 * 16;
+  static constexpr int SS = WitnessSlotStride<A, LOG_N>::value;
+  static constexpr size_t SMEM = OFF2 + TWI + (size_t)kInttRows * SS * sizeof(E);
+  static constexpr int GROUPS = NT / G::T;
+  static_assert(kInttRows % GROUPS == 0, "whole transform passes");
+};
+
+// Every CTA arrives once per barrier (the `round`-th barrier of the launch
+// waits for round * gridDim arrivals); false if the others did not all arrive
+// within the spin bound (the error word is set).
+LC_D bool grid_barrier(unsigned int* ctr, uint32_t round, uint32_t* err) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();  // this CTA's writes are visible before it arrives
+    atomicAdd(ctr, 1u);
+    const unsigned int target = round * gridDim.x;
+    // polls back off from 64 ns to 2 us, so that CTAs which finished early do
+    // not flood the counter's L2 line while the others still load; at most
+    // 2^20 polls (about two seconds)
+    bool ok = false;
+    uint32_t ns = 64;
+    for (uint32_t i = 0; i < (1u << 20); ++i) {
+      if (*reinterpret_cast<volatile unsigned int*>(ctr) >= target) {
+        ok = true;
+        break;
+      }
+      __nanosleep(ns);
+      ns = ns < 2048 ? 2 * ns : ns;
+    }
+    __threadfence();
+    if (!ok) record_error(err, LC_DEVERR_TIMEOUT);
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+template <class A, int LOG_N, int LOG_V, int JB, int FORM>
+__global__ void __launch_bounds__(256, 2) commit_mac_intt_kernel(const __grid_constant__ MacInttParams p) {
+  using C = MacInttCfg<A, LOG_N, LOG_V, JB, FORM>;
+  using E = typename A::T;
+  using Tw = typename A::Tw;
+  using G = typename C::G;
+  constexpr int N = G::N, SS = C::SS;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const E* ahat = static_cast<const E*>(p.ahat_t);
+  const E* what = static_cast<const E*>(p.what_t);
+  E* part = static_cast<E*>(p.partial);
+  E* chat = static_cast<E*>(p.chat);
+  const int tid = threadIdx.x;
+  const size_t gtid = blockIdx.x * (size_t)blockDim.x + tid, gthreads = (size_t)gridDim.x * blockDim.x;
+
+  // ---- phase 1: the product items
+  bool ok = true;
+  if constexpr (FORM == kFormTiled) {
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + 2 * MacCfg<E, JB>::STAGE);
+    if (tid == 0) {
+      mbar_init(&bar[0], 1);
+      mbar_init(&bar[1], 1);
+      fence_mbar_init();
+    }
+    __syncthreads();
+    uint32_t parity = 0;
+    const uint32_t items = p.n * p.btiles * p.splits;
+    for (uint32_t it = blockIdx.x; it < items && ok; it += gridDim.x) {
+      const uint32_t t = it % p.n, rest = it / p.n;
+      ok = mac_tile<E, JB>(ahat, p.am, what, part, p.m, p.b_pad, p.n, p.splits, p.q, p.err, t, rest % p.btiles,
+                           rest / p.btiles, smem_raw, bar, parity);
+    }
+  } else if constexpr (FORM == kFormQuad) {
+    mac_quad_items<E>(ahat, p.am, what, part, p.m, p.b_pad, p.n, p.splits, p.kappa, p.q, gtid, gthreads);
+  } else {
+    mac_small_items<E>(ahat, p.am, what, part, p.m, p.b_pad, p.n, p.splits, p.kappa, p.batch, p.q, gtid,
+                       gthreads);
+  }
+  // a CTA whose products timed out still arrives, so no other CTA waits on it
+  if (!grid_barrier(p.barrier, 1, p.err)) return;
+
+  // ---- phase 2: Chat[b][i][t] = sum over the splits, every thread of the grid
+  const size_t outs = (size_t)p.batch * p.kappa * N;
+  for (size_t idx = gtid; idx < outs; idx += gthreads) {
+    const uint32_t t = idx % N, i = (idx / N) % p.kappa;
+    const uint32_t b = (uint32_t)(idx / ((size_t)N * p.kappa));
+    const E* src = part + ((size_t)t * kIPad + i) * p.b_pad + b;
+    const size_t sstride = (size_t)N * kIPad * p.b_pad;
+    E s0 = 0, s1 = 0, s2 = 0, s3 = 0;  // four loads in flight
+    uint32_t sp = 0;
+    for (; sp + 4 <= p.splits; sp += 4) {
+      const E v0 = __ldcg(src + sp * sstride), v1 = __ldcg(src + (sp + 1) * sstride);
+      const E v2 = __ldcg(src + (sp + 2) * sstride), v3 = __ldcg(src + (sp + 3) * sstride);
+      s0 = Field<E>::add(s0, v0, p.q);
+      s1 = Field<E>::add(s1, v1, p.q);
+      s2 = Field<E>::add(s2, v2, p.q);
+      s3 = Field<E>::add(s3, v3, p.q);
+    }
+    for (; sp < p.splits; ++sp) s0 = Field<E>::add(s0, __ldcg(src + sp * sstride), p.q);
+    chat[idx] = Field<E>::add(Field<E>::add(s0, s1, p.q), Field<E>::add(s2, s3, p.q), p.q);
+  }
+  if (!grid_barrier(p.barrier, 2, p.err)) return;
+  if (*reinterpret_cast<volatile uint32_t*>(p.err) != 0) return;  // some CTA failed: outputs are not formed
+
+  // ---- phase 3: inverse transforms of 32 rows (b, i) per item, into the output
+  Tw* twi = reinterpret_cast<Tw*>(smem_raw + C::OFF2);
+  E* slots = reinterpret_cast<E*>(smem_raw + C::OFF2 + C::TWI);
+  for (int i = tid; i < G::inv_entries(); i += C::NT) twi[i] = static_cast<const Tw*>(p.twi)[i];
+  const A ar = make_arith_q<A>(p.q, p.qinv);
+  const int grp = tid / G::T;
+  const uint32_t lt = (uint32_t)(tid % G::T);
+  const uint32_t rows = p.batch * p.kappa;
+  E* out = static_cast<E*>(p.out);
+  for (uint32_t r0 = blockIdx.x * kInttRows; r0 < rows; r0 += gridDim.x * kInttRows) {
+    const uint32_t nr = min(kInttRows, rows - r0);
+    __syncthreads();  // twiddles written; the previous item's slots are read out
+    for (uint32_t e = tid; e < kInttRows * N; e += C::NT) {
+      const uint32_t rr = e / N, c = e % N;
+      slots[rr * SS + c] = rr < nr ? __ldcg(chat + (size_t)(r0 + rr) * N + c) : E(0);
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (uint32_t base = 0; base < kInttRows; base += C::GROUPS)
+      transform_slot<A, LOG_N, LOG_V, true>(slots + (base + grp) * SS, twi, ar, lt);
+    __syncthreads();
+    for (uint32_t e = tid; e < nr * N; e += C::NT) out[(size_t)r0 * N + e] = slots[(e / N) * SS + e % N];
   }
 }
 
@@ -675,6 +864,106 @@ static int witness_ntt(lc_ajtai_key* key, const S* w, size_t batch, uint32_t b_p
   return LC_ERR_INVALID_ARGUMENT;
 }
 
+// One cooperative launch: products of `form`, split sums, inverse transforms.
+template <class A, int LOG_N, int LOG_V, int FORM>
+static int launch_mac_intt(lc_ajtai_key* key, size_t batch, uint32_t b_pad, uint32_t splits, uint32_t btiles,
+                           void* out, cudaStream_t st) {
+  using E = typename A::T;
+  constexpr int JB = sizeof(E) == 8 ? 16 : 32;
+  using C = MacInttCfg<A, LOG_N, LOG_V, JB, FORM>;
+  auto kern = commit_mac_intt_kernel<A, LOG_N, LOG_V, JB, FORM>;
+  static std::atomic<uint64_t> attr_done{0};
+  cudaError_t e = smem_attr_once(attr_done, kern, C::SMEM);
+  if (e != cudaSuccess) return map_cuda(e);
+  if (!key->d_grid) {
+    if (cudaMalloc(&key->d_grid, 256) != cudaSuccess) {
+      cudaGetLastError();
+      return LC_ERR_OUT_OF_MEMORY;
+    }
+  }
+  e = cudaMemsetAsync(key->d_grid, 0, sizeof(unsigned int), st);
+  if (e != cudaSuccess) return map_cuda(e);
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, C::NT, C::SMEM);
+  if (e != cudaSuccess) return map_cuda(e);
+  if (per_sm < 1) return LC_ERR_UNSUPPORTED;
+  const uint32_t n = key->n, kappa = key->k;
+  const size_t resident = (size_t)per_sm * device_sm_count();
+  if (FORM == kFormTiled) {
+    // enough K splits for at least four waves of the resident grid, so the
+    // last, partly filled wave is short (at least 64 ring elements per item)
+    const size_t per_split = (size_t)n * btiles;
+    const size_t want = (4 * resident + per_split - 1) / per_split;
+    splits = (uint32_t)std::max<size_t>(
+        splits, std::min<size_t>(want, std::max<uint32_t>(1, key->m / 64)));
+    const int rc = grow(&key->d_partial, &key->partial_bytes, (size_t)splits * n * kIPad * b_pad * sizeof(E));
+    if (rc) return rc;
+  }
+  size_t work1;
+  if (FORM == kFormTiled)
+    work1 = (size_t)n * btiles * splits;
+  else if (FORM == kFormQuad)
+    work1 = ((size_t)splits * n * (b_pad / 4) * ((kappa + 1) / 2) + C::NT - 1) / C::NT;
+  else
+    work1 = ((size_t)splits * n * kappa * batch + C::NT - 1) / C::NT;
+  const size_t work2 = ((size_t)batch * kappa + kInttRows - 1) / kInttRows;
+  const size_t grid = std::max<size_t>(1, std::min<size_t>(resident, std::max(work1, work2)));
+  MacInttParams prm{};
+  prm.ahat_t = key->d_ahat_t;
+  prm.what_t = key->d_what_t;
+  prm.partial = key->d_partial;
+  prm.chat = key->d_chat;
+  prm.out = out;
+  prm.twi = key->plan->d_tw_inv;
+  prm.am = key->a_m;
+  prm.m = key->m;
+  prm.b_pad = b_pad;
+  prm.n = n;
+  prm.splits = splits;
+  prm.kappa = kappa;
+  prm.batch = (uint32_t)batch;
+  prm.q = key->plan->q[0];
+  prm.qinv = key->plan->qinv[0];
+  prm.btiles = btiles;
+  prm.err = key->d_err;
+  prm.barrier = key->d_grid;
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(C::NT);
+  cfg.dynamicSmemBytes = C::SMEM;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return map_cuda(cudaLaunchKernelEx(&cfg, kern, prm));
+}
+
+template <class A, int FORM>
+static int mac_intt_as(lc_ajtai_key* key, size_t batch, uint32_t b_pad, uint32_t splits, uint32_t btiles, void* out,
+                       cudaStream_t st) {
+  switch (key->log_n) {
+    case 6: return launch_mac_intt<A, 6, 3, FORM>(key, batch, b_pad, splits, btiles, out, st);
+    case 7: return launch_mac_intt<A, 7, 4, FORM>(key, batch, b_pad, splits, btiles, out, st);
+    case 8: return launch_mac_intt<A, 8, 4, FORM>(key, batch, b_pad, splits, btiles, out, st);
+    default: return LC_ERR_UNSUPPORTED;
+  }
+}
+
+template <class E, int FORM>
+static int mac_intt(lc_ajtai_key* key, size_t batch, uint32_t b_pad, uint32_t splits, uint32_t btiles, void* out,
+                    cudaStream_t st) {
+  const PlanKind kind = key->plan->kind;
+  if constexpr (std::is_same<E, uint64_t>::value) {
+    if (kind == PlanKind::Goldilocks) return mac_intt_as<Goldilocks, FORM>(key, batch, b_pad, splits, btiles, out, st);
+  } else {
+    if (kind == PlanKind::U32Lazy) return mac_intt_as<ShoupLazy, FORM>(key, batch, b_pad, splits, btiles, out, st);
+    if (kind == PlanKind::U32Mont) return mac_intt_as<MontCanon, FORM>(key, batch, b_pad, splits, btiles, out, st);
+  }
+  return LC_ERR_UNSUPPORTED;
+}
+
 template <class E>
 static int commit_core(lc_ajtai_key* key, size_t batch, uint32_t b_pad, void* out, cudaStream_t st) {
   const uint32_t n = key->n, m = key->m, kappa = key->k;
@@ -705,6 +994,17 @@ static int commit_core(lc_ajtai_key* key, size_t batch, uint32_t b_pad, void* ou
   if (rc) return rc;
   rc = grow(&key->d_chat, &key->chat_bytes, (size_t)batch * kappa * n * sizeof(E));
   if (rc) return rc;
+  // the products, their split sums and the inverse transforms in one launch:
+  // by default for the smallest batches (at most 3 witnesses), where it
+  // measured faster than the three launches below; for every form when the
+  // key asks for it (lc_ajtai_key_set_fused(key, 2)); never with 0
+  const int form = tiled ? kFormTiled : quad ? kFormQuad : kFormSmall;
+  if (key->fused && key->log_n >= 6 && key->log_n <= 8 && (key->fused == 2 || form == kFormSmall)) {
+    rc = form == kFormTiled ? mac_intt<E, kFormTiled>(key, batch, b_pad, splits, btiles, out, st)
+         : form == kFormQuad ? mac_intt<E, kFormQuad>(key, batch, b_pad, splits, btiles, out, st)
+                             : mac_intt<E, kFormSmall>(key, batch, b_pad, splits, btiles, out, st);
+    if (rc != LC_ERR_UNSUPPORTED) return rc;
+  }
   const E* ahat = reinterpret_cast<const E*>(key->d_ahat_t);
   const E* what = reinterpret_cast<const E*>(key->d_what_t);
   E* part = reinterpret_cast<E*>(key->d_partial);
@@ -1050,7 +1350,7 @@ LC_API int lc_ajtai_key_create_ex(const lc_ntt_plan* plan, uint32_t k, uint32_t 
 LC_API void lc_ajtai_key_destroy(lc_ajtai_key* key) {
   if (!key) return;
   if (key->owns_ahat && key->d_ahat_t) cudaFree(key->d_ahat_t);
-  for (void* p : {key->d_what_t, key->d_partial, key->d_chat, key->d_wtmp, key->d_fused, key->d_in,
+  for (void* p : {key->d_what_t, key->d_partial, key->d_chat, key->d_wtmp, key->d_fused, (void*)key->d_grid, key->d_in,
                   key->d_out, (void*)key->d_err})
     if (p) cudaFree(p);
   if (key->host_stream) cudaStreamDestroy(key->host_stream);
@@ -1101,12 +1401,12 @@ LC_API int lc_ajtai_key_set_engine(lc_ajtai_key* key, int engine) {
 LC_API int lc_ajtai_key_get_engine(const lc_ajtai_key* key) { return key ? key->engine : -1; }
 
 LC_API int lc_ajtai_key_set_fused(lc_ajtai_key* key, int enable) {
-  if (!key || (enable != 0 && enable != 1)) return LC_ERR_INVALID_ARGUMENT;
-  key->fused = enable == 1;
+  if (!key || enable < 0 || enable > 2) return LC_ERR_INVALID_ARGUMENT;
+  key->fused = enable;
   return LC_OK;
 }
 
-LC_API int lc_ajtai_key_get_fused(const lc_ajtai_key* key) { return key ? (key->fused ? 1 : 0) : -1; }
+LC_API int lc_ajtai_key_get_fused(const lc_ajtai_key* key) { return key ? key->fused : -1; }
 
 LC_API int lc_ajtai_key_set_slot_products(lc_ajtai_key* key, int mode) {
   if (!key || (mode != LC_PRODUCTS_INT64 && mode != LC_PRODUCTS_TENSOR)) return LC_ERR_INVALID_ARGUMENT;
@@ -1126,7 +1426,8 @@ uint64_t commit_scratch_signature(const lc_ajtai_key* key) {
   uint64_t h = 1469598103934665603ull;
   for (uintptr_t v : {(uintptr_t)key->d_what_t, (uintptr_t)key->d_partial, (uintptr_t)key->d_chat,
                       (uintptr_t)key->d_wtmp, (uintptr_t)key->what_bytes, (uintptr_t)key->partial_bytes,
-                      (uintptr_t)key->chat_bytes, (uintptr_t)key->wtmp_bytes, (uintptr_t)key->d_fused})
+                      (uintptr_t)key->chat_bytes, (uintptr_t)key->wtmp_bytes, (uintptr_t)key->d_fused,
+                      (uintptr_t)key->d_grid})
     h = (h ^ (uint64_t)v) * 1099511628211ull;
   return h;
 }

@@ -111,7 +111,8 @@ struct lc_ajtai_key {
   size_t wtmp_bytes = 0;
   void* d_fused = nullptr;  // single-launch commit: ticket (16 B), then 128-bit accumulators
   size_t fused_bytes = 0;
-  bool fused = true;        // small commits as one launch (lc_ajtai_key_set_fused)
+  unsigned int* d_grid = nullptr;  // grid-barrier counter of the one-launch products + inverse NTT
+  int fused = 1;            // one-launch forms: 0 never, 1 where faster, 2 every form (lc_ajtai_key_set_fused)
   bool last_fused = false;  // the last commit on this key ran as one launch
   int slot_products = LC_PRODUCTS_TENSOR;  // lc_ajtai_key_set_slot_products
   void* d_in = nullptr;  // host-API staging

@@ -139,7 +139,7 @@ def test_fused_switch_arguments():
     _, key = gl_case(6, 2, 8, seed=1)
     L = _lib.lib()
     assert L.lc_ajtai_key_get_fused(key.handle) == 1
-    assert L.lc_ajtai_key_set_fused(key.handle, 2) == _lib.LC_ERR_INVALID_ARGUMENT
+    assert L.lc_ajtai_key_set_fused(key.handle, 3) == _lib.LC_ERR_INVALID_ARGUMENT
     assert L.lc_ajtai_key_set_fused(None, 0) == _lib.LC_ERR_INVALID_ARGUMENT
     assert L.lc_ajtai_key_get_fused(None) == -1
     assert L.lc_ajtai_key_set_fused(key.handle, 0) == 0

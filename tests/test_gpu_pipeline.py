@@ -56,11 +56,16 @@ def check_outputs(pipe, want):
     assert np.array_equal(pipe.crt_ntt.cpu().numpy().view(np.uint32), crt)
 
 
-@pytest.mark.parametrize("use_graph", [False, True])
-def test_fold_pipeline_small(use_graph):
+@pytest.mark.parametrize("use_graph,products", [(False, GoldilocksAjtaiKey.PRODUCTS_TENSOR),
+                                                (True, GoldilocksAjtaiKey.PRODUCTS_TENSOR),
+                                                (True, GoldilocksAjtaiKey.PRODUCTS_INT64)])
+def test_fold_pipeline_small(use_graph, products):
+    """The integer-product form runs its products, split sums and inverse
+    transforms as one cooperative launch, captured in the graph too."""
     kappa, m = 16, 300
     A = synth.synth_gl(31, 0, kappa * m * 64)
     key = GoldilocksAjtaiKey(6, kappa, m, A.reshape(kappa, m, 64))
+    key.slot_products = products
     crt = NttTables(CRT_SET_30BIT, 6)
     pipe = FoldPipeline(key, crt, use_graph=use_graph)
     z = synth.synth_gl(31, 1, m * 64)
