@@ -695,6 +695,17 @@ __global__ void __launch_bounds__(kTpThreads, 1)
     const uint32_t boff = (k >> 3) * C::B_ATOM;  // swizzle atom of the chunk
     const uint32_t kc = k & 7;
     const int first_job = kTpJobs * (int)it.blk + (int)(k * J);
+    // R[jb .. jb + 16] (job counts) and Rp[jb .. jb + 15] (row starts) of a
+    // stage, loaded one stage ahead so their latency hides behind the wait
+    // for the copies two stages back
+    auto offsets = [&](int s, uint64_t& r, uint64_t& rp) {
+      const uint32_t jb = j0 + kTpRows * s + 16 * g;
+      const bool in_r = s < nst && lane <= 16 && jb + lane <= L.n_max;
+      r = in_r ? __ldg(L.R + jb + lane) : 0;
+      rp = in_r ? __ldg(L.Rp + jb + lane) : 0;
+    };
+    uint64_t rl, rpl;
+    offsets(0, rl, rpl);
     bool ok = true;
     for (int s = 0; s < nst; ++s) {
       if (*abort_flag) {
@@ -707,10 +718,8 @@ __global__ void __launch_bounds__(kTpThreads, 1)
         break;
       }
       const uint32_t jb = j0 + kTpRows * s + 16 * g;
-      // R[jb .. jb + 16] (job counts) and Rp[jb .. jb + 15] (row starts)
-      const bool in_r = lane <= 16 && jb + lane <= L.n_max;
-      const uint64_t rl = in_r ? __ldg(L.R + jb + lane) : 0;
-      const uint64_t rpl = in_r ? __ldg(L.Rp + jb + lane) : 0;
+      uint64_t rl_next, rpl_next;
+      offsets(s + 1, rl_next, rpl_next);
       const uint32_t sb = smem_u32(stage(s)) + C::A_BYTES + boff;
 #pragma unroll
       for (int rr = 0; rr < 16; rr += RPI) {
@@ -730,6 +739,8 @@ __global__ void __launch_bounds__(kTpThreads, 1)
         fence_proxy_async_smem();
         mbar_arrive(&full[(s - kTpLag) % kTpStages]);
       }
+      rl = rl_next;
+      rpl = rpl_next;
     }
     cp_async_wait<0>();
     fence_proxy_async_smem();
