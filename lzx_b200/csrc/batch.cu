@@ -525,6 +525,294 @@ __global__ void __launch_bounds__(kBatchThreads, sizeof(E) == 8 ? 2 : 3)
   }
 }
 
+// ---- launch 1 on the tensor cores: witness transforms of u32 lanes, d = 128 / 256
+//
+// For q < 2^30 and ring degree d the forward transform of a digit row w
+// (natural order, out[t] = sum_c w_c psi^((2t+1) c), ntt.rs:118-146) is the
+// fixed product What[t] = sum_c V[t][c] w[c] (mod q), V[t][c] = psi^((2t+1) c).
+// With V's residues split into 4 byte limbs it is 4 exact INT8 GEMMs,
+//   D[p][(t,l)] = sum_c w_p[c] V_l[t][c]   (s8 x u8 -> s32, |D| <= d 128 255 < 2^23),
+// folded per output as v = sum_l 2^(8l) D (|v| < 2^48), u = v + q 2^19 > 0,
+// two folds by 2^30 == 2^30 - q (mod q) and one conditional subtract.  A tile
+// is 128 consecutive staircase polynomials of a lane (M = 128), gathered from
+// the jobs' digit rows by four warps with cp.async into the K-major
+// 128-byte-swizzled layout (K = d bytes in 128-byte atoms); N = the 4d
+// columns (t, l) in passes of 256 (64 slots), each pass's V-limb rows loaded by
+// TMA from the lane's [4d][d] image in global memory (L2-resident); two TMEM
+// accumulators of 256 columns alternate between passes, so four epilogue
+// warps fold pass k and store What[t][Rp[j] + b] while pass k + 1 runs.
+// EW epilogue warps (8 or 16; warp w reads TMEM lanes 32 (w % 4).. and a
+// 256 / (EW / 4)-column share of each pass), then 4 gather warps, the TMA
+// warp and the MMA warp.
+template <int EW>
+struct TwCfg {
+  static_assert(EW == 8 || EW == 16, "epilogue warps");
+  static constexpr int THREADS = 32 * (EW + 6);
+  static constexpr int GATHER = EW, TMA = EW + 4, MMA = EW + 5;
+  static constexpr uint32_t COLS = 256 / (EW / 4);  // TMEM columns per epilogue warp and pass
+};
+constexpr int kTwEpi = 8;
+constexpr int kTwRows = 128;          // polynomials per tile
+constexpr int kTwABytes = kTwRows * 256;  // A stage (d <= 256)
+constexpr int kTwBBytes = 256 * 256;      // B stage: 256 rows (t, l) x d <= 256
+constexpr int kTwOffB = 2 * kTwABytes;
+constexpr int kTwOffInfo = kTwOffB + 2 * kTwBBytes;          // per A stage: 128 x u64 destinations
+constexpr int kTwOffBar = kTwOffInfo + 2 * kTwRows * 8;
+constexpr size_t kTwSmem = 1024 + kTwOffBar + 256;
+static_assert(kTwSmem <= 227 * 1024, "shared memory");
+
+struct TwItem {
+  uint32_t lane, tile, jlo, pad;
+};
+
+// D = s32, A = s8, B = u8, both K-major, N = 256, M = 128
+constexpr uint32_t kTwIdesc = (2u << 4) | (1u << 7) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
+
+// OR of `v` over the `count` threads of named barrier `id` (all of them
+// receive it): keeps a warp group's loop decisions uniform.
+LC_D bool named_bar_or(bool v, uint32_t id, uint32_t count) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.or.pred q, %2, %3, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(id), "r"(count)
+      : "memory");
+  return r != 0;
+}
+
+// v (|v| < 2^48) mod q, canonical, for the q tw_fold_exact accepts (2^30 - c,
+// c <= 2^20): u = v + q 2^19 in (0, 2^50), then two folds by 2^30 == c
+LC_D uint32_t tw_fold(int64_t v, uint32_t q, uint32_t c) {
+  const uint64_t u = (uint64_t)(v + ((int64_t)q << 19));
+  const uint64_t x = (uint64_t)(uint32_t)(u >> 30) * c + ((uint32_t)u & 0x3FFFFFFFu);  // < 2^40 + 2^30
+  const uint32_t y = (uint32_t)(x >> 30) * c + ((uint32_t)x & 0x3FFFFFFFu);            // < 2q
+  return y >= q ? y - q : y;
+}
+
+template <int EW>
+__global__ void __launch_bounds__(TwCfg<EW>::THREADS, 1)
+    lane_witness_tc_kernel(const TwItem* __restrict__ items, uint64_t nitems, const LaneDesc* __restrict__ lanes,
+                           const SubJob* __restrict__ subs, const CUtensorMap* __restrict__ vmaps, uint32_t* err) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char* base =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* info = reinterpret_cast<uint64_t*>(base + kTwOffInfo);  // [2][128] staircase offset, ~0 = none
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + kTwOffBar);
+  uint64_t* a_full = bars;        // [2] 128 gather threads
+  uint64_t* a_free = bars + 2;    // [2] MMA commit + EW epilogue warps
+  uint64_t* b_full = bars + 4;    // [2] V rows landed (tx)
+  uint64_t* b_empty = bars + 6;   // [2] MMA commit
+  uint64_t* acc_full = bars + 8;  // [2] MMA commit
+  uint64_t* acc_empty = bars + 10;  // [2] EW epilogue warps
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 12);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 13);
+  uint64_t* done = bars + 14;     // every MMA issued has finished
+  using Cfg = TwCfg<EW>;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  if (tid == 0) {
+    mbar_init(done, 1);
+    for (int s = 0; s < 2; ++s) {
+      mbar_init(&a_full[s], 128);
+      mbar_init(&a_free[s], 1 + EW);
+      mbar_init(&b_full[s], 1);
+      mbar_init(&b_empty[s], 1);
+      mbar_init(&acc_full[s], 1);
+      mbar_init(&acc_empty[s], EW);
+    }
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == Cfg::MMA) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(512));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint64_t n_my = nitems > blockIdx.x ? (nitems - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  auto item_at = [&](uint64_t i) { return items[blockIdx.x + i * gridDim.x]; };
+  auto fail = [&]() {
+    record_error(err, LC_DEVERR_TIMEOUT);
+    *abort_flag = 1;
+  };
+  auto a_stage = [&](uint64_t i) { return base + (i & 1) * kTwABytes; };
+  auto b_stage = [&](uint64_t g) { return base + kTwOffB + (g & 1) * kTwBBytes; };
+  int64_t tma_last = -1;    // TMA thread: last pass index loaded
+
+  if (warp == Cfg::TMA) {
+    // ---------------- TMA: V-limb rows of each pass
+    if (lane == 0) {
+      uint64_t g = 0;
+      for (uint64_t i = 0; i < n_my && !*abort_flag; ++i) {
+        const TwItem it = item_at(i);
+        const uint32_t d = 1u << lanes[it.lane].log_n, passes = d / 64;
+        const CUtensorMap* vm = vmaps + it.lane;
+        for (uint32_t k = 0; k < passes && !*abort_flag; ++k, ++g) {
+          if (g >= 2 && !mbar_wait(&b_empty[g & 1], (uint32_t)(((g - 2) >> 1) & 1))) {
+            fail();
+            break;
+          }
+          mbar_arrive_expect_tx(&b_full[g & 1], 256 * d);
+          for (uint32_t kk = 0; kk < d / 128; ++kk)
+            tma_load_2d(b_stage(g) + kk * 32768, vm, (int)(kk * 128), (int)(k * 256), &b_full[g & 1]);
+          tma_last = (int64_t)g;
+        }
+      }
+    }
+  } else if (warp == Cfg::MMA) {
+    // ---------------- MMA issuer
+    if (lane == 0) {
+      uint64_t g = 0;
+      bool ok = true;
+      for (uint64_t i = 0; i < n_my && ok && !*abort_flag; ++i) {
+        const TwItem it = item_at(i);
+        const uint32_t d = 1u << lanes[it.lane].log_n, passes = d / 64;
+        if (!mbar_wait(&a_full[i & 1], (uint32_t)((i >> 1) & 1))) {
+          fail();
+          break;
+        }
+        const uint32_t aa = smem_u32(a_stage(i));
+        for (uint32_t k = 0; k < passes; ++k, ++g) {
+          if (!mbar_wait(&b_full[g & 1], (uint32_t)((g >> 1) & 1)) ||
+              (g >= 2 && !mbar_wait(&acc_empty[g & 1], (uint32_t)(((g - 2) >> 1) & 1)))) {
+            fail();
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t bb = smem_u32(b_stage(g));
+          for (uint32_t ks = 0; ks < d / 32; ++ks) {
+            const uint32_t off = (ks >> 2) * 16384u + (ks & 3) * 32u;
+            mma_i8(tmem + (uint32_t)(g & 1) * 256, umma_desc_sw128(aa + off),
+                   umma_desc_sw128(bb + (ks >> 2) * 32768u + (ks & 3) * 32u), kTwIdesc, ks > 0 ? 1u : 0u);
+          }
+          mma_commit(&acc_full[g & 1]);
+          mma_commit(&b_empty[g & 1]);
+        }
+        if (ok) mma_commit(&a_free[i & 1]);
+      }
+      mma_commit(done);
+      if (!mbar_wait(done, 0)) fail();
+    }
+  } else if (warp >= Cfg::GATHER) {
+    // ---------------- gather: row info (thread r = row r), then the digit rows
+    const int gt = tid - 32 * Cfg::GATHER;  // 0..127
+    for (uint64_t i = 0; i < n_my; ++i) {
+      // one decision for the four gather warps (they share named barrier 1)
+      bool timed_out = false;
+      if (!*abort_flag && i >= 2) timed_out = !mbar_wait(&a_free[i & 1], (uint32_t)(((i - 2) >> 1) & 1));
+      if (timed_out) fail();
+      if (named_bar_or(timed_out || *abort_flag, 1, 128)) break;
+      const TwItem it = item_at(i);
+      const LaneDesc& L = lanes[it.lane];
+      const uint32_t d = 1u << L.log_n;
+      uint64_t* inf = info + (i & 1) * kTwRows;
+      // row r: staircase polynomial p = 128 tile + r -> ring element j (R[j] <= p < R[j + 1]), job b
+      const uint64_t p = (uint64_t)it.tile * kTwRows + gt;
+      const int8_t* src = nullptr;
+      uint64_t dst = ~0ull;
+      if (p < L.S) {
+        uint32_t lo = it.jlo, hi = min(L.n_max, it.jlo + kTwRows);  // R[lo] <= p < R[hi]
+        while (hi - lo > 1) {
+          const uint32_t mid = (lo + hi) >> 1;
+          if (__ldg(L.R + mid) <= p) lo = mid; else hi = mid;
+        }
+        const uint32_t b = (uint32_t)(p - __ldg(L.R + lo));
+        src = subs[L.sub0 + b].w + (size_t)lo * d;
+        dst = __ldg(L.Rp + lo) + b;
+      }
+      inf[gt] = dst;
+      __shared__ const int8_t* s_src[kTwRows];
+      s_src[gt] = src;
+      asm volatile("bar.sync 1, 128;" ::: "memory");  // the four gather warps
+      const uint32_t cpr = d / 16;                 // 16-byte chunks per row
+      const uint32_t rpi = 128 / cpr;              // rows per pass of the 128 threads
+      const uint32_t c = (uint32_t)gt % cpr;
+      const uint32_t a = smem_u32(a_stage(i));
+      for (uint32_t r = (uint32_t)gt / cpr; r < kTwRows; r += rpi) {
+        const int8_t* sp = s_src[r];
+        const uint32_t dsto = a + (c >> 3) * 16384u + (r >> 3) * 1024u + (r & 7) * 128u + (((c & 7) ^ (r & 7)) << 4);
+        cp_async16_zfill(dsto, sp ? (const void*)(sp + c * 16) : (const void*)L.what, sp ? 16u : 0u);
+      }
+      cp_async_commit();
+      cp_async_wait<0>();
+      fence_proxy_async_smem();
+      asm volatile("bar.sync 1, 128;" ::: "memory");  // s_src is rewritten by the next tile
+      mbar_arrive(&a_full[i & 1]);
+    }
+    cp_async_wait<0>();
+  } else {
+    // ---------------- epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31
+    // (rows = polynomials) and columns COLS (w / 4) .. + COLS - 1 of each pass
+    const uint32_t quad = warp & 3, row = 32 * quad + lane, cbeg = (uint32_t)(warp >> 2) * Cfg::COLS;
+    uint64_t g = 0;
+    for (uint64_t i = 0; i < n_my; ++i) {
+      const TwItem it = item_at(i);
+      const LaneDesc& L = lanes[it.lane];
+      const uint32_t d = 1u << L.log_n, passes = d / 64, q = L.q, cq = (1u << 30) - q;
+      const size_t Sp = L.Sp;
+      bool stop = false;
+      // the gather's row table of this tile (its a_full phase; the stage is
+      // not refilled before this warp releases it)
+      const bool rows_ok = !*abort_flag && mbar_wait(&a_full[i & 1], (uint32_t)((i >> 1) & 1));
+      if (!__all_sync(0xffffffffu, rows_ok)) {
+        if (lane == 0) fail();
+        break;
+      }
+      const uint64_t dst = info[(i & 1) * kTwRows + row];
+      for (uint32_t k = 0; k < passes; ++k, ++g) {
+        const bool ok = !*abort_flag && mbar_wait(&acc_full[g & 1], (uint32_t)((g >> 1) & 1));
+        if (!__all_sync(0xffffffffu, ok)) {  // warp-uniform: the TMEM loads are .sync.aligned
+          if (lane == 0) fail();
+          stop = true;
+          break;
+        }
+        tc_fence_after();
+        // output slot t = 64 k + (cbeg + c0) / 4 + u, row dst of the staircase
+        uint32_t* what = reinterpret_cast<uint32_t*>(L.what) + (dst == ~0ull ? 0 : dst) +
+                         (size_t)(64 * k + cbeg / 4) * Sp;
+        const uint32_t taddr = tmem + ((32 * quad) << 16) + (uint32_t)(g & 1) * 256 + cbeg;
+#pragma unroll 1
+        for (uint32_t c0 = 0; c0 < Cfg::COLS; c0 += 32) {
+          uint32_t v0[16], v1[16];
+          tmem_ld16(taddr + c0, v0);
+          tmem_ld16(taddr + c0 + 16, v1);
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const uint32_t* x = u < 4 ? v0 + 4 * u : v1 + 4 * (u - 4);
+            const int64_t vv = (int64_t)(int32_t)x[0] + ((int64_t)(int32_t)x[1] << 8) +
+                               ((int64_t)(int32_t)x[2] << 16) + ((int64_t)(int32_t)x[3] << 24);
+            if (dst != ~0ull) *what = tw_fold(vv, q, cq);
+            what += Sp;
+          }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&acc_empty[g & 1]);
+      }
+      if (stop) break;
+      if (lane == 0) mbar_arrive(&a_free[i & 1]);
+    }
+  }
+  // ---------------- nothing in flight when TMEM and shared memory go
+  __syncthreads();
+  if (warp == Cfg::TMA && lane == 0) {
+    for (int64_t g = tma_last >= 1 ? tma_last - 1 : 0; g <= tma_last; ++g)
+      mbar_wait(&b_full[g & 1], (uint32_t)((g >> 1) & 1));
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == Cfg::MMA) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+  }
+}
+
 // ---- launch 2 on the tensor cores: lane products as exact byte-limb GEMMs
 //
 // C_t[i][b] = sum_j Ahat[t][j][i] * What[t][j][b] over j < n_b, with both
@@ -577,16 +865,6 @@ struct TpIdesc {
       (2u << 4) | (1u << 15) | (1u << 16) | ((uint32_t)(N >> 3) << 17) | ((128u >> 4) << 24);
 };
 
-// 16-byte global -> shared copy of `bytes` (0..16) source bytes, the rest zero
-// (src and dst 16-byte aligned; no byte is read when bytes = 0)
-LC_D void cp_async16_zfill(uint32_t dst, const void* src, uint32_t bytes) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
-}
-LC_D void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-LC_D void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
 
 template <int EB>
 __global__ void __launch_bounds__(kTpThreads, 1)
@@ -842,6 +1120,12 @@ struct lc_batch {
   uint64_t titems[2] = {0, 0};           // Goldilocks items, then u32 items
   std::vector<int32_t*> lane_tpart;
   std::vector<const uint32_t*> lane_tchunk0;
+  // tensor-core witness transforms (lane_witness_tc_kernel): u32 lanes with q < 2^30, d = 128 / 256
+  std::vector<uint8_t> lane_tw;            // per lane: its witness transforms run there
+  std::vector<std::pair<uint64_t, void*>> vimgs;  // V-limb images by (q << 16 | d)
+  CUtensorMap* d_vmaps = nullptr;
+  lc::TwItem* d_twitems = nullptr;
+  uint64_t twitems = 0;
   bool warmed = false, dirty = true;
   cudaStream_t cap = nullptr;
   cudaGraph_t graph = nullptr;
@@ -857,8 +1141,9 @@ static void batch_free(lc_batch* b) {
   for (void* p : {(void*)b->d_lanes, (void*)b->d_subs, (void*)b->d_R, (void*)b->d_itemj, (void*)b->d_what,
                   (void*)b->d_partial, (void*)b->d_counters, (void*)b->d_err, (void*)b->d_citem,
                   (void*)b->d_cblk, (void*)b->d_tpart, (void*)b->d_tchunk0, (void*)b->d_amaps,
-                  (void*)b->d_titems})
+                  (void*)b->d_titems, (void*)b->d_vmaps, (void*)b->d_twitems})
     if (p) cudaFree(p);
+  for (auto& v : b->vimgs) cudaFree(v.second);
   delete b;
 }
 
@@ -931,6 +1216,102 @@ static int batch_tensor_setup(lc_batch* b) {
   return map_cuda(cudaGetLastError());
 }
 
+static uint64_t mulmod64(uint64_t a, uint64_t b, uint64_t q) { return (uint64_t)((unsigned __int128)a * b % q); }
+static uint64_t powmod64(uint64_t a, uint64_t e, uint64_t q) {
+  uint64_t r = 1 % q;
+  for (a %= q; e; e >>= 1, a = mulmod64(a, a, q))
+    if (e & 1) r = mulmod64(r, a, q);
+  return r;
+}
+
+// The [4d rows (t, l)][d bytes c] image of V[t][c] = psi^((2t+1) c) mod q
+// split into byte limbs l, psi = g^((q - 1) >> (log d + 1)) as the plan's
+// forward transform uses (natural output order, ntt.rs:118-146).
+static void tw_image(uint64_t q, uint64_t g, uint32_t log_d, std::vector<uint8_t>& img) {
+  const uint32_t d = 1u << log_d;
+  const uint64_t psi = powmod64(g, (q - 1) >> (log_d + 1), q);
+  img.assign((size_t)4 * d * d, 0);
+  for (uint32_t t = 0; t < d; ++t) {
+    const uint64_t step = powmod64(psi, 2 * t + 1, q);
+    uint64_t v = 1;
+    for (uint32_t c = 0; c < d; ++c, v = mulmod64(v, step, q))
+      for (uint32_t l = 0; l < 4; ++l) img[((size_t)t * 4 + l) * d + c] = (uint8_t)(v >> (8 * l));
+  }
+}
+
+// Whether tw_fold is exact for q and ring degree d: the offset q 2^19 must
+// exceed the largest |v| = d 128 255 (1 + 2^8 + 2^16 + 2^24), c = 2^30 - q
+// at most 2^20, and after two folds by 2^30 == c the value below 2q (so q
+// close to 2^30, as the 30-bit CRT primes are; other q keep the CUDA cores).
+static bool tw_fold_exact(uint64_t q, uint32_t d) {
+  if (q >= (1ull << 30) || q < (1ull << 29)) return false;
+  const uint64_t vmax = (uint64_t)d * 128 * 255 * 16843009ull, off = q << 19;
+  if (off <= vmax) return false;
+  const uint64_t c = (1ull << 30) - q, m = (1ull << 30) - 1;
+  if (c > (1ull << 20)) return false;  // the second fold multiplies in 32 bits
+  const uint64_t umax = vmax + off;
+  const uint64_t xmax = (umax >> 30) * c + m;
+  const uint64_t ymax = (xmax >> 30) * c + m;
+  return ymax < 2 * q;
+}
+
+// Tensor-core witness transforms: per eligible lane a TMA map of its (q, d)
+// image and the tiles of 128 staircase polynomials with their first ring
+// element.  Lanes that cannot run there keep the CUDA-core transforms.
+static int batch_tw_setup(lc_batch* b, const std::vector<uint32_t>& plan_gen) {
+  EncodeTiledFn enc = encode_fn();
+  const size_t nl = b->lanes.size();
+  b->lane_tw.assign(nl, 0);
+  if (!enc || !nl) return LC_OK;
+  std::vector<CUtensorMap> maps(nl);
+  std::vector<TwItem> items;
+  for (size_t l = 0; l < nl; ++l) {
+    const LaneDesc& L = b->lanes[l];
+    if (L.kind != (uint32_t)PlanKind::U32Lazy || (L.log_n != 7 && L.log_n != 8) || L.S == 0) continue;
+    const uint32_t d = 1u << L.log_n;
+    if (!tw_fold_exact(L.q, d)) continue;
+    const uint64_t key = ((uint64_t)L.q << 16) | d;
+    void* img = nullptr;
+    for (auto& v : b->vimgs)
+      if (v.first == key) img = v.second;
+    if (!img) {
+      std::vector<uint8_t> h;
+      tw_image(L.q, plan_gen[l], L.log_n, h);
+      if (cudaMalloc(&img, h.size()) != cudaSuccess) {
+        cudaGetLastError();
+        return LC_ERR_OUT_OF_MEMORY;
+      }
+      cudaMemcpy(img, h.data(), h.size(), cudaMemcpyHostToDevice);
+      b->vimgs.push_back({key, img});
+    }
+    const cuuint64_t dims[2] = {d, (cuuint64_t)4 * d};
+    const cuuint64_t strides[1] = {d};
+    const cuuint32_t box[2] = {128, 256};
+    const cuuint32_t estr[2] = {1, 1};
+    if (enc(&maps[l], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, img, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      continue;
+    const std::vector<uint64_t>& R = b->R[l];
+    uint32_t j = 0;
+    for (uint64_t tile = 0; tile * kTwRows < L.S; ++tile) {
+      while (R[j + 1] <= tile * kTwRows) ++j;
+      items.push_back(TwItem{(uint32_t)l, (uint32_t)tile, j, 0});
+    }
+    b->lane_tw[l] = 1;
+  }
+  if (items.empty()) return LC_OK;
+  if (cudaMalloc(&b->d_vmaps, nl * sizeof(CUtensorMap)) != cudaSuccess ||
+      cudaMalloc(&b->d_twitems, items.size() * sizeof(TwItem)) != cudaSuccess) {
+    cudaGetLastError();
+    return LC_ERR_OUT_OF_MEMORY;
+  }
+  cudaMemcpy(b->d_vmaps, maps.data(), nl * sizeof(CUtensorMap), cudaMemcpyHostToDevice);
+  cudaMemcpy(b->d_twitems, items.data(), items.size() * sizeof(TwItem), cudaMemcpyHostToDevice);
+  b->twitems = items.size();
+  return map_cuda(cudaGetLastError());
+}
+
 // The lanes' partial pointers for the current product mode.
 static void batch_apply_products(lc_batch* b) {
   for (size_t l = 0; l < b->lanes.size(); ++l) {
@@ -982,7 +1363,8 @@ static int batch_layout(lc_batch* b) {
     LaneDesc& L = b->lanes[l];
     L.citem = b->d_citem + coff[l];
     L.cblk = b->d_cblk + coff[l];
-    const uint64_t items[3] = {(L.S + L.pb - 1) / L.pb, citem[coff[l] + L.nchunks], L.nb};
+    const bool tw = b->products == LC_PRODUCTS_TENSOR && b->tensor_ok && b->twitems && b->lane_tw[l];
+    const uint64_t items[3] = {tw ? 0 : (L.S + L.pb - 1) / L.pb, citem[coff[l] + L.nchunks], L.nb};
     for (int ph = 0; ph < 3; ++ph) {
       L.item0[ph] = base[ph];
       base[ph] += items[ph];
@@ -1024,6 +1406,14 @@ static int batch_launch(lc_batch* b, cudaStream_t st) {
     if (e != cudaSuccess) return map_cuda(e);
   }
   batch_kernel<0><<<grid, kBatchThreads, b->smem[0], st>>>(p);
+  if (b->products == LC_PRODUCTS_TENSOR && b->tensor_ok && b->twitems) {
+    static std::atomic<uint64_t> attr_tw{0};
+    e = smem_attr_once(attr_tw, lane_witness_tc_kernel<kTwEpi>, kTwSmem);
+    if (e != cudaSuccess) return map_cuda(e);
+    const unsigned tgrid = (unsigned)std::min<uint64_t>(b->twitems, (uint64_t)std::max(1, device_sm_count()));
+    lane_witness_tc_kernel<kTwEpi><<<tgrid, TwCfg<kTwEpi>::THREADS, kTwSmem, st>>>(b->d_twitems, b->twitems, b->d_lanes, b->d_subs,
+                                                                b->d_vmaps, b->d_err);
+  }
   if (b->products == LC_PRODUCTS_TENSOR && b->tensor_ok) {
     static std::atomic<uint64_t> attr8{0}, attr4{0};
     e = smem_attr_once(attr8, lane_products_tc_kernel<8>, TpCfg<8>::SMEM);
@@ -1084,6 +1474,7 @@ LC_API int lc_batch_create(const lc_commit_class* classes, uint32_t num_classes,
   std::vector<size_t> r_off, ij_off;
   size_t what_bytes = 0, partial_bytes = 0;
   std::vector<size_t> what_off, part_off;
+  std::vector<uint32_t> lane_gen;  // generator of each lane's modulus (for the V-limb images)
   // Goldilocks classes first, so each element type's product items are one range
   std::vector<uint32_t> corder;
   for (int pass = 0; pass < 2; ++pass)
@@ -1101,6 +1492,7 @@ LC_API int lc_batch_create(const lc_commit_class* classes, uint32_t num_classes,
       for (size_t g0 = 0; g0 < idx.size(); g0 += kLaneJobs) {
         const size_t g1 = std::min(idx.size(), g0 + (size_t)kLaneJobs);
         LaneDesc L{};
+        lane_gen.push_back(K->plan->generator[0]);
         L.kind = (uint32_t)K->plan->kind;
         L.log_n = K->log_n;
         L.q = K->plan->q[0];
@@ -1204,6 +1596,13 @@ LC_API int lc_batch_create(const lc_commit_class* classes, uint32_t num_classes,
     return rc;
   }
   if (b->titems[0] > 0x7FFFFFFFull || b->titems[1] > 0x7FFFFFFFull) b->tensor_ok = false;
+  if (b->tensor_ok) {
+    rc = batch_tw_setup(b, lane_gen);
+    if (rc) {
+      batch_free(b);
+      return rc;
+    }
+  }
   b->products = b->tensor_ok ? LC_PRODUCTS_TENSOR : LC_PRODUCTS_INT64;
   batch_apply_products(b);
   rc = batch_layout(b);
@@ -1248,7 +1647,8 @@ LC_API int lc_batch_get_config(const lc_batch* b, uint32_t* chunk, uint32_t* cta
 LC_API int lc_batch_info(const lc_batch* b, uint64_t* items_ntt, uint64_t* items_product, uint64_t* items_finish,
                          uint32_t* lanes) {
   if (!b) return LC_ERR_INVALID_ARGUMENT;
-  if (items_ntt) *items_ntt = b->total[0];
+  const bool tw = b->products == LC_PRODUCTS_TENSOR && b->tensor_ok;
+  if (items_ntt) *items_ntt = b->total[0] + (tw ? b->twitems : 0);
   if (items_product)
     *items_product = b->products == LC_PRODUCTS_TENSOR && b->tensor_ok ? b->titems[0] + b->titems[1] : b->total[1];
   if (items_finish) *items_finish = b->total[2];

@@ -109,6 +109,18 @@ LC_D uint64_t umma_desc_mn(uint32_t saddr, uint32_t lbo, uint32_t sbo, uint32_t 
   return d;
 }
 
+// 16-byte global -> shared copy of `bytes` (0..16) source bytes, the rest
+// zero (src and dst 16-byte aligned; no byte is read when bytes = 0), and the
+// per-thread commit / wait of those copies.
+LC_D void cp_async16_zfill(uint32_t dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+LC_D void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+LC_D void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // ------------------------------------------------------------------ host side
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,

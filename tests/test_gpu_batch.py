@@ -97,7 +97,8 @@ def as_u(x):
 def mixed_classes():
     return [gl_class(6, 300, 1), gl_class(7, 200, 2), gl_class(8, 90, 3),
             u32_class(CRT_SET_30BIT, 6, 300, 4), u32_class(CRT_SET_30BIT, 8, 90, 5),
-            u32_class([Modulus32.Q_32], 6, 150, 6)]
+            u32_class([Modulus32.Q_32], 6, 150, 6), u32_class(CRT_SET_30BIT[1:3], 7, 140, 7),
+            u32_class([Modulus32.Q_12289], 7, 60, 8)]
 
 
 def test_key_view_matches_submatrix_key(mixed_classes):
