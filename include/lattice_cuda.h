@@ -404,11 +404,12 @@ LC_API int lc_batch_get_config(const lc_batch *batch, uint32_t *chunk, uint32_t 
  * zeros -- or LC_PRODUCTS_INT64 with 160-bit / 64-bit multiply-accumulates on
  * the CUDA cores (one item per slot, chunk and 16-job block; `chunk` of
  * lc_batch_set_config applies to this form only).  Identical results.
- * In the tensor mode the witness NTTs of lanes with ring degree 128 or 256
- * and a 30-bit modulus q = 2^30 - c, c <= 2^20 (the 4-prime CRT set) run on
- * the tensor cores too: per tile of 128 witness polynomials the product with
- * the fixed matrix V[t][k] = psi^((2t+1)k) split into byte limbs (the values
- * ntt.rs:118-146 computes); the other lanes keep the CUDA-core transforms.
+ * In the tensor mode the witness NTTs run on the tensor cores too, for
+ * Goldilocks lanes and lanes of a 30-bit modulus q = 2^30 - c, c <= 2^20
+ * (the 4-prime CRT set): per tile of 128 witness polynomials the product
+ * with the fixed matrix V[t][k] = psi^((2t+1)k) split into byte limbs (the
+ * values ntt.rs:118-146 computes); lanes of other moduli keep the CUDA-core
+ * transforms.
  * lc_batch_set_products returns LC_ERR_UNSUPPORTED when the tensor form
  * cannot run (no tensor-map encoder in the driver); lc_batch_get_products
  * returns the mode (-1 for a null batch). */

@@ -525,38 +525,47 @@ __global__ void __launch_bounds__(kBatchThreads, sizeof(E) == 8 ? 2 : 3)
   }
 }
 
-// ---- launch 1 on the tensor cores: witness transforms of u32 lanes, d = 128 / 256
+// ---- launch 1 on the tensor cores: witness transforms, d = 64 / 128 / 256
 //
-// For q < 2^30 and ring degree d the forward transform of a digit row w
-// (natural order, out[t] = sum_c w_c psi^((2t+1) c), ntt.rs:118-146) is the
-// fixed product What[t] = sum_c V[t][c] w[c] (mod q), V[t][c] = psi^((2t+1) c).
-// With V's residues split into 4 byte limbs it is 4 exact INT8 GEMMs,
+// For ring degree d the forward transform of a digit row w (natural order,
+// out[t] = sum_c w_c psi^((2t+1) c), ntt.rs:118-146) is the fixed product
+// What[t] = sum_c V[t][c] w[c] (mod q), V[t][c] = psi^((2t+1) c).  With V's
+// residues split into L byte limbs (4 for a 30-bit q, 8 for Goldilocks) it
+// is L exact INT8 GEMMs,
 //   D[p][(t,l)] = sum_c w_p[c] V_l[t][c]   (s8 x u8 -> s32, |D| <= d 128 255 < 2^23),
-// folded per output as v = sum_l 2^(8l) D (|v| < 2^48), u = v + q 2^19 > 0,
-// two folds by 2^30 == 2^30 - q (mod q) and one conditional subtract.  A tile
-// is 128 consecutive staircase polynomials of a lane (M = 128), gathered from
-// the jobs' digit rows by four warps with cp.async into the K-major
-// 128-byte-swizzled layout (K = d bytes in 128-byte atoms); N = the 4d
-// columns (t, l) in passes of 256 (64 slots), each pass's V-limb rows loaded by
-// TMA from the lane's [4d][d] image in global memory (L2-resident); two TMEM
-// accumulators of 256 columns alternate between passes, so four epilogue
-// warps fold pass k and store What[t][Rp[j] + b] while pass k + 1 runs.
+// folded per output: for q = 2^30 - c (c <= 2^20) v = sum_l 2^(8l) D
+// (|v| < 2^48), u = v + q 2^19 > 0, two folds by 2^30 == c and one
+// conditional subtract (tw_fold); for Goldilocks tw_fold_gl.  A tile is 128
+// consecutive staircase polynomials of a lane (M = 128), gathered from the
+// jobs' digit rows by four warps with cp.async into the K-major
+// 128-byte-swizzled layout (K = d bytes in 128-byte atoms; d = 64 fills half
+// an atom and runs 2 K-steps); N = the L d columns (t, l) in passes of PN
+// (PN / L slots), each pass's V-limb rows loaded by TMA from the lane's
+// [L d][max(d, 128)] image in global memory (L2-resident) into one of
+// NS = 512 / PN stages; NS TMEM accumulators of PN columns rotate between
+// passes, so the epilogue warps fold pass k and store What[t][Rp[j] + b]
+// while the next passes load and run.
 // EW epilogue warps (8 or 16; warp w reads TMEM lanes 32 (w % 4).. and a
-// 256 / (EW / 4)-column share of each pass), then 4 gather warps, the TMA
+// PN / (EW / 4)-column share of each pass), then 4 gather warps, the TMA
 // warp and the MMA warp.
-template <int EW>
+template <int EW, int PN>
 struct TwCfg {
   static_assert(EW == 8 || EW == 16, "epilogue warps");
+  static_assert(PN == 128 || PN == 256, "pass width");
   static constexpr int THREADS = 32 * (EW + 6);
   static constexpr int GATHER = EW, TMA = EW + 4, MMA = EW + 5;
-  static constexpr uint32_t COLS = 256 / (EW / 4);  // TMEM columns per epilogue warp and pass
+  static constexpr uint32_t COLS = PN / (EW / 4);  // TMEM columns per epilogue warp and pass
+  static constexpr uint32_t NS = 512 / PN;         // B stages = TMEM accumulators
+  static constexpr uint32_t BSTAGE = PN * 256;     // bytes of a B stage (PN rows x d <= 256)
+  // D = s32, A = s8, B = u8, both K-major, N = PN, M = 128
+  static constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | ((uint32_t)(PN >> 3) << 17) | ((128u >> 4) << 24);
 };
-constexpr int kTwEpi = 8;
+constexpr int kTwEpi = 16;
+constexpr int kTwPN = 128;
 constexpr int kTwRows = 128;          // polynomials per tile
 constexpr int kTwABytes = kTwRows * 256;  // A stage (d <= 256)
-constexpr int kTwBBytes = 256 * 256;      // B stage: 256 rows (t, l) x d <= 256
 constexpr int kTwOffB = 2 * kTwABytes;
-constexpr int kTwOffInfo = kTwOffB + 2 * kTwBBytes;          // per A stage: 128 x u64 destinations
+constexpr int kTwOffInfo = kTwOffB + 512 * 256;              // per A stage: 128 x u64 destinations
 constexpr int kTwOffBar = kTwOffInfo + 2 * kTwRows * 8;
 constexpr size_t kTwSmem = 1024 + kTwOffBar + 256;
 static_assert(kTwSmem <= 227 * 1024, "shared memory");
@@ -564,9 +573,6 @@ static_assert(kTwSmem <= 227 * 1024, "shared memory");
 struct TwItem {
   uint32_t lane, tile, jlo, pad;
 };
-
-// D = s32, A = s8, B = u8, both K-major, N = 256, M = 128
-constexpr uint32_t kTwIdesc = (2u << 4) | (1u << 7) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
 
 // OR of `v` over the `count` threads of named barrier `id` (all of them
 // receive it): keeps a warp group's loop decisions uniform.
@@ -590,8 +596,27 @@ LC_D uint32_t tw_fold(int64_t v, uint32_t q, uint32_t c) {
   return y >= q ? y - q : y;
 }
 
-template <int EW>
-__global__ void __launch_bounds__(TwCfg<EW>::THREADS, 1)
+// Goldilocks: v = A + 2^32 B with A, B the limb sums 0-3 and 4-7 (|A|, |B|
+// <= 256 128 255 (1 + 2^8 + 2^16 + 2^24) < 2^47.01), reduced mod p with
+// 2^64 == 2^32 - 1: A + (B >> 32)(2^32 - 1) + 2^49 lies in (0, 2^50); adding
+// (B mod 2^32) 2^32 wraps at most once, and one step removes the offset.
+LC_D uint64_t tw_fold_gl(const uint32_t* x) {
+  const int64_t A = (int64_t)(int32_t)x[0] + ((int64_t)(int32_t)x[1] << 8) + ((int64_t)(int32_t)x[2] << 16) +
+                    ((int64_t)(int32_t)x[3] << 24);
+  const int64_t B = (int64_t)(int32_t)x[4] + ((int64_t)(int32_t)x[5] << 8) + ((int64_t)(int32_t)x[6] << 16) +
+                    ((int64_t)(int32_t)x[7] << 24);
+  const uint64_t t = (uint64_t)(A + (B >> 32) * (int64_t)0xFFFFFFFFll + ((int64_t)1 << 49));
+  uint64_t r = t + ((uint64_t)(uint32_t)B << 32);
+  if (r < t) r += 0xFFFFFFFFull;
+  constexpr uint64_t kOff = 1ull << 49;
+  return r - kOff + (r < kOff ? kGlP : 0);
+}
+
+// limbs of a lane's V image (8 Goldilocks, 4 u32) and its passes of PN columns
+LC_D uint32_t tw_limbs(const LaneDesc& L) { return L.kind == (uint32_t)PlanKind::Goldilocks ? 8u : 4u; }
+
+template <int EW, int PN>
+__global__ void __launch_bounds__(TwCfg<EW, PN>::THREADS, 1)
     lane_witness_tc_kernel(const TwItem* __restrict__ items, uint64_t nitems, const LaneDesc* __restrict__ lanes,
                            const SubJob* __restrict__ subs, const CUtensorMap* __restrict__ vmaps, uint32_t* err) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -601,14 +626,15 @@ __global__ void __launch_bounds__(TwCfg<EW>::THREADS, 1)
   uint64_t* bars = reinterpret_cast<uint64_t*>(base + kTwOffBar);
   uint64_t* a_full = bars;        // [2] 128 gather threads
   uint64_t* a_free = bars + 2;    // [2] MMA commit + EW epilogue warps
-  uint64_t* b_full = bars + 4;    // [2] V rows landed (tx)
-  uint64_t* b_empty = bars + 6;   // [2] MMA commit
-  uint64_t* acc_full = bars + 8;  // [2] MMA commit
-  uint64_t* acc_empty = bars + 10;  // [2] EW epilogue warps
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 12);
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 13);
-  uint64_t* done = bars + 14;     // every MMA issued has finished
-  using Cfg = TwCfg<EW>;
+  uint64_t* b_full = bars + 4;    // [NS] V rows landed (tx)
+  uint64_t* b_empty = bars + 8;   // [NS] MMA commit
+  uint64_t* acc_full = bars + 12;   // [NS] MMA commit
+  uint64_t* acc_empty = bars + 16;  // [NS] EW epilogue warps
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 20);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 21);
+  uint64_t* done = bars + 22;     // every MMA issued has finished
+  using Cfg = TwCfg<EW, PN>;
+  constexpr uint32_t NS = Cfg::NS;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   if (tid == 0) {
@@ -616,6 +642,8 @@ __global__ void __launch_bounds__(TwCfg<EW>::THREADS, 1)
     for (int s = 0; s < 2; ++s) {
       mbar_init(&a_full[s], 128);
       mbar_init(&a_free[s], 1 + EW);
+    }
+    for (uint32_t s = 0; s < NS; ++s) {
       mbar_init(&b_full[s], 1);
       mbar_init(&b_empty[s], 1);
       mbar_init(&acc_full[s], 1);
@@ -640,7 +668,7 @@ __global__ void __launch_bounds__(TwCfg<EW>::THREADS, 1)
     *abort_flag = 1;
   };
   auto a_stage = [&](uint64_t i) { return base + (i & 1) * kTwABytes; };
-  auto b_stage = [&](uint64_t g) { return base + kTwOffB + (g & 1) * kTwBBytes; };
+  auto b_stage = [&](uint64_t g) { return base + kTwOffB + (g % NS) * Cfg::BSTAGE; };
   int64_t tma_last = -1;    // TMA thread: last pass index loaded
 
   if (warp == Cfg::TMA) {
@@ -649,16 +677,17 @@ __global__ void __launch_bounds__(TwCfg<EW>::THREADS, 1)
       uint64_t g = 0;
       for (uint64_t i = 0; i < n_my && !*abort_flag; ++i) {
         const TwItem it = item_at(i);
-        const uint32_t d = 1u << lanes[it.lane].log_n, passes = d / 64;
+        const LaneDesc& L = lanes[it.lane];
+        const uint32_t d = 1u << L.log_n, passes = tw_limbs(L) * d / PN, kb = d > 128 ? d / 128 : 1;
         const CUtensorMap* vm = vmaps + it.lane;
         for (uint32_t k = 0; k < passes && !*abort_flag; ++k, ++g) {
-          if (g >= 2 && !mbar_wait(&b_empty[g & 1], (uint32_t)(((g - 2) >> 1) & 1))) {
+          if (g >= NS && !mbar_wait(&b_empty[g % NS], (uint32_t)(((g - NS) / NS) & 1))) {
             fail();
             break;
           }
-          mbar_arrive_expect_tx(&b_full[g & 1], 256 * d);
-          for (uint32_t kk = 0; kk < d / 128; ++kk)
-            tma_load_2d(b_stage(g) + kk * 32768, vm, (int)(kk * 128), (int)(k * 256), &b_full[g & 1]);
+          mbar_arrive_expect_tx(&b_full[g % NS], PN * 128 * kb);
+          for (uint32_t kk = 0; kk < kb; ++kk)
+            tma_load_2d(b_stage(g) + kk * (PN * 128), vm, (int)(kk * 128), (int)(k * PN), &b_full[g % NS]);
           tma_last = (int64_t)g;
         }
       }
@@ -670,15 +699,16 @@ __global__ void __launch_bounds__(TwCfg<EW>::THREADS, 1)
       bool ok = true;
       for (uint64_t i = 0; i < n_my && ok && !*abort_flag; ++i) {
         const TwItem it = item_at(i);
-        const uint32_t d = 1u << lanes[it.lane].log_n, passes = d / 64;
+        const LaneDesc& L = lanes[it.lane];
+        const uint32_t d = 1u << L.log_n, passes = tw_limbs(L) * d / PN;
         if (!mbar_wait(&a_full[i & 1], (uint32_t)((i >> 1) & 1))) {
           fail();
           break;
         }
         const uint32_t aa = smem_u32(a_stage(i));
         for (uint32_t k = 0; k < passes; ++k, ++g) {
-          if (!mbar_wait(&b_full[g & 1], (uint32_t)((g >> 1) & 1)) ||
-              (g >= 2 && !mbar_wait(&acc_empty[g & 1], (uint32_t)(((g - 2) >> 1) & 1)))) {
+          if (!mbar_wait(&b_full[g % NS], (uint32_t)((g / NS) & 1)) ||
+              (g >= NS && !mbar_wait(&acc_empty[g % NS], (uint32_t)(((g - NS) / NS) & 1)))) {
             fail();
             ok = false;
             break;
@@ -687,11 +717,11 @@ __global__ void __launch_bounds__(TwCfg<EW>::THREADS, 1)
           const uint32_t bb = smem_u32(b_stage(g));
           for (uint32_t ks = 0; ks < d / 32; ++ks) {
             const uint32_t off = (ks >> 2) * 16384u + (ks & 3) * 32u;
-            mma_i8(tmem + (uint32_t)(g & 1) * 256, umma_desc_sw128(aa + off),
-                   umma_desc_sw128(bb + (ks >> 2) * 32768u + (ks & 3) * 32u), kTwIdesc, ks > 0 ? 1u : 0u);
+            mma_i8(tmem + (uint32_t)(g % NS) * PN, umma_desc_sw128(aa + off),
+                   umma_desc_sw128(bb + (ks >> 2) * (PN * 128u) + (ks & 3) * 32u), Cfg::IDESC, ks > 0 ? 1u : 0u);
           }
-          mma_commit(&acc_full[g & 1]);
-          mma_commit(&b_empty[g & 1]);
+          mma_commit(&acc_full[g % NS]);
+          mma_commit(&b_empty[g % NS]);
         }
         if (ok) mma_commit(&a_free[i & 1]);
       }
@@ -699,8 +729,39 @@ __global__ void __launch_bounds__(TwCfg<EW>::THREADS, 1)
       if (!mbar_wait(done, 0)) fail();
     }
   } else if (warp >= Cfg::GATHER) {
-    // ---------------- gather: row info (thread r = row r), then the digit rows
+    // ---------------- gather: row info (thread r = row r), then the digit rows.
+    // A tile's row table is worked out while the previous tile's copies are
+    // in flight: R[jlo .. jlo + 128] staged in shared memory, each row's ring
+    // element found there, then its source row and staircase destination.
     const int gt = tid - 32 * Cfg::GATHER;  // 0..127
+    __shared__ uint64_t s_R[kTwRows + 1];
+    __shared__ const int8_t* s_src[kTwRows];
+    auto row_of = [&](uint64_t ii, const int8_t*& src, uint64_t& dst) {
+      const TwItem it = item_at(ii);
+      const LaneDesc& L = lanes[it.lane];
+      const uint32_t hi = min(L.n_max, it.jlo + kTwRows);  // R[jlo] <= the tile's polynomials < R[hi]
+      if (it.jlo + gt <= hi) s_R[gt] = __ldg(L.R + it.jlo + gt);
+      if (gt == 0 && it.jlo + kTwRows <= hi) s_R[kTwRows] = __ldg(L.R + it.jlo + kTwRows);
+      asm volatile("bar.sync 1, 128;" ::: "memory");
+      // row r: staircase polynomial p = 128 tile + r -> ring element j (R[j] <= p < R[j + 1]), job b
+      const uint64_t p = (uint64_t)it.tile * kTwRows + gt;
+      src = nullptr;
+      dst = ~0ull;
+      if (p < L.S) {
+        uint32_t lo = 0, h = hi - it.jlo;
+        while (h - lo > 1) {
+          const uint32_t mid = (lo + h) >> 1;
+          if (s_R[mid] <= p) lo = mid; else h = mid;
+        }
+        const uint32_t b = (uint32_t)(p - s_R[lo]);
+        src = subs[L.sub0 + b].w + (size_t)(it.jlo + lo) * (1u << L.log_n);
+        dst = __ldg(L.Rp + it.jlo + lo) + b;
+      }
+      asm volatile("bar.sync 1, 128;" ::: "memory");  // s_R is rewritten by the next call
+    };
+    const int8_t* src = nullptr;
+    uint64_t dst = ~0ull;
+    if (n_my) row_of(0, src, dst);
     for (uint64_t i = 0; i < n_my; ++i) {
       // one decision for the four gather warps (they share named barrier 1)
       bool timed_out = false;
@@ -710,23 +771,7 @@ __global__ void __launch_bounds__(TwCfg<EW>::THREADS, 1)
       const TwItem it = item_at(i);
       const LaneDesc& L = lanes[it.lane];
       const uint32_t d = 1u << L.log_n;
-      uint64_t* inf = info + (i & 1) * kTwRows;
-      // row r: staircase polynomial p = 128 tile + r -> ring element j (R[j] <= p < R[j + 1]), job b
-      const uint64_t p = (uint64_t)it.tile * kTwRows + gt;
-      const int8_t* src = nullptr;
-      uint64_t dst = ~0ull;
-      if (p < L.S) {
-        uint32_t lo = it.jlo, hi = min(L.n_max, it.jlo + kTwRows);  // R[lo] <= p < R[hi]
-        while (hi - lo > 1) {
-          const uint32_t mid = (lo + hi) >> 1;
-          if (__ldg(L.R + mid) <= p) lo = mid; else hi = mid;
-        }
-        const uint32_t b = (uint32_t)(p - __ldg(L.R + lo));
-        src = subs[L.sub0 + b].w + (size_t)lo * d;
-        dst = __ldg(L.Rp + lo) + b;
-      }
-      inf[gt] = dst;
-      __shared__ const int8_t* s_src[kTwRows];
+      info[(i & 1) * kTwRows + gt] = dst;
       s_src[gt] = src;
       asm volatile("bar.sync 1, 128;" ::: "memory");  // the four gather warps
       const uint32_t cpr = d / 16;                 // 16-byte chunks per row
@@ -739,9 +784,12 @@ __global__ void __launch_bounds__(TwCfg<EW>::THREADS, 1)
         cp_async16_zfill(dsto, sp ? (const void*)(sp + c * 16) : (const void*)L.what, sp ? 16u : 0u);
       }
       cp_async_commit();
+      // the next tile's rows while these copies fly (its first barrier also
+      // ends this tile's reads of s_src; the barrier at the top of the next
+      // iteration does when there is none)
+      if (i + 1 < n_my) row_of(i + 1, src, dst);
       cp_async_wait<0>();
       fence_proxy_async_smem();
-      asm volatile("bar.sync 1, 128;" ::: "memory");  // s_src is rewritten by the next tile
       mbar_arrive(&a_full[i & 1]);
     }
     cp_async_wait<0>();
@@ -753,7 +801,8 @@ __global__ void __launch_bounds__(TwCfg<EW>::THREADS, 1)
     for (uint64_t i = 0; i < n_my; ++i) {
       const TwItem it = item_at(i);
       const LaneDesc& L = lanes[it.lane];
-      const uint32_t d = 1u << L.log_n, passes = d / 64, q = L.q, cq = (1u << 30) - q;
+      const bool gl = L.kind == (uint32_t)PlanKind::Goldilocks;
+      const uint32_t d = 1u << L.log_n, passes = tw_limbs(L) * d / PN, q = L.q, cq = (1u << 30) - q;
       const size_t Sp = L.Sp;
       bool stop = false;
       // the gather's row table of this tile (its a_full phase; the stage is
@@ -765,35 +814,53 @@ __global__ void __launch_bounds__(TwCfg<EW>::THREADS, 1)
       }
       const uint64_t dst = info[(i & 1) * kTwRows + row];
       for (uint32_t k = 0; k < passes; ++k, ++g) {
-        const bool ok = !*abort_flag && mbar_wait(&acc_full[g & 1], (uint32_t)((g >> 1) & 1));
+        const bool ok = !*abort_flag && mbar_wait(&acc_full[g % NS], (uint32_t)((g / NS) & 1));
         if (!__all_sync(0xffffffffu, ok)) {  // warp-uniform: the TMEM loads are .sync.aligned
           if (lane == 0) fail();
           stop = true;
           break;
         }
         tc_fence_after();
-        // output slot t = 64 k + (cbeg + c0) / 4 + u, row dst of the staircase
-        uint32_t* what = reinterpret_cast<uint32_t*>(L.what) + (dst == ~0ull ? 0 : dst) +
-                         (size_t)(64 * k + cbeg / 4) * Sp;
-        const uint32_t taddr = tmem + ((32 * quad) << 16) + (uint32_t)(g & 1) * 256 + cbeg;
+        const uint32_t taddr = tmem + ((32 * quad) << 16) + (uint32_t)(g % NS) * PN + cbeg;
+        if (gl) {
+          // output slot t = (PN / 8) k + (cbeg + c0) / 8 + u, row dst of the staircase
+          uint64_t* what = reinterpret_cast<uint64_t*>(L.what) + (dst == ~0ull ? 0 : dst) +
+                           (size_t)((PN / 8) * k + cbeg / 8) * Sp;
 #pragma unroll 1
-        for (uint32_t c0 = 0; c0 < Cfg::COLS; c0 += 32) {
-          uint32_t v0[16], v1[16];
-          tmem_ld16(taddr + c0, v0);
-          tmem_ld16(taddr + c0 + 16, v1);
-          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          for (uint32_t c0 = 0; c0 < Cfg::COLS; c0 += 32) {
+            uint32_t v0[16], v1[16];
+            tmem_ld16(taddr + c0, v0);
+            tmem_ld16(taddr + c0 + 16, v1);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-          for (int u = 0; u < 8; ++u) {
-            const uint32_t* x = u < 4 ? v0 + 4 * u : v1 + 4 * (u - 4);
-            const int64_t vv = (int64_t)(int32_t)x[0] + ((int64_t)(int32_t)x[1] << 8) +
-                               ((int64_t)(int32_t)x[2] << 16) + ((int64_t)(int32_t)x[3] << 24);
-            if (dst != ~0ull) *what = tw_fold(vv, q, cq);
-            what += Sp;
+            for (int u = 0; u < 4; ++u) {
+              if (dst != ~0ull) *what = tw_fold_gl(u < 2 ? v0 + 8 * u : v1 + 8 * (u - 2));
+              what += Sp;
+            }
+          }
+        } else {
+          // output slot t = (PN / 4) k + (cbeg + c0) / 4 + u, row dst of the staircase
+          uint32_t* what = reinterpret_cast<uint32_t*>(L.what) + (dst == ~0ull ? 0 : dst) +
+                           (size_t)((PN / 4) * k + cbeg / 4) * Sp;
+#pragma unroll 1
+          for (uint32_t c0 = 0; c0 < Cfg::COLS; c0 += 32) {
+            uint32_t v0[16], v1[16];
+            tmem_ld16(taddr + c0, v0);
+            tmem_ld16(taddr + c0 + 16, v1);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+              const uint32_t* x = u < 4 ? v0 + 4 * u : v1 + 4 * (u - 4);
+              const int64_t vv = (int64_t)(int32_t)x[0] + ((int64_t)(int32_t)x[1] << 8) +
+                                 ((int64_t)(int32_t)x[2] << 16) + ((int64_t)(int32_t)x[3] << 24);
+              if (dst != ~0ull) *what = tw_fold(vv, q, cq);
+              what += Sp;
+            }
           }
         }
         tc_fence_before();
         __syncwarp();
-        if (lane == 0) mbar_arrive(&acc_empty[g & 1]);
+        if (lane == 0) mbar_arrive(&acc_empty[g % NS]);
       }
       if (stop) break;
       if (lane == 0) mbar_arrive(&a_free[i & 1]);
@@ -802,8 +869,8 @@ __global__ void __launch_bounds__(TwCfg<EW>::THREADS, 1)
   // ---------------- nothing in flight when TMEM and shared memory go
   __syncthreads();
   if (warp == Cfg::TMA && lane == 0) {
-    for (int64_t g = tma_last >= 1 ? tma_last - 1 : 0; g <= tma_last; ++g)
-      mbar_wait(&b_full[g & 1], (uint32_t)((g >> 1) & 1));
+    for (int64_t g = tma_last >= (int64_t)NS - 1 ? tma_last - (NS - 1) : 0; g <= tma_last; ++g)
+      mbar_wait(&b_full[g % NS], (uint32_t)((g / NS) & 1));
   }
   tc_fence_before();
   __syncthreads();
@@ -1224,18 +1291,19 @@ static uint64_t powmod64(uint64_t a, uint64_t e, uint64_t q) {
   return r;
 }
 
-// The [4d rows (t, l)][d bytes c] image of V[t][c] = psi^((2t+1) c) mod q
-// split into byte limbs l, psi = g^((q - 1) >> (log d + 1)) as the plan's
-// forward transform uses (natural output order, ntt.rs:118-146).
-static void tw_image(uint64_t q, uint64_t g, uint32_t log_d, std::vector<uint8_t>& img) {
-  const uint32_t d = 1u << log_d;
+// The [limbs d rows (t, l)][max(d, 128) bytes c] image of V[t][c] =
+// psi^((2t+1) c) mod q split into byte limbs l (zero for c >= d), psi =
+// g^((q - 1) >> (log d + 1)) as the plan's forward transform uses (natural
+// output order, ntt.rs:118-146; Goldilocks: g = 7, field.rs:195-200).
+static void tw_image(uint64_t q, uint64_t g, uint32_t log_d, uint32_t limbs, std::vector<uint8_t>& img) {
+  const uint32_t d = 1u << log_d, cols = std::max(d, 128u);
   const uint64_t psi = powmod64(g, (q - 1) >> (log_d + 1), q);
-  img.assign((size_t)4 * d * d, 0);
+  img.assign((size_t)limbs * d * cols, 0);
   for (uint32_t t = 0; t < d; ++t) {
     const uint64_t step = powmod64(psi, 2 * t + 1, q);
     uint64_t v = 1;
     for (uint32_t c = 0; c < d; ++c, v = mulmod64(v, step, q))
-      for (uint32_t l = 0; l < 4; ++l) img[((size_t)t * 4 + l) * d + c] = (uint8_t)(v >> (8 * l));
+      for (uint32_t l = 0; l < limbs; ++l) img[((size_t)t * limbs + l) * cols + c] = (uint8_t)(v >> (8 * l));
   }
 }
 
@@ -1267,16 +1335,17 @@ static int batch_tw_setup(lc_batch* b, const std::vector<uint32_t>& plan_gen) {
   std::vector<TwItem> items;
   for (size_t l = 0; l < nl; ++l) {
     const LaneDesc& L = b->lanes[l];
-    if (L.kind != (uint32_t)PlanKind::U32Lazy || (L.log_n != 7 && L.log_n != 8) || L.S == 0) continue;
-    const uint32_t d = 1u << L.log_n;
-    if (!tw_fold_exact(L.q, d)) continue;
-    const uint64_t key = ((uint64_t)L.q << 16) | d;
+    const bool gl = L.kind == (uint32_t)PlanKind::Goldilocks;
+    if (L.log_n < 6 || L.log_n > 8 || L.S == 0) continue;
+    const uint32_t d = 1u << L.log_n, limbs = gl ? 8 : 4, cols = std::max(d, 128u);
+    if (!gl && (L.kind != (uint32_t)PlanKind::U32Lazy || !tw_fold_exact(L.q, d))) continue;
+    const uint64_t key = gl ? (1ull << 63) | d : ((uint64_t)L.q << 16) | d;
     void* img = nullptr;
     for (auto& v : b->vimgs)
       if (v.first == key) img = v.second;
     if (!img) {
       std::vector<uint8_t> h;
-      tw_image(L.q, plan_gen[l], L.log_n, h);
+      tw_image(gl ? kGlP : L.q, gl ? 7 : plan_gen[l], L.log_n, limbs, h);
       if (cudaMalloc(&img, h.size()) != cudaSuccess) {
         cudaGetLastError();
         return LC_ERR_OUT_OF_MEMORY;
@@ -1284,9 +1353,9 @@ static int batch_tw_setup(lc_batch* b, const std::vector<uint32_t>& plan_gen) {
       cudaMemcpy(img, h.data(), h.size(), cudaMemcpyHostToDevice);
       b->vimgs.push_back({key, img});
     }
-    const cuuint64_t dims[2] = {d, (cuuint64_t)4 * d};
-    const cuuint64_t strides[1] = {d};
-    const cuuint32_t box[2] = {128, 256};
+    const cuuint64_t dims[2] = {cols, (cuuint64_t)limbs * d};
+    const cuuint64_t strides[1] = {cols};
+    const cuuint32_t box[2] = {128, kTwPN};
     const cuuint32_t estr[2] = {1, 1};
     if (enc(&maps[l], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, img, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -1405,13 +1474,13 @@ static int batch_launch(lc_batch* b, cudaStream_t st) {
     e = cudaFuncSetAttribute(batch_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem[0]);
     if (e != cudaSuccess) return map_cuda(e);
   }
-  batch_kernel<0><<<grid, kBatchThreads, b->smem[0], st>>>(p);
+  if (b->total[0]) batch_kernel<0><<<grid, kBatchThreads, b->smem[0], st>>>(p);
   if (b->products == LC_PRODUCTS_TENSOR && b->tensor_ok && b->twitems) {
     static std::atomic<uint64_t> attr_tw{0};
-    e = smem_attr_once(attr_tw, lane_witness_tc_kernel<kTwEpi>, kTwSmem);
+    e = smem_attr_once(attr_tw, lane_witness_tc_kernel<kTwEpi, kTwPN>, kTwSmem);
     if (e != cudaSuccess) return map_cuda(e);
     const unsigned tgrid = (unsigned)std::min<uint64_t>(b->twitems, (uint64_t)std::max(1, device_sm_count()));
-    lane_witness_tc_kernel<kTwEpi><<<tgrid, TwCfg<kTwEpi>::THREADS, kTwSmem, st>>>(b->d_twitems, b->twitems, b->d_lanes, b->d_subs,
+    lane_witness_tc_kernel<kTwEpi, kTwPN><<<tgrid, TwCfg<kTwEpi, kTwPN>::THREADS, kTwSmem, st>>>(b->d_twitems, b->twitems, b->d_lanes, b->d_subs,
                                                                 b->d_vmaps, b->d_err);
   }
   if (b->products == LC_PRODUCTS_TENSOR && b->tensor_ok) {
