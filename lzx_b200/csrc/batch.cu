@@ -561,7 +561,7 @@ struct TwCfg {
   static constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | ((uint32_t)(PN >> 3) << 17) | ((128u >> 4) << 24);
 };
 constexpr int kTwEpi = 16;
-constexpr int kTwPN = 128;
+constexpr int kTwPN = 256;
 constexpr int kTwRows = 128;          // polynomials per tile
 constexpr int kTwABytes = kTwRows * 256;  // A stage (d <= 256)
 constexpr int kTwOffB = 2 * kTwABytes;
@@ -587,13 +587,19 @@ LC_D bool named_bar_or(bool v, uint32_t id, uint32_t count) {
   return r != 0;
 }
 
-// v (|v| < 2^48) mod q, canonical, for the q tw_fold_exact accepts (2^30 - c,
-// c <= 2^20): u = v + q 2^19 in (0, 2^50), then two folds by 2^30 == c
-LC_D uint32_t tw_fold(int64_t v, uint32_t q, uint32_t c) {
-  const uint64_t u = (uint64_t)(v + ((int64_t)q << 19));
-  const uint64_t x = (uint64_t)(uint32_t)(u >> 30) * c + ((uint32_t)u & 0x3FFFFFFFu);  // < 2^40 + 2^30
-  const uint32_t y = (uint32_t)(x >> 30) * c + ((uint32_t)x & 0x3FFFFFFFu);            // < 2q
-  return y >= q ? y - q : y;
+// One output from its four limb sums x[l]: v = sum_l 2^(8l) D_l (|v| < 2^48)
+// mod q, canonical, for the q tw_fold_exact accepts (2^30 - c, c <= 2^20):
+// u = v + off (off = q 2^19) in (0, 2^50), two folds by 2^30 == c, and
+// min(y, y - q) for the final subtract (y < 2q).
+LC_D uint32_t tw_fold(const uint32_t* x, uint32_t q, uint32_t c, int64_t off) {
+  int64_t v = off + (int32_t)x[0];
+  v += (int64_t)(int32_t)x[1] * 256;
+  v += (int64_t)(int32_t)x[2] * 65536;
+  v += (int64_t)(int32_t)x[3] * 16777216;
+  const uint64_t u = (uint64_t)v;
+  const uint64_t w = (uint64_t)(uint32_t)(u >> 30) * c + ((uint32_t)u & 0x3FFFFFFFu);  // < 2^40 + 2^30
+  const uint32_t y = (uint32_t)(w >> 30) * c + ((uint32_t)w & 0x3FFFFFFFu);            // < 2q
+  return min(y, y - q);
 }
 
 // Goldilocks: v = A + 2^32 B with A, B the limb sums 0-3 and 4-7 (|A|, |B|
@@ -601,10 +607,13 @@ LC_D uint32_t tw_fold(int64_t v, uint32_t q, uint32_t c) {
 // 2^64 == 2^32 - 1: A + (B >> 32)(2^32 - 1) + 2^49 lies in (0, 2^50); adding
 // (B mod 2^32) 2^32 wraps at most once, and one step removes the offset.
 LC_D uint64_t tw_fold_gl(const uint32_t* x) {
-  const int64_t A = (int64_t)(int32_t)x[0] + ((int64_t)(int32_t)x[1] << 8) + ((int64_t)(int32_t)x[2] << 16) +
-                    ((int64_t)(int32_t)x[3] << 24);
-  const int64_t B = (int64_t)(int32_t)x[4] + ((int64_t)(int32_t)x[5] << 8) + ((int64_t)(int32_t)x[6] << 16) +
-                    ((int64_t)(int32_t)x[7] << 24);
+  int64_t A = (int32_t)x[0], B = (int32_t)x[4];
+  A += (int64_t)(int32_t)x[1] * 256;
+  B += (int64_t)(int32_t)x[5] * 256;
+  A += (int64_t)(int32_t)x[2] * 65536;
+  B += (int64_t)(int32_t)x[6] * 65536;
+  A += (int64_t)(int32_t)x[3] * 16777216;
+  B += (int64_t)(int32_t)x[7] * 16777216;
   const uint64_t t = (uint64_t)(A + (B >> 32) * (int64_t)0xFFFFFFFFll + ((int64_t)1 << 49));
   uint64_t r = t + ((uint64_t)(uint32_t)B << 32);
   if (r < t) r += 0xFFFFFFFFull;
@@ -803,6 +812,7 @@ __global__ void __launch_bounds__(TwCfg<EW, PN>::THREADS, 1)
       const LaneDesc& L = lanes[it.lane];
       const bool gl = L.kind == (uint32_t)PlanKind::Goldilocks;
       const uint32_t d = 1u << L.log_n, passes = tw_limbs(L) * d / PN, q = L.q, cq = (1u << 30) - q;
+      const int64_t off = (int64_t)q << 19;
       const size_t Sp = L.Sp;
       bool stop = false;
       // the gather's row table of this tile (its a_full phase; the stage is
@@ -850,10 +860,7 @@ __global__ void __launch_bounds__(TwCfg<EW, PN>::THREADS, 1)
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
-              const uint32_t* x = u < 4 ? v0 + 4 * u : v1 + 4 * (u - 4);
-              const int64_t vv = (int64_t)(int32_t)x[0] + ((int64_t)(int32_t)x[1] << 8) +
-                                 ((int64_t)(int32_t)x[2] << 16) + ((int64_t)(int32_t)x[3] << 24);
-              if (dst != ~0ull) *what = tw_fold(vv, q, cq);
+              if (dst != ~0ull) *what = tw_fold(u < 4 ? v0 + 4 * u : v1 + 4 * (u - 4), q, cq, off);
               what += Sp;
             }
           }
@@ -904,6 +911,7 @@ __global__ void __launch_bounds__(TwCfg<EW, PN>::THREADS, 1)
 constexpr int kTpRows = 64;            // ring elements per stage
 constexpr int kTpStages = 4;
 constexpr int kTpLag = 2;              // gather stages in flight before a stage is handed to the MMA
+constexpr int kTpAhead = 2;            // stages the staircase offsets are loaded ahead of their copies
 constexpr int kTpThreads = 192;        // warp 0 TMA, 1 MMA + TMEM, 2..5 gather + epilogue
 
 struct TpItem {
@@ -1041,16 +1049,17 @@ __global__ void __launch_bounds__(kTpThreads, 1)
     const uint32_t kc = k & 7;
     const int first_job = kTpJobs * (int)it.blk + (int)(k * J);
     // R[jb .. jb + 16] (job counts) and Rp[jb .. jb + 15] (row starts) of a
-    // stage, loaded one stage ahead so their latency hides behind the wait
-    // for the copies two stages back
+    // stage, loaded kTpAhead stages ahead (a register queue) so their
+    // latency hides behind the copies and waits of the stages between
     auto offsets = [&](int s, uint64_t& r, uint64_t& rp) {
       const uint32_t jb = j0 + kTpRows * s + 16 * g;
       const bool in_r = s < nst && lane <= 16 && jb + lane <= L.n_max;
       r = in_r ? __ldg(L.R + jb + lane) : 0;
       rp = in_r ? __ldg(L.Rp + jb + lane) : 0;
     };
-    uint64_t rl, rpl;
-    offsets(0, rl, rpl);
+    uint64_t rq[kTpAhead], rpq[kTpAhead];
+#pragma unroll
+    for (int a = 0; a < kTpAhead; ++a) offsets(a, rq[a], rpq[a]);
     bool ok = true;
     for (int s = 0; s < nst; ++s) {
       if (*abort_flag) {
@@ -1063,8 +1072,13 @@ __global__ void __launch_bounds__(kTpThreads, 1)
         break;
       }
       const uint32_t jb = j0 + kTpRows * s + 16 * g;
-      uint64_t rl_next, rpl_next;
-      offsets(s + 1, rl_next, rpl_next);
+      const uint64_t rl = rq[0], rpl = rpq[0];
+#pragma unroll
+      for (int a = 0; a + 1 < kTpAhead; ++a) {
+        rq[a] = rq[a + 1];
+        rpq[a] = rpq[a + 1];
+      }
+      offsets(s + kTpAhead, rq[kTpAhead - 1], rpq[kTpAhead - 1]);
       const uint32_t sb = smem_u32(stage(s)) + C::A_BYTES + boff;
 #pragma unroll
       for (int rr = 0; rr < 16; rr += RPI) {
@@ -1084,8 +1098,6 @@ __global__ void __launch_bounds__(kTpThreads, 1)
         fence_proxy_async_smem();
         mbar_arrive(&full[(s - kTpLag) % kTpStages]);
       }
-      rl = rl_next;
-      rpl = rpl_next;
     }
     cp_async_wait<0>();
     fence_proxy_async_smem();
