@@ -287,7 +287,8 @@ LC_API int lc_ajtai_key_get_slot_products(const lc_ajtai_key *key);
  * rounded up to 128.  A larger request returns LC_ERR_INVALID_ARGUMENT
  * without touching the GPU.
  * The first call on each device looks up the array's device address through
- * the CUDA runtime (later calls reuse it).  All calls share the one array, so
+ * the CUDA runtime (later calls reuse it); make that first call on a device
+ * before any stream capture begins.  All calls share the one array, so
  * calls whose kernels overlap on the GPU (different streams, or different host
  * threads on one device) race with each other: serialise them.  The array
  * keeps the previous call's contents; no part of it needs to start at zero,

@@ -190,18 +190,6 @@ class AjtaiPublicKey:
         key._matrix = dev.cpu().numpy().view(np.uint32)
         return key
 
-    @classmethod
-    def from_seed_host(cls, params: AjtaiParams, seed: bytes) -> "AjtaiPublicKey":
-        """The same expansion element by element on the host (ring.rs:102-180)."""
-        if len(seed) != 32:
-            raise ValueError("seed must be 32 bytes")
-        ring = params.ring
-        total = params.k * params.m
-        mat = np.empty((total, ring.n()), dtype=np.uint32)
-        for idx in range(total):
-            mat[idx] = ring.uniform_from_seed(b"ajtai-A", seed, idx).coeffs()
-        return cls(params, seed, mat)
-
     @property
     def fused(self) -> bool:
         """Small commitments as one launch (the default); False runs them staged."""
