@@ -153,6 +153,23 @@ def test_out_of_place_device_and_host_agree():
     assert _lib.lib().lc_ntt_plan_check(t.handle, None) == 0
 
 
+def test_host_entry_points_over_many_chunks():
+    """The host-buffer transforms stream each modulus's polynomials in chunks
+    of about 16 MiB; a batch of two full chunks plus a ragged one per modulus
+    gives the device transform's residues and comes back by the inverse."""
+    count, n = 2 * 16384 + 123, 256
+    a = synth.crt_batch(31, CRT_SET_30BIT, count, n)
+    t = NttTables(CRT_SET_30BIT, 8)
+    dev = to_dev(a.copy())
+    t.forward_fast(dev)
+    torch.cuda.synchronize()
+    host = t.forward_fast(a.copy())
+    assert np.array_equal(from_dev(dev, np.uint32).reshape(host.shape), host)
+    back = t.inverse_fast(host)
+    assert np.array_equal(back, a)
+    assert _lib.lib().lc_ntt_plan_check(t.handle, None) == 0
+
+
 def test_full_size_crt_round_trip_and_samples():
     """2^16 polynomials x d=256 x 4 primes: the bench workload."""
     count, n = 1 << 16, 256
