@@ -714,6 +714,67 @@ __global__ void __launch_bounds__(256, 2) commit_mac_intt_kernel(const __grid_co
   }
 }
 
+// ------------------------------------------------------------------ split sums and inverse NTT in one launch
+//
+// After the tiled products (a handful of K splits), the rest of ajtai.rs:
+// 139-150 for GROUPS output rows per CTA: rows (b0 .. b0 + GROUPS - 1, i),
+// summed over the splits straight into shared-memory slots (consecutive
+// threads take consecutive witnesses b, so every read of
+// partial[split][t][i][b] is one contiguous run), inverse-transformed there
+// and written to out[b][i][..] -- no Chat round trip and no second launch.
+struct SumInttParams {
+  const void* partial;  // [splits][n][kIPad][b_pad]
+  void* out;            // [batch][kappa][n]
+  const void* twi;      // inverse twiddle table of the plan
+  uint32_t splits, kappa, batch, b_pad, q, qinv;
+};
+
+template <class A, int LOG_N, int LOG_V>
+struct SumInttCfg {
+  using E = typename A::T;
+  using G = Geo<LOG_N, LOG_V>;
+  static constexpr int NT = 128;
+  static constexpr int ROWS = NT / G::T;  // one transform pass
+  static constexpr int SS = WitnessSlotStride<A, LOG_N>::value;
+  static constexpr size_t TWI = ((size_t)G::inv_entries() * sizeof(typename A::Tw) + 15) / 16 * 16;
+  static constexpr size_t SMEM = TWI + (size_t)ROWS * SS * sizeof(E);
+};
+
+template <class A, int LOG_N, int LOG_V>
+__global__ void __launch_bounds__(128) sum_intt_kernel(const __grid_constant__ SumInttParams p) {
+  using C = SumInttCfg<A, LOG_N, LOG_V>;
+  using E = typename A::T;
+  using Tw = typename A::Tw;
+  using G = typename C::G;
+  constexpr int N = G::N, SS = C::SS, ROWS = C::ROWS;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  Tw* twi = reinterpret_cast<Tw*>(smem_raw);
+  E* slots = reinterpret_cast<E*>(smem_raw + C::TWI);
+  const int tid = threadIdx.x;
+  for (int e = tid; e < G::inv_entries(); e += C::NT) twi[e] = static_cast<const Tw*>(p.twi)[e];
+  const uint32_t i = blockIdx.x % p.kappa, b0 = (blockIdx.x / p.kappa) * ROWS;
+  const E* part = static_cast<const E*>(p.partial);
+  const size_t sstride = (size_t)N * kIPad * p.b_pad;  // one K split
+  for (int e = tid; e < ROWS * N; e += C::NT) {
+    const uint32_t rr = e % ROWS, t = e / ROWS, b = b0 + rr;
+    E s = 0;
+    if (b < p.batch) {
+      const E* src = part + ((size_t)t * kIPad + i) * p.b_pad + b;
+      for (uint32_t sp = 0; sp < p.splits; ++sp) s = Field<E>::add(s, __ldg(src + sp * sstride), p.q);
+    }
+    slots[rr * SS + t] = s;
+  }
+  __syncthreads();
+  const A ar = make_arith_q<A>(p.q, p.qinv);
+  transform_slot<A, LOG_N, LOG_V, true>(slots + (tid / G::T) * SS, twi, ar, (uint32_t)(tid % G::T));
+  __syncthreads();
+  E* out = static_cast<E*>(p.out);
+  for (int e = tid; e < ROWS * N; e += C::NT) {
+    const uint32_t rr = e / N, c = e % N, b = b0 + rr;
+    if (b < p.batch) out[((size_t)b * p.kappa + i) * N + c] = slots[rr * SS + c];
+  }
+}
+
 }  // namespace lc
 
 using namespace lc;
@@ -964,6 +1025,54 @@ static int mac_intt(lc_ajtai_key* key, size_t batch, uint32_t b_pad, uint32_t sp
   return LC_ERR_UNSUPPORTED;
 }
 
+template <class A, int LOG_N, int LOG_V>
+static int launch_sum_intt(lc_ajtai_key* key, size_t batch, uint32_t b_pad, uint32_t splits, void* out,
+                           cudaStream_t st) {
+  using C = SumInttCfg<A, LOG_N, LOG_V>;
+  auto kern = sum_intt_kernel<A, LOG_N, LOG_V>;
+  static std::atomic<uint64_t> attr_done{0};
+  const cudaError_t e = smem_attr_once(attr_done, kern, C::SMEM);
+  if (e != cudaSuccess) return map_cuda(e);
+  SumInttParams prm{};
+  prm.partial = key->d_partial;
+  prm.out = out;
+  prm.twi = key->plan->d_tw_inv;
+  prm.splits = splits;
+  prm.kappa = key->k;
+  prm.batch = (uint32_t)batch;
+  prm.b_pad = b_pad;
+  prm.q = key->plan->q[0];
+  prm.qinv = key->plan->qinv[0];
+  const size_t grid = (size_t)key->k * ((batch + C::ROWS - 1) / C::ROWS);
+  kern<<<(unsigned)grid, C::NT, C::SMEM, st>>>(prm);
+  return map_cuda(cudaGetLastError());
+}
+
+template <class A>
+static int sum_intt_as(lc_ajtai_key* key, size_t batch, uint32_t b_pad, uint32_t splits, void* out,
+                       cudaStream_t st) {
+  switch (key->log_n) {
+    case 6: return launch_sum_intt<A, 6, 3>(key, batch, b_pad, splits, out, st);
+    case 7: return launch_sum_intt<A, 7, 4>(key, batch, b_pad, splits, out, st);
+    case 8: return launch_sum_intt<A, 8, 4>(key, batch, b_pad, splits, out, st);
+    default: return LC_ERR_UNSUPPORTED;
+  }
+}
+
+// The tiled form's split sums and inverse transforms as one launch
+// (sum_intt_kernel); LC_ERR_UNSUPPORTED outside d = 64 .. 256.
+template <class E>
+static int sum_intt(lc_ajtai_key* key, size_t batch, uint32_t b_pad, uint32_t splits, void* out, cudaStream_t st) {
+  const PlanKind kind = key->plan->kind;
+  if constexpr (std::is_same<E, uint64_t>::value) {
+    if (kind == PlanKind::Goldilocks) return sum_intt_as<Goldilocks>(key, batch, b_pad, splits, out, st);
+  } else {
+    if (kind == PlanKind::U32Lazy) return sum_intt_as<ShoupLazy>(key, batch, b_pad, splits, out, st);
+    if (kind == PlanKind::U32Mont) return sum_intt_as<MontCanon>(key, batch, b_pad, splits, out, st);
+  }
+  return LC_ERR_UNSUPPORTED;
+}
+
 template <class E>
 static int commit_core(lc_ajtai_key* key, size_t batch, uint32_t b_pad, void* out, cudaStream_t st) {
   const uint32_t n = key->n, m = key->m, kappa = key->k;
@@ -1031,6 +1140,11 @@ static int commit_core(lc_ajtai_key* key, size_t batch, uint32_t b_pad, void* ou
   }
   rc = map_cuda(cudaGetLastError());
   if (rc) return rc;
+  if (tiled) {
+    // few K splits: their sums and the inverse transforms in one launch
+    rc = sum_intt<E>(key, batch, b_pad, splits, out, st);
+    if (rc != LC_ERR_UNSUPPORTED) return rc;
+  }
   {
     const size_t total = (size_t)batch * kappa * n;
     const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, 65535);
