@@ -22,6 +22,7 @@
 #include "arith.cuh"
 #include "common.cuh"
 #include "internal.h"
+#include "ntt_kernels.cuh"
 
 namespace lc {
 
@@ -75,6 +76,192 @@ int crt_residues(const lc_ntt_plan* plan, const uint64_t* z, size_t count, uint3
   return map_cuda(cudaGetLastError());
 }
 
+// The CRT branch in one pass over z: every CTA brings tiles of P ring
+// elements of z (u64) into shared memory by TMA (a ring of STAGES tiles) and,
+// for each prime of the set, reduces them mod q (the canonical remainder, as
+// crt_residues_kernel), transforms them in shared memory (the forward
+// transform of ntt_tile_kernel) and writes them to out[prime][..] with bulk
+// stores.  z is read once and the residues never go through HBM: 1.5 bytes
+// of traffic per residue instead of 3.5 for the two separate launches.  Two
+// residue buffers alternate, so one prime's bulk stores drain while the next
+// prime's residues are formed.
+struct CrtNttParams {
+  NttParams np;  // out = [nm][count][n] residues; tw = the forward tables; q, qinv, err
+  const uint64_t* z;  // [count][n]
+  uint64_t mu[kMaxModuli];  // floor(2^64 / q)
+};
+
+template <class A, int LOG_N, int LOG_V, int NT, int STAGES>
+struct CrtNttCfg {
+  using G = Geo<LOG_N, LOG_V>;
+  using SL = Slots<A, LOG_N, LOG_V>;
+  static constexpr int P = NT / G::T;  // polynomials per tile
+  static constexpr size_t ZSTAGE = (size_t)P * G::N * 8;
+  static constexpr size_t RBUF = (size_t)P * SL::S * 4;
+  static constexpr size_t OFF_R = STAGES * ZSTAGE;
+  static constexpr size_t OFF_BAR = OFF_R + 2 * RBUF;
+  static constexpr size_t OFF_TW = (OFF_BAR + 8 * STAGES + 15) / 16 * 16;
+  static constexpr int TW_ENTRIES = G::fwd_entries();
+  static size_t smem(uint32_t nm) { return OFF_TW + (size_t)nm * TW_ENTRIES * sizeof(typename A::Tw); }
+  static_assert(ZSTAGE % 16 == 0 && RBUF % 16 == 0, "bulk copy alignment");
+};
+
+template <class A, int LOG_N, int LOG_V, int NT, int STAGES>
+__global__ void __launch_bounds__(NT) crt_ntt_kernel(const __grid_constant__ CrtNttParams p) {
+  using C = CrtNttCfg<A, LOG_N, LOG_V, NT, STAGES>;
+  using G = typename C::G;
+  using Tw = typename A::Tw;
+  constexpr int N = G::N, TT = G::T, S = C::SL::S, P = C::P;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* zst = reinterpret_cast<uint64_t*>(smem_raw);
+  uint32_t* rbuf = reinterpret_cast<uint32_t*>(smem_raw + C::OFF_R);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + C::OFF_BAR);
+  Tw* tw = reinterpret_cast<Tw*>(smem_raw + C::OFF_TW);
+  const uint32_t nm = p.np.num_moduli;
+  const int tid = threadIdx.x;
+  const int grp = tid / TT;
+  const uint32_t t = (uint32_t)(tid % TT);
+  {
+    const Tw* src = reinterpret_cast<const Tw*>(p.np.tw);
+    for (uint32_t mi = 0; mi < nm; ++mi)
+      for (int i = tid; i < C::TW_ENTRIES; i += NT)
+        tw[mi * C::TW_ENTRIES + i] = src[(size_t)mi * p.np.tw_stride + i];
+  }
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; ++s) mbar_init(&bar[s], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  const unsigned long long count = p.np.count;
+  uint32_t* out = static_cast<uint32_t*>(p.np.out);
+  const uint32_t ntiles = (uint32_t)((count + P - 1) / P);
+  const uint32_t stride = gridDim.x;
+  auto valid = [&](uint32_t tile) -> int {
+    const unsigned long long first = (unsigned long long)tile * P;
+    return (int)((count - first) < (unsigned long long)P ? (count - first) : P);
+  };
+  auto issue_load = [&](uint32_t tile, int s) {
+    const uint32_t bytes = (uint32_t)(valid(tile) * N * 8);
+    mbar_arrive_expect_tx(&bar[s], bytes);
+    bulk_g2s(zst + (size_t)s * P * N, p.z + (size_t)tile * P * N, bytes, &bar[s]);
+  };
+  if (tid == 0) {
+    for (int k = 0; k < STAGES - 1; ++k) {
+      const unsigned long long tk = blockIdx.x + (unsigned long long)k * stride;
+      if (tk < ntiles) issue_load((uint32_t)tk, k);
+    }
+  }
+  uint32_t parity = 0;
+  bool refilled = false;
+  int failed_at = -1;
+  uint32_t use = 0;  // residue buffers used so far (they alternate)
+  uint32_t tile = blockIdx.x;
+  for (int i = 0; tile < ntiles; ++i, tile += stride) {
+    const int s = i % STAGES;
+    if (tid == 0) {
+      // the stage consumed by iteration i-1 is free: every thread passed the
+      // barriers after its last residue reads
+      refilled = false;
+      const unsigned long long ahead = tile + (unsigned long long)(STAGES - 1) * stride;
+      if (ahead < ntiles) {
+        issue_load((uint32_t)ahead, (i + STAGES - 1) % STAGES);
+        refilled = true;
+      }
+    }
+    const bool ok = mbar_wait(&bar[s], (parity >> s) & 1u);
+    parity ^= 1u << s;
+    if (__syncthreads_or(!ok)) {
+      failed_at = i;
+      break;
+    }
+    const uint64_t* zt = zst + (size_t)s * P * N;
+    const int nv = valid(tile);
+    for (uint32_t mi = 0; mi < nm; ++mi, ++use) {
+      uint32_t* rb = rbuf + (use & 1) * (C::RBUF / 4);
+      if (tid == 0) bulk_wait_read<1>();  // the stores that last read rb (two primes ago) are done
+      __syncthreads();
+      const uint32_t q = p.np.q[mi];
+      const uint64_t mu = p.mu[mi];
+      for (int e = tid; e < P * N; e += NT) {
+        const uint64_t x = zt[e];
+        const uint64_t r = x - __umul64hi(x, mu) * q;  // < 2q
+        rb[(e / N) * S + e % N] = (uint32_t)(r >= q ? r - q : r);
+      }
+      __syncthreads();
+      const A ar = make_arith<A>(p.np, mi);
+      transform_slot<A, LOG_N, LOG_V, false>(rb + grp * S, tw + mi * C::TW_ENTRIES, ar, t);
+      fence_proxy_async_smem();
+      __syncthreads();
+      if (tid == 0) {
+        uint32_t* dst = out + ((size_t)mi * count + (size_t)tile * P) * N;
+        for (int qq = 0; qq < nv; ++qq) bulk_s2g(dst + (size_t)qq * N, rb + qq * S, N * 4);
+        bulk_commit();
+      }
+    }
+  }
+  if (tid == 0) {
+    if (failed_at >= 0) {
+      record_error(p.np.err, LC_DEVERR_TIMEOUT);
+      // loads still in flight must land before the CTA exits (bounded waits;
+      // the timed-out stage is not waited for again)
+      for (int k = 1; k < STAGES; ++k) {
+        const unsigned long long tk = tile + (unsigned long long)k * stride;
+        const bool issued = (k < STAGES - 1) || refilled;
+        if (tk >= ntiles || !issued) continue;
+        const int sk = (failed_at + k) % STAGES;
+        mbar_wait(&bar[sk], (parity >> sk) & 1u);
+      }
+    }
+    bulk_wait<0>();
+  }
+}
+
+template <class A>
+static int launch_crt_ntt(const lc_ntt_plan* plan, const uint64_t* z, size_t count, uint32_t* out,
+                          cudaStream_t st) {
+  constexpr int NT = 128, STAGES = 3;
+  using C = CrtNttCfg<A, 6, 3, NT, STAGES>;
+  auto kern = crt_ntt_kernel<A, 6, 3, NT, STAGES>;
+  const size_t smem = C::smem(plan->num_moduli);
+  static std::atomic<uint64_t> attr_done{0};
+  cudaError_t e = smem_attr_once(attr_done, kern, C::smem(kMaxModuli));
+  if (e != cudaSuccess) return map_cuda(e);
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem);
+  if (e != cudaSuccess) return map_cuda(e);
+  per_sm = std::max(per_sm, 1);
+  CrtNttParams p{};
+  p.np.out = out;
+  p.np.count = count;
+  p.np.tw = plan->d_tw_fwd;
+  p.np.tw_stride = plan->tw_fwd_entries;
+  p.np.num_moduli = plan->num_moduli;
+  p.np.err = plan->d_err;
+  for (uint32_t i = 0; i < plan->num_moduli; ++i) {
+    p.np.q[i] = plan->q[i];
+    p.np.qinv[i] = plan->qinv[i];
+    p.mu[i] = ~0ull / plan->q[i];
+  }
+  p.z = z;
+  const unsigned long long ntiles = (count + C::P - 1) / C::P;
+  const unsigned long long gx =
+      std::max<unsigned long long>(1, std::min<unsigned long long>(ntiles, (unsigned long long)device_sm_count() * per_sm));
+  kern<<<(unsigned)gx, NT, smem, st>>>(p);
+  return map_cuda(cudaGetLastError());
+}
+
+// Residues of z under the plan's moduli, forward-transformed, in one launch:
+// out[mod][count][64] = NTT(z mod q_mod).  d = 64 u32 plans only
+// (LC_ERR_UNSUPPORTED otherwise: the caller runs crt_residues + the NTT).
+int crt_ntt_forward(const lc_ntt_plan* plan, const uint64_t* z, size_t count, uint32_t* out, cudaStream_t st) {
+  if (count == 0) return LC_OK;
+  if (plan->log_n != 6 || count > ((size_t)1 << 29)) return LC_ERR_UNSUPPORTED;
+  if (((uintptr_t)z & 15) || ((uintptr_t)out & 15)) return LC_ERR_UNSUPPORTED;
+  if (plan->kind == PlanKind::U32Lazy) return launch_crt_ntt<ShoupLazy>(plan, z, count, out, st);
+  if (plan->kind == PlanKind::U32Mont) return launch_crt_ntt<MontCanon>(plan, z, count, out, st);
+  return LC_ERR_UNSUPPORTED;
+}
+
 }  // namespace lc
 
 struct lc_fold_pipeline {
@@ -103,8 +290,11 @@ static int fold_stages(lc_fold_pipeline* f, cudaStream_t st) {
   cudaError_t e = cudaEventRecord(f->ev_fork, st);
   if (e == cudaSuccess) e = cudaStreamWaitEvent(f->side, f->ev_fork, 0);
   if (e != cudaSuccess) return map_cuda(e);
-  int rc_crt = crt_residues(f->crt, f->z, coeffs, f->crt_out, f->side);
-  if (!rc_crt) rc_crt = lc_ntt_forward(f->crt, f->crt_out, f->crt_out, f->m, f->side);
+  int rc_crt = crt_ntt_forward(f->crt, f->z, f->m, f->crt_out, f->side);
+  if (rc_crt == LC_ERR_UNSUPPORTED) {
+    rc_crt = crt_residues(f->crt, f->z, coeffs, f->crt_out, f->side);
+    if (!rc_crt) rc_crt = lc_ntt_forward(f->crt, f->crt_out, f->crt_out, f->m, f->side);
+  }
   int rc = lc_decomp_b(f->z, coeffs, 8, f->digits, st);
   if (!rc) rc = lc_ajtai_commit_u8(f->key, f->digits, 8, f->commits, st);
   // join: st continues after both branches (also closes the side stream's

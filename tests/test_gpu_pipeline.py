@@ -87,6 +87,30 @@ def test_fold_pipeline_small(use_graph, products):
     pipe.check()
 
 
+def test_fold_pipeline_crt_branch_montgomery_moduli():
+    """The CRT branch (residues of z formed in shared memory and transformed
+    in the same launch) over a plan of primes above 2^30, which run the
+    signed-Montgomery arithmetic: every row equals the oracle's NTT of
+    z mod q, with a ragged last tile (m = 333)."""
+    from lzx_b200 import Modulus32
+    kappa, m = 2, 333
+    A = synth.synth_gl(32, 0, kappa * m * 64)
+    key = GoldilocksAjtaiKey(6, kappa, m, A.reshape(kappa, m, 64))
+    mods = [Modulus32.Q_32, Modulus32.Q_2013265921]
+    crt = NttTables(mods, 6)
+    pipe = FoldPipeline(key, crt, use_graph=False)
+    z = synth.synth_u64(32, 1, m * 64)
+    pipe.z.copy_(torch.from_numpy(z.view(np.int64)).reshape(m, 64))
+    pipe.run()
+    pipe.check()
+    torch.cuda.synchronize()
+    got = pipe.crt_ntt.cpu().numpy().view(np.uint32).reshape(len(mods), m, 64)
+    for i, md in enumerate(mods):
+        tb = oracle.NttTables32(oracle.Modulus32(md.q, md.two_adicity, md.generator), 6)
+        want = tb.forward_batch((z % np.uint64(md.q)).astype(np.uint32).reshape(m, 64))
+        assert np.array_equal(got[i], want), md.q
+
+
 def test_fold_pipeline_folding_size():
     """2^20 ring elements, kappa = 16 (the folding-step workload)."""
     kappa, m = 16, 1 << 20
