@@ -603,9 +603,11 @@ LC_D uint32_t tw_fold(const uint32_t* x, uint32_t q, uint32_t c, int64_t off) {
 }
 
 // Goldilocks: v = A + 2^32 B with A, B the limb sums 0-3 and 4-7 (|A|, |B|
-// <= 256 128 255 (1 + 2^8 + 2^16 + 2^24) < 2^47.01), reduced mod p with
-// 2^64 == 2^32 - 1: A + (B >> 32)(2^32 - 1) + 2^49 lies in (0, 2^50); adding
-// (B mod 2^32) 2^32 wraps at most once, and one step removes the offset.
+// <= 256 128 255 (1 + 2^8 + 2^16 + 2^24) < 2^47.01), returned as a 64-bit
+// value congruent mod p, not necessarily canonical (the products read any
+// 64-bit representative): S = A + hi(B) (2^32 - 1), |S| < 2^48.02; U = S +
+// 2^32 lo(B) = R + k 2^64 with R = U mod 2^64, k = carry - [S < 0], and the
+// value R + k (2^32 - 1) stays inside [0, 2^64) (the reasoning of tn_fold).
 LC_D uint64_t tw_fold_gl(const uint32_t* x) {
   int64_t A = (int32_t)x[0], B = (int32_t)x[4];
   A += (int64_t)(int32_t)x[1] * 256;
@@ -614,11 +616,11 @@ LC_D uint64_t tw_fold_gl(const uint32_t* x) {
   B += (int64_t)(int32_t)x[6] * 65536;
   A += (int64_t)(int32_t)x[3] * 16777216;
   B += (int64_t)(int32_t)x[7] * 16777216;
-  const uint64_t t = (uint64_t)(A + (B >> 32) * (int64_t)0xFFFFFFFFll + ((int64_t)1 << 49));
-  uint64_t r = t + ((uint64_t)(uint32_t)B << 32);
-  if (r < t) r += 0xFFFFFFFFull;
-  constexpr uint64_t kOff = 1ull << 49;
-  return r - kOff + (r < kOff ? kGlP : 0);
+  const int64_t S = A + (B >> 32) * (int64_t)0xFFFFFFFFll;
+  const uint64_t lo = (uint64_t)(uint32_t)B << 32;
+  const uint64_t R = (uint64_t)S + lo;
+  const int k = (int)(R < lo) - (int)(S < 0);
+  return R + (uint64_t)(int64_t)k * 0xFFFFFFFFull;
 }
 
 // limbs of a lane's V image (8 Goldilocks, 4 u32) and its passes of PN columns

@@ -379,12 +379,17 @@ struct TnParams {
   uint32_t* err;
 };
 
-// sum_l 2^(8l) D_l mod p for one output (|D_l| < 2^22).  A = D0 + 2^8 D1 +
-// 2^16 D2 + 2^24 D3 and B (limbs 4..7) are exact in int64 (|A|, |B| < 2^47);
-// the value is A + B 2^32 and B 2^32 = lo(B) 2^32 + hi(B) 2^64 with
-// 2^64 == 2^32 - 1 (mod p), |hi(B)| < 2^15.  The offset 2^48 keeps
-// A + hi(B) (2^32 - 1) positive and below 2^49; adding lo(B) 2^32 wraps 2^64
-// at most once, folded as 2^32 - 1; the offset comes off mod p at the end.
+// sum_l 2^(8l) D_l mod p for one output (|D_l| < 2^22), as a 64-bit value
+// congruent mod p but not necessarily canonical (it may lie in [p, 2^64)):
+// every reader of the witness transforms -- the byte-limb slot products and
+// the 160-bit integer products -- takes any 64-bit representative.  A = D0 +
+// 2^8 D1 + 2^16 D2 + 2^24 D3 and B (limbs 4..7) are exact in int64 (|A|,
+// |B| < 2^47); the value is A + 2^32 B == S + 2^32 lo(B) with
+// S = A + hi(B) (2^32 - 1) (2^64 == 2^32 - 1 mod p), |S| < 2^48.  With
+// U = S + 2^32 lo(B) in (-2^48, 2^64 + 2^48), R = U mod 2^64 and
+// U = R + k 2^64, k = carry - [S < 0] in {-1, 0, 1}: the value is
+// R + k (2^32 - 1), which stays inside [0, 2^64) in each case (k = 1 only
+// when R < 2^48, k = -1 only when R > 2^64 - 2^48).
 LC_D uint64_t tn_fold(const uint32_t (&d)[8][8], int u) {
   // limb pairs in 32 bits: |D| < 2^21 (s8 digits) or 0 <= D < 2^22 (u8), so
   // D_l + 2^8 D_(l+1) stays inside int32
@@ -394,13 +399,11 @@ LC_D uint64_t tn_fold(const uint32_t (&d)[8][8], int u) {
   const int32_t p67 = (int32_t)d[6][u] + (int32_t)d[7][u] * 256;
   const int64_t A = (int64_t)p01 + (int64_t)p23 * 65536;
   const int64_t B = (int64_t)p45 + (int64_t)p67 * 65536;
-  const uint64_t t = (uint64_t)(A + (B >> 32) * (int64_t)kGlEps + ((int64_t)1 << 48));  // in (0, 2^49)
-  uint64_t r = t + ((uint64_t)(uint32_t)B << 32);
-  if (r < t) r += kGlEps;  // no second wrap: r < 2^49 after the first
-  // r - 2^48 is canonical for r >= 2^48 (r - 2^48 < 2^64 - 2^48 < p);
-  // below, adding p once brings it into [0, p)
-  constexpr uint64_t kOff = (uint64_t)1 << 48;
-  return r - kOff + (r < kOff ? kGlP : 0);
+  const int64_t S = A + (B >> 32) * (int64_t)kGlEps;
+  const uint64_t lo = (uint64_t)(uint32_t)B << 32;
+  const uint64_t R = (uint64_t)S + lo;
+  const int k = (int)(R < lo) - (int)(S < 0);
+  return R + (uint64_t)(int64_t)k * kGlEps;
 }
 
 template <bool S8>
