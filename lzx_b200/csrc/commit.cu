@@ -717,7 +717,7 @@ __global__ void __launch_bounds__(256, 2) commit_mac_intt_kernel(const __grid_co
 // ------------------------------------------------------------------ split sums and inverse NTT in one launch
 //
 // After the tiled products (a handful of K splits), the rest of ajtai.rs:
-// 139-150 for GROUPS output rows per CTA: rows (b0 .. b0 + GROUPS - 1, i),
+// 139-150 for ROWS output rows per CTA: rows (b0 .. b0 + ROWS - 1, i),
 // summed over the splits straight into shared-memory slots (consecutive
 // threads take consecutive witnesses b, so every read of
 // partial[split][t][i][b] is one contiguous run), inverse-transformed there
@@ -733,15 +733,16 @@ template <class A, int LOG_N, int LOG_V>
 struct SumInttCfg {
   using E = typename A::T;
   using G = Geo<LOG_N, LOG_V>;
-  static constexpr int NT = 128;
-  static constexpr int ROWS = NT / G::T;  // one transform pass
+  static constexpr int NT = 256;          // the split sums: all threads
+  static constexpr int XT = 128;          // the transform: the first four warps
+  static constexpr int ROWS = XT / G::T;  // one transform pass
   static constexpr int SS = WitnessSlotStride<A, LOG_N>::value;
   static constexpr size_t TWI = ((size_t)G::inv_entries() * sizeof(typename A::Tw) + 15) / 16 * 16;
   static constexpr size_t SMEM = TWI + (size_t)ROWS * SS * sizeof(E);
 };
 
 template <class A, int LOG_N, int LOG_V>
-__global__ void __launch_bounds__(128) sum_intt_kernel(const __grid_constant__ SumInttParams p) {
+__global__ void __launch_bounds__(256) sum_intt_kernel(const __grid_constant__ SumInttParams p) {
   using C = SumInttCfg<A, LOG_N, LOG_V>;
   using E = typename A::T;
   using Tw = typename A::Tw;
@@ -760,13 +761,21 @@ __global__ void __launch_bounds__(128) sum_intt_kernel(const __grid_constant__ S
     E s = 0;
     if (b < p.batch) {
       const E* src = part + ((size_t)t * kIPad + i) * p.b_pad + b;
-      for (uint32_t sp = 0; sp < p.splits; ++sp) s = Field<E>::add(s, __ldg(src + sp * sstride), p.q);
+      for (uint32_t sp = 0; sp < p.splits; sp += 8) {  // up to eight loads in flight, then their sum
+        E v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = sp + k < p.splits ? __ldg(src + (sp + k) * sstride) : E(0);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) s = Field<E>::add(s, v[k], p.q);
+      }
     }
     slots[rr * SS + t] = s;
   }
   __syncthreads();
-  const A ar = make_arith_q<A>(p.q, p.qinv);
-  transform_slot<A, LOG_N, LOG_V, true>(slots + (tid / G::T) * SS, twi, ar, (uint32_t)(tid % G::T));
+  if (tid < C::XT) {  // whole warps: the transform's __syncwarp sees all its lanes
+    const A ar = make_arith_q<A>(p.q, p.qinv);
+    transform_slot<A, LOG_N, LOG_V, true>(slots + (tid / G::T) * SS, twi, ar, (uint32_t)(tid % G::T));
+  }
   __syncthreads();
   E* out = static_cast<E*>(p.out);
   for (int e = tid; e < ROWS * N; e += C::NT) {

@@ -78,13 +78,13 @@ int crt_residues(const lc_ntt_plan* plan, const uint64_t* z, size_t count, uint3
 
 // The CRT branch in one pass over z: every CTA brings tiles of P ring
 // elements of z (u64) into shared memory by TMA (a ring of STAGES tiles) and,
-// for each prime of the set, reduces them mod q (the canonical remainder, as
-// crt_residues_kernel), transforms them in shared memory (the forward
-// transform of ntt_tile_kernel) and writes them to out[prime][..] with bulk
-// stores.  z is read once and the residues never go through HBM: 1.5 bytes
-// of traffic per residue instead of 3.5 for the two separate launches.  Two
-// residue buffers alternate, so one prime's bulk stores drain while the next
-// prime's residues are formed.
+// for each prime of the set, every thread group reduces its ring element mod
+// q into its own shared-memory slot (the canonical remainder, as
+// crt_residues_kernel), transforms it there (the forward transform of
+// ntt_tile_kernel) and stores it to out[prime][..] with 16-byte stores -- z
+// is read once and the residues never go through HBM: 1.5 bytes of traffic
+// per residue instead of 3.5 for the two separate launches.  A group
+// synchronises only its own warp; the CTA meets once per tile.
 struct CrtNttParams {
   NttParams np;  // out = [nm][count][n] residues; tw = the forward tables; q, qinv, err
   const uint64_t* z;  // [count][n]
@@ -95,15 +95,16 @@ template <class A, int LOG_N, int LOG_V, int NT, int STAGES>
 struct CrtNttCfg {
   using G = Geo<LOG_N, LOG_V>;
   using SL = Slots<A, LOG_N, LOG_V>;
-  static constexpr int P = NT / G::T;  // polynomials per tile
+  static constexpr int P = NT / G::T;  // polynomials per tile, one per thread group
   static constexpr size_t ZSTAGE = (size_t)P * G::N * 8;
   static constexpr size_t RBUF = (size_t)P * SL::S * 4;
   static constexpr size_t OFF_R = STAGES * ZSTAGE;
-  static constexpr size_t OFF_BAR = OFF_R + 2 * RBUF;
+  static constexpr size_t OFF_BAR = OFF_R + RBUF;
   static constexpr size_t OFF_TW = (OFF_BAR + 8 * STAGES + 15) / 16 * 16;
   static constexpr int TW_ENTRIES = G::fwd_entries();
   static size_t smem(uint32_t nm) { return OFF_TW + (size_t)nm * TW_ENTRIES * sizeof(typename A::Tw); }
-  static_assert(ZSTAGE % 16 == 0 && RBUF % 16 == 0, "bulk copy alignment");
+  static_assert(ZSTAGE % 16 == 0 && (SL::S * 4) % 16 == 0, "16-byte alignment");
+  static_assert(G::N % (4 * G::T) == 0, "whole 16-byte stores per thread");
 };
 
 template <class A, int LOG_N, int LOG_V, int NT, int STAGES>
@@ -112,6 +113,7 @@ __global__ void __launch_bounds__(NT) crt_ntt_kernel(const __grid_constant__ Crt
   using G = typename C::G;
   using Tw = typename A::Tw;
   constexpr int N = G::N, TT = G::T, S = C::SL::S, P = C::P;
+  constexpr int PER = N / TT;  // values per thread of a group
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t* zst = reinterpret_cast<uint64_t*>(smem_raw);
   uint32_t* rbuf = reinterpret_cast<uint32_t*>(smem_raw + C::OFF_R);
@@ -134,6 +136,7 @@ __global__ void __launch_bounds__(NT) crt_ntt_kernel(const __grid_constant__ Crt
   __syncthreads();
   const unsigned long long count = p.np.count;
   uint32_t* out = static_cast<uint32_t*>(p.np.out);
+  uint32_t* slot = rbuf + grp * S;  // this group's ring element
   const uint32_t ntiles = (uint32_t)((count + P - 1) / P);
   const uint32_t stride = gridDim.x;
   auto valid = [&](uint32_t tile) -> int {
@@ -154,13 +157,12 @@ __global__ void __launch_bounds__(NT) crt_ntt_kernel(const __grid_constant__ Crt
   uint32_t parity = 0;
   bool refilled = false;
   int failed_at = -1;
-  uint32_t use = 0;  // residue buffers used so far (they alternate)
   uint32_t tile = blockIdx.x;
   for (int i = 0; tile < ntiles; ++i, tile += stride) {
     const int s = i % STAGES;
     if (tid == 0) {
       // the stage consumed by iteration i-1 is free: every thread passed the
-      // barriers after its last residue reads
+      // barrier that ends each iteration
       refilled = false;
       const unsigned long long ahead = tile + (unsigned long long)(STAGES - 1) * stride;
       if (ahead < ntiles) {
@@ -174,45 +176,42 @@ __global__ void __launch_bounds__(NT) crt_ntt_kernel(const __grid_constant__ Crt
       failed_at = i;
       break;
     }
-    const uint64_t* zt = zst + (size_t)s * P * N;
-    const int nv = valid(tile);
-    for (uint32_t mi = 0; mi < nm; ++mi, ++use) {
-      uint32_t* rb = rbuf + (use & 1) * (C::RBUF / 4);
-      if (tid == 0) bulk_wait_read<1>();  // the stores that last read rb (two primes ago) are done
-      __syncthreads();
+    const uint64_t* zt = zst + (size_t)s * P * N + (size_t)grp * N;
+    const bool mine = grp < valid(tile);
+    for (uint32_t mi = 0; mi < nm; ++mi) {
       const uint32_t q = p.np.q[mi];
       const uint64_t mu = p.mu[mi];
-      for (int e = tid; e < P * N; e += NT) {
-        const uint64_t x = zt[e];
+#pragma unroll
+      for (int k = 0; k < PER; ++k) {
+        const uint64_t x = zt[t + k * TT];
         const uint64_t r = x - __umul64hi(x, mu) * q;  // < 2q
-        rb[(e / N) * S + e % N] = (uint32_t)(r >= q ? r - q : r);
+        slot[t + k * TT] = (uint32_t)(r >= q ? r - q : r);
       }
-      __syncthreads();
+      __syncwarp();
       const A ar = make_arith<A>(p.np, mi);
-      transform_slot<A, LOG_N, LOG_V, false>(rb + grp * S, tw + mi * C::TW_ENTRIES, ar, t);
-      fence_proxy_async_smem();
-      __syncthreads();
-      if (tid == 0) {
-        uint32_t* dst = out + ((size_t)mi * count + (size_t)tile * P) * N;
-        for (int qq = 0; qq < nv; ++qq) bulk_s2g(dst + (size_t)qq * N, rb + qq * S, N * 4);
-        bulk_commit();
+      transform_slot<A, LOG_N, LOG_V, false>(slot, tw + mi * C::TW_ENTRIES, ar, t);
+      __syncwarp();
+      if (mine) {
+        uint4* dst = reinterpret_cast<uint4*>(out + ((size_t)mi * count + (size_t)tile * P + grp) * N + t * PER);
+        const uint4* src = reinterpret_cast<const uint4*>(slot + t * PER);
+#pragma unroll
+        for (int k = 0; k < PER / 4; ++k) dst[k] = src[k];
       }
+      __syncwarp();  // the slot is read out before the next prime's residues
     }
+    __syncthreads();  // the z stage is read out before its refill
   }
-  if (tid == 0) {
-    if (failed_at >= 0) {
-      record_error(p.np.err, LC_DEVERR_TIMEOUT);
-      // loads still in flight must land before the CTA exits (bounded waits;
-      // the timed-out stage is not waited for again)
-      for (int k = 1; k < STAGES; ++k) {
-        const unsigned long long tk = tile + (unsigned long long)k * stride;
-        const bool issued = (k < STAGES - 1) || refilled;
-        if (tk >= ntiles || !issued) continue;
-        const int sk = (failed_at + k) % STAGES;
-        mbar_wait(&bar[sk], (parity >> sk) & 1u);
-      }
+  if (tid == 0 && failed_at >= 0) {
+    record_error(p.np.err, LC_DEVERR_TIMEOUT);
+    // loads still in flight must land before the CTA exits (bounded waits;
+    // the timed-out stage is not waited for again)
+    for (int k = 1; k < STAGES; ++k) {
+      const unsigned long long tk = tile + (unsigned long long)k * stride;
+      const bool issued = (k < STAGES - 1) || refilled;
+      if (tk >= ntiles || !issued) continue;
+      const int sk = (failed_at + k) % STAGES;
+      mbar_wait(&bar[sk], (parity >> sk) & 1u);
     }
-    bulk_wait<0>();
   }
 }
 
