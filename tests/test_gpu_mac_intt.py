@@ -88,6 +88,29 @@ def test_u32_one_launch_equals_staged_and_oracle(modulus, log_n, k, m, batch):
         assert np.array_equal(fused[b], oracle.ajtai32_commit_naive(t, pk._matrix, k, m, W[b]))
 
 
+def test_key_view_tiled_products_match_oracle():
+    """128 witnesses on a view (rows a_m = 3000 apart, m = 2333 committed):
+    the tiled integer products, then the split sums and inverse transforms
+    in one launch, equal the oracle's commitment under the view's sub-matrix."""
+    kappa, m, log_d = 8, 3000, 6
+    A = synth.synth_gl(6, 0, kappa * m * 64).reshape(kappa, m, 64)
+    key = GoldilocksAjtaiKey(log_d, kappa, m, A)
+    kv, nv, batch = 5, 2333, 128
+    view = key_view(key, kv, nv)
+    L = _lib.lib()
+    assert L.lc_ajtai_key_set_slot_products(view.handle, INT64) == 0
+    W = synth.synth_i8(14, 1, batch * nv * 64).reshape(batch, nv, 64)
+    w = torch.from_numpy(W).cuda()
+    out = torch.empty((batch, kv, 64), dtype=torch.int64, device="cuda")
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    assert L.lc_ajtai_commit_i8(view.handle, C.c_void_p(w.data_ptr()), batch, C.c_void_p(out.data_ptr()), st) == 0
+    assert L.lc_ajtai_key_check(view.handle, st) == 0
+    t = oracle.NttTablesGl(log_d)
+    sub = np.ascontiguousarray(A[:kv, :nv]).reshape(-1, 64)
+    want = oracle.ajtaigl_commit_batch(t, t.forward_batch(sub), kv, nv, W)
+    assert np.array_equal(out.cpu().numpy().view(np.uint64).reshape(want.shape), want)
+
+
 def test_key_view_one_launch():
     """A view's row stride differs from its width; the one-launch form reads it."""
     kappa, m, log_d = 8, 3000, 6

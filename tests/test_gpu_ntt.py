@@ -170,6 +170,50 @@ def test_host_entry_points_over_many_chunks():
     assert _lib.lib().lc_ntt_plan_check(t.handle, None) == 0
 
 
+@pytest.mark.parametrize("kind", ["crt", "q32", "goldilocks"])
+def test_host_entry_points_on_pinned_buffers(kind):
+    """Pinned host buffers through the host-buffer entry points (chunks copied
+    straight from and to them): the residues equal the device transform's,
+    out of place and in place, and for a buffer starting 4 bytes into a
+    pinned allocation, with the inverse bringing the input back each time."""
+    L = _lib.lib()
+    if kind == "goldilocks":
+        count, n, log_n = 3001, 64, 6
+        t = GoldilocksNttTables(log_n)
+        a = synth.synth_gl(41, 0, count * n).reshape(count, n)
+        tdt, ndt = torch.int64, np.uint64
+    else:
+        mods = CRT_SET_30BIT if kind == "crt" else [Modulus32.Q_32]
+        count, n, log_n = (20003, 256, 8) if kind == "crt" else (777, 128, 7)
+        t = NttTables(mods, log_n)
+        a = synth.crt_batch(43, mods, count, n) if kind == "crt" else \
+            synth.synth_mod32(43, 0, Modulus32.Q_32.q, count * n).reshape(count, n)
+        tdt, ndt = torch.int32, np.uint32
+    want = to_dev(a.copy())
+    t.forward_fast(want)
+    torch.cuda.synchronize()
+    want = from_dev(want, ndt).reshape(a.shape)
+    flat = a.reshape(-1)
+    size, eb = flat.size, flat.itemsize
+    src = torch.from_numpy(flat.view(np.int64 if eb == 8 else np.int32).copy()).pin_memory()
+    dst = torch.empty_like(src).pin_memory()
+    for inp, outp in ((src, dst), (dst, dst)):
+        if inp is dst:
+            dst.copy_(src)
+        st = L.lc_ntt_forward_host(t.handle, C.c_void_p(inp.data_ptr()), C.c_void_p(outp.data_ptr()), count)
+        assert st == 0, _lib.lib().lc_status_string(st)
+        assert np.array_equal(outp.numpy().view(ndt).reshape(a.shape), want)
+        st = L.lc_ntt_inverse_host(t.handle, C.c_void_p(outp.data_ptr()), C.c_void_p(outp.data_ptr()), count)
+        assert st == 0
+        assert np.array_equal(outp.numpy().view(ndt).reshape(a.shape), a)
+    big = torch.zeros(size + 16 // eb, dtype=tdt).pin_memory()
+    big[1:1 + size] = src
+    p = C.c_void_p(big.data_ptr() + eb)
+    assert L.lc_ntt_forward_host(t.handle, p, p, count) == 0
+    assert np.array_equal(big[1:1 + size].numpy().view(ndt).reshape(a.shape), want)
+    assert L.lc_ntt_plan_check(t.handle, None) == 0
+
+
 def test_full_size_crt_round_trip_and_samples():
     """2^16 polynomials x d=256 x 4 primes: the bench workload."""
     count, n = 1 << 16, 256
