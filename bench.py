@@ -19,7 +19,8 @@ each coefficient once, 2^27 per step).
   launch (4 B read + 4 B written) over its CUDA-event duration, against the
   measured HBM copy bandwidth.
 * cpu_baseline: the oracle restatement of the reference's forward_fast /
-  inverse_fast on this host's cores (a bounded sample).
+  inverse_fast on this host's cores (a bounded sample), timed in single-GPU
+  runs only.
 * --impl reference: the reference's CPU path (its scalar algorithm restated in
   C, the Rust reference cannot be built here) on all host threads, same
   metric and unit.
@@ -1323,6 +1324,9 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        # the CPU baselines are timed at N = 1 only (rank 0 of a single-GPU run)
+        args.no_cpu_baseline = True
     if args.commit_only or args.only:
         return run_only(args, args.only or "commit")
     return run_ours(args)
