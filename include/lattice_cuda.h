@@ -166,7 +166,12 @@ LC_API int lc_ajtai_commit_i8(lc_ajtai_key *key, const int8_t *s, size_t batch, 
  * b <= 8, lattice-folding/src/neo.rs:253-266, each row one witness). */
 LC_API int lc_ajtai_commit_u8(lc_ajtai_key *key, const uint8_t *s, size_t batch, void *out,
                               lc_stream stream);
-/* Host-buffer variants (synchronous). */
+/* Host-buffer variants (synchronous).  Small commitments (those the
+ * single-launch kernel takes: at most 4 witnesses, 2048 ring elements) run
+ * that kernel directly on page-locked host memory -- the caller's buffers
+ * when they are pinned (output 16-byte aligned), else the key's pinned
+ * staging buffers -- with no copies queued; larger ones upload, commit on
+ * the device and download. */
 LC_API int lc_ajtai_commit_host(lc_ajtai_key *key, const void *s, size_t batch, void *out);
 LC_API int lc_ajtai_commit_i8_host(lc_ajtai_key *key, const int8_t *s, size_t batch, void *out);
 LC_API int lc_ajtai_commit_u8_host(lc_ajtai_key *key, const uint8_t *s, size_t batch, void *out);

@@ -1598,6 +1598,19 @@ static bool host_pinned(const void* p) {
   return a.type == cudaMemoryTypeHost;
 }
 
+// Device address of page-locked host memory (mapped into the device address
+// space under unified addressing); false for pageable and device memory.
+static bool mapped_host(const void* p, void** dev) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (a.type != cudaMemoryTypeHost || a.devicePointer == nullptr) return false;
+  *dev = a.devicePointer;
+  return true;
+}
+
 static int grow_pinned(void** p, size_t* have, size_t need) {
   if (need <= *have) return LC_OK;
   if (*p) cudaFreeHost(*p);
@@ -1640,6 +1653,35 @@ static int commit_host(lc_ajtai_key* key, const void* s, size_t in_elem, size_t 
     if (rc) return rc;
   }
   cudaStream_t st = key->host_stream;
+  {
+    // a commitment small enough for the single-launch kernel, with input and
+    // output in page-locked host memory (the staging buffers or the caller's):
+    // the kernel reads the witness and writes the rows over the host link
+    // itself, so neither copy is queued
+    const void* hin = stage_in ? key->h_stage_in : s;
+    void* hout = stage_out ? key->h_stage_out : out;
+    void* din = nullptr;
+    void* dout = nullptr;
+    if (key->engine == LC_ENGINE_NTT && mapped_host(hin, &din) && mapped_host(hout, &dout) &&
+        reinterpret_cast<uintptr_t>(din) % in_elem == 0 && (reinterpret_cast<uintptr_t>(dout) & 15) == 0) {
+      int frc = LC_ERR_UNSUPPORTED;
+      if (in_elem == 1)
+        frc = i8 ? commit_fused<int8_t>(key, static_cast<const int8_t*>(din), batch, dout, st)
+                 : commit_fused<uint8_t>(key, static_cast<const uint8_t*>(din), batch, dout, st);
+      else if (key->wide)
+        frc = commit_fused<uint64_t>(key, static_cast<const uint64_t*>(din), batch, dout, st);
+      else
+        frc = commit_fused<uint32_t>(key, static_cast<const uint32_t*>(din), batch, dout, st);
+      if (frc != LC_ERR_UNSUPPORTED) {
+        // the single-launch kernel has no bounded waits and sets no error word
+        const cudaError_t e = cudaStreamSynchronize(st);
+        if (frc) return frc;
+        if (e != cudaSuccess) return map_cuda(e);
+        if (stage_out) std::memcpy(out, key->h_stage_out, out_bytes);
+        return LC_OK;
+      }
+    }
+  }
   if (cudaMemcpyAsync(key->d_in, stage_in ? key->h_stage_in : s, in_bytes, cudaMemcpyHostToDevice, st) !=
       cudaSuccess)
     return map_cuda(cudaGetLastError());

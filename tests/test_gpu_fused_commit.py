@@ -144,3 +144,48 @@ def test_fused_switch_arguments():
     assert L.lc_ajtai_key_get_fused(None) == -1
     assert L.lc_ajtai_key_set_fused(key.handle, 0) == 0
     assert L.lc_ajtai_key_get_fused(key.handle) == 0
+
+
+@pytest.mark.parametrize("kind", ["i8", "u8", "residues"])
+def test_host_call_reads_and_writes_host_memory(kind):
+    """A synchronous host call of a small commitment runs the single-launch
+    kernel straight on page-locked host memory (the key's staging buffers for
+    pageable arguments, or the caller's pinned buffers), with no copies
+    queued; pageable, pinned and misaligned pinned outputs all give the
+    device call's residues, on repeated calls."""
+    import ctypes as C
+    kappa, m, log_d = 8, 256, 6
+    A, key = gl_case(log_d, kappa, m, 71)
+    L = _lib.lib()
+    if kind == "residues":
+        W = synth.synth_gl(72, 1, 2 * m * 64).reshape(2, m, 64)
+        fn, dev_fn = L.lc_ajtai_commit_host, L.lc_ajtai_commit
+        wt = torch.from_numpy(W.view(np.int64))
+    else:
+        W = synth.synth_i8(72, 1, 2 * m * 64).reshape(2, m, 64)
+        if kind == "u8":
+            W = W.view(np.uint8)
+        fn = L.lc_ajtai_commit_i8_host if kind == "i8" else L.lc_ajtai_commit_u8_host
+        dev_fn = L.lc_ajtai_commit_i8 if kind == "i8" else L.lc_ajtai_commit_u8
+        wt = torch.from_numpy(W.view(np.int8))
+    wd = wt.cuda()
+    want = torch.empty((2, kappa, 64), dtype=torch.int64, device="cuda")
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    assert dev_fn(key.handle, C.c_void_p(wd.data_ptr()), 2, C.c_void_p(want.data_ptr()), st) == 0
+    torch.cuda.synchronize()
+    want = want.cpu().numpy().view(np.uint64)
+    assert np.array_equal(want, gl_oracle(A, log_d, kappa, m, W))
+    wp = wt.clone().pin_memory()
+    pinned_out = torch.zeros((2, kappa, 64), dtype=torch.int64).pin_memory()
+    big = torch.zeros(2 * kappa * 64 + 1, dtype=torch.int64).pin_memory()
+    for _ in range(2):
+        got = np.zeros((2, kappa, 64), dtype=np.uint64)  # pageable in and out: staged
+        assert fn(key.handle, W.ctypes.data_as(C.c_void_p), 2, got.ctypes.data_as(C.c_void_p)) == 0
+        assert np.array_equal(got, want)
+        # the caller's pinned buffers
+        assert fn(key.handle, C.c_void_p(wp.data_ptr()), 2, C.c_void_p(pinned_out.data_ptr())) == 0
+        assert np.array_equal(pinned_out.numpy().view(np.uint64), want)
+        # a pinned output 8 bytes into its allocation (not 16-byte aligned)
+        assert fn(key.handle, C.c_void_p(wp.data_ptr()), 2, C.c_void_p(big.data_ptr() + 8)) == 0
+        assert np.array_equal(big[1:].numpy().view(np.uint64).reshape(want.shape), want)
+    assert L.lc_ajtai_key_check(key.handle, None) == 0
