@@ -1382,25 +1382,31 @@ static int noalloc_commit(const lc_ajtai_key* key, const E* s, size_t batch, voi
 
 }  // namespace lc
 
-extern "C" {
+namespace lc {
 
-LC_API int lc_ajtai_key_create(const lc_ntt_plan* plan, uint32_t k, uint32_t m, const void* matrix,
-                               int matrix_on_device, lc_ajtai_key** out) {
-  return lc_ajtai_key_create_ex(plan, k, m, matrix, matrix_on_device, 0, out);
-}
-
-LC_API int lc_ajtai_key_create_ex(const lc_ntt_plan* plan, uint32_t k, uint32_t m, const void* matrix,
-                                  int matrix_on_device, uint32_t flags, lc_ajtai_key** out) {
-  if (!plan || !matrix || !out || k == 0 || m == 0) return LC_ERR_INVALID_ARGUMENT;
-  *out = nullptr;
+// Arguments a key can be created with (LC_OK) or the status that refuses them.
+int key_create_check(const lc_ntt_plan* plan, uint32_t k, uint32_t m, uint32_t flags) {
   if (flags & ~LC_KEY_TENSOR_I8) return LC_ERR_INVALID_ARGUMENT;
   if (plan->num_moduli != 1) return LC_ERR_UNSUPPORTED;
   if ((flags & LC_KEY_TENSOR_I8) && (plan->kind != PlanKind::Goldilocks || plan->log_n != 6))
     return LC_ERR_UNSUPPORTED;
   if (k > (uint32_t)kIPad) return LC_ERR_UNSUPPORTED;
   if (plan->log_n > (plan->kind == PlanKind::Goldilocks ? 9u : 10u)) return LC_ERR_UNSUPPORTED;
+  (void)m;
+  return LC_OK;
+}
+
+// A key from the coefficient-form matrix in `tmp` (device memory holding
+// k*m*n residues, row-major (i, j)), which the call takes over: it is
+// transformed in place, transposed into the key's Ahat_T and freed, on every
+// return path.  One device synchronisation reports the kernels' errors.
+int key_create_from(const lc_ntt_plan* plan, uint32_t k, uint32_t m, void* tmp, uint32_t flags,
+                    lc_ajtai_key** out) {
   lc_ajtai_key* key = new (std::nothrow) lc_ajtai_key();
-  if (!key) return LC_ERR_OUT_OF_MEMORY;
+  if (!key) {
+    cudaFree(tmp);
+    return LC_ERR_OUT_OF_MEMORY;
+  }
   key->k = k;
   key->m = m;
   key->a_m = m;
@@ -1413,26 +1419,23 @@ LC_API int lc_ajtai_key_create_ex(const lc_ntt_plan* plan, uint32_t k, uint32_t 
   else
     rc = lc_ntt_plan_create_u32(plan->log_n, plan->q, plan->two_adicity, plan->generator, 1, &key->plan);
   if (rc) {
+    cudaFree(tmp);
     delete key;
     return rc;
   }
   const size_t eb = key->wide ? 8 : 4;
-  const size_t elems = (size_t)k * m * key->n;
-  void* tmp = nullptr;
-  if (cudaMalloc(&tmp, elems * eb) != cudaSuccess ||
-      cudaMalloc(&key->d_ahat_t, (size_t)key->n * m * kIPad * eb) != cudaSuccess ||
+  if (cudaMalloc(&key->d_ahat_t, (size_t)key->n * m * kIPad * eb) != cudaSuccess ||
       cudaMalloc(&key->d_err, 4) != cudaSuccess) {
     cudaGetLastError();
-    if (tmp) cudaFree(tmp);
+    cudaFree(tmp);
     lc_ajtai_key_destroy(key);
     return LC_ERR_OUT_OF_MEMORY;
   }
-  cudaMemset(key->d_err, 0, 4);
-  cudaMemcpy(tmp, matrix, elems * eb, matrix_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice);
-  // rotation-limb tables from the coefficient form (before it is transformed in place)
+  cudaMemsetAsync(key->d_err, 0, 4, nullptr);
   // the tensor-core witness transform's matrix image (once per device; a
   // failure only leaves the CUDA-core transform in use)
   if (plan->kind == PlanKind::Goldilocks && plan->log_n == 6) tc_ntt_prepare();
+  // rotation-limb tables from the coefficient form (before it is transformed in place)
   if (flags & LC_KEY_TENSOR_I8) {
     rc = tc_tables_create(static_cast<const uint64_t*>(tmp), k, m, &key->tc);
     if (rc) {
@@ -1460,14 +1463,47 @@ LC_API int lc_ajtai_key_create_ex(const lc_ntt_plan* plan, uint32_t k, uint32_t 
                                                         k, m, key->n);
     rc = map_cuda(cudaGetLastError());
   }
+  // one synchronisation: the kernels' errors, and nothing reads tmp any more
+  const cudaError_t e = cudaDeviceSynchronize();
+  if (!rc) rc = map_cuda(e);
   cudaFree(tmp);
-  if (!rc) rc = map_cuda(cudaDeviceSynchronize());
   if (rc) {
     lc_ajtai_key_destroy(key);
     return rc;
   }
   *out = key;
   return LC_OK;
+}
+
+}  // namespace lc
+
+extern "C" {
+
+LC_API int lc_ajtai_key_create(const lc_ntt_plan* plan, uint32_t k, uint32_t m, const void* matrix,
+                               int matrix_on_device, lc_ajtai_key** out) {
+  return lc_ajtai_key_create_ex(plan, k, m, matrix, matrix_on_device, 0, out);
+}
+
+LC_API int lc_ajtai_key_create_ex(const lc_ntt_plan* plan, uint32_t k, uint32_t m, const void* matrix,
+                                  int matrix_on_device, uint32_t flags, lc_ajtai_key** out) {
+  if (!plan || !matrix || !out || k == 0 || m == 0) return LC_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int rc = lc::key_create_check(plan, k, m, flags);
+  if (rc) return rc;
+  const size_t eb = plan->kind == PlanKind::Goldilocks ? 8 : 4;
+  const size_t bytes = (size_t)k * m * ((size_t)1 << plan->log_n) * eb;
+  void* tmp = nullptr;
+  if (cudaMalloc(&tmp, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return LC_ERR_OUT_OF_MEMORY;
+  }
+  const cudaError_t e =
+      cudaMemcpy(tmp, matrix, bytes, matrix_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(tmp);
+    return map_cuda(e);
+  }
+  return lc::key_create_from(plan, k, m, tmp, flags, out);
 }
 
 LC_API void lc_ajtai_key_destroy(lc_ajtai_key* key) {

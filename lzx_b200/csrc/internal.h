@@ -146,6 +146,11 @@ inline cudaError_t smem_attr_once(std::atomic<uint64_t>& done, K kern, size_t by
 }
 
 int device_sm_count();
+// Ajtai key creation (commit.cu): the argument check, and the creation from a
+// device buffer of the coefficient-form matrix that the call takes over.
+int key_create_check(const lc_ntt_plan* plan, uint32_t k, uint32_t m, uint32_t flags);
+int key_create_from(const lc_ntt_plan* plan, uint32_t k, uint32_t m, void* tmp, uint32_t flags,
+                    lc_ajtai_key** out);
 int map_cuda(cudaError_t e);
 int run_ntt(const lc_ntt_plan* plan, const void* in, void* out, size_t count, bool inverse,
             cudaStream_t s);

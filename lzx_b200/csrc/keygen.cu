@@ -238,17 +238,22 @@ LC_API int lc_ajtai_key_from_seed(const lc_ntt_plan* plan, uint32_t k, uint32_t 
   if (!plan || !seed || !out || k == 0 || m == 0) return LC_ERR_INVALID_ARGUMENT;
   *out = nullptr;
   if (plan->kind == PlanKind::Goldilocks || plan->num_moduli != 1) return LC_ERR_UNSUPPORTED;
+  int rc = key_create_check(plan, k, m, 0);
+  if (rc) return rc;
   const size_t count = (size_t)k * m, n = (size_t)1 << plan->log_n;
   uint32_t* mat = nullptr;
   if (cudaMalloc(&mat, count * n * 4) != cudaSuccess) {
     cudaGetLastError();
     return LC_ERR_OUT_OF_MEMORY;
   }
+  // the expansion is written straight into the buffer the key is built from
   static const uint8_t dom[7] = {'a', 'j', 't', 'a', 'i', '-', 'A'};
-  int rc = uniform_from_seed(plan, dom, 7, seed, 32, 0, count, mat, nullptr);
-  if (!rc) rc = lc_ajtai_key_create(plan, k, m, mat, 1, out);
-  cudaFree(mat);
-  return rc;
+  rc = uniform_from_seed(plan, dom, 7, seed, 32, 0, count, mat, nullptr);
+  if (rc) {
+    cudaFree(mat);
+    return rc;
+  }
+  return key_create_from(plan, k, m, mat, 0, out);  // takes over mat
 }
 
 }  // extern "C"
