@@ -78,6 +78,8 @@ struct lc_ntt_plan {
   uint32_t qinv[8] = {};
   uint32_t two_adicity[8] = {};
   uint32_t generator[8] = {};
+  // one device block: the forward table, the inverse table, the error word
+  void* d_block = nullptr;
   void* d_tw_fwd = nullptr;
   void* d_tw_inv = nullptr;
   uint32_t tw_fwd_entries = 0;

@@ -318,20 +318,20 @@ LC_API int lc_device_available(void) { return device_sm_count() > 0 ? 1 : 0; }
 
 static int finish_plan(lc_ntt_plan* plan, const std::vector<uint64_t>& fwd_raw_all,
                        const std::vector<uint64_t>& inv_raw_all) {
-  // convert raw residues into kernel twiddle entries
+  // convert raw residues into kernel twiddle entries (8 bytes each): the
+  // forward table, the inverse table and the zeroed error word go to the
+  // device as one block in one copy
   const uint32_t M = plan->num_moduli;
   const uint32_t ef = plan->tw_fwd_entries, ei = plan->tw_inv_entries;
+  plan->tw_bytes = 8;
+  const size_t nf = fwd_raw_all.size(), ni = inv_raw_all.size();
+  std::vector<uint64_t> img(nf + ni + 2, 0);  // + 16 bytes: the error word, zero
   if (plan->kind == PlanKind::Goldilocks) {
-    plan->tw_bytes = 8;
-    std::vector<uint64_t> f(fwd_raw_all), i(inv_raw_all);
-    if (cudaMalloc(&plan->d_tw_fwd, f.size() * 8) != cudaSuccess ||
-        cudaMalloc(&plan->d_tw_inv, i.size() * 8) != cudaSuccess)
-      return LC_ERR_OUT_OF_MEMORY;
-    cudaMemcpy(plan->d_tw_fwd, f.data(), f.size() * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(plan->d_tw_inv, i.data(), i.size() * 8, cudaMemcpyHostToDevice);
+    std::copy(fwd_raw_all.begin(), fwd_raw_all.end(), img.begin());
+    std::copy(inv_raw_all.begin(), inv_raw_all.end(), img.begin() + nf);
   } else {
-    plan->tw_bytes = 8;
-    std::vector<uint2> f(fwd_raw_all.size()), i(inv_raw_all.size());
+    uint2* f = reinterpret_cast<uint2*>(img.data());
+    uint2* i = f + nf;
     for (uint32_t m = 0; m < M; ++m) {
       const uint64_t q = plan->q[m];
       auto conv = [&](uint64_t w) -> uint2 {
@@ -342,15 +342,16 @@ static int finish_plan(lc_ntt_plan* plan, const std::vector<uint64_t>& fwd_raw_a
       for (uint32_t k = 0; k < ef; ++k) f[m * ef + k] = conv(fwd_raw_all[m * ef + k]);
       for (uint32_t k = 0; k < ei; ++k) i[m * ei + k] = conv(inv_raw_all[m * ei + k]);
     }
-    if (cudaMalloc(&plan->d_tw_fwd, f.size() * 8) != cudaSuccess ||
-        cudaMalloc(&plan->d_tw_inv, i.size() * 8) != cudaSuccess)
-      return LC_ERR_OUT_OF_MEMORY;
-    cudaMemcpy(plan->d_tw_fwd, f.data(), f.size() * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(plan->d_tw_inv, i.data(), i.size() * 8, cudaMemcpyHostToDevice);
   }
-  if (cudaMalloc(&plan->d_err, 4) != cudaSuccess) return LC_ERR_OUT_OF_MEMORY;
-  cudaMemset(plan->d_err, 0, 4);
-  return map_cuda(cudaDeviceSynchronize());
+  if (cudaMalloc(&plan->d_block, img.size() * 8) != cudaSuccess) {
+    cudaGetLastError();
+    plan->d_block = nullptr;
+    return LC_ERR_OUT_OF_MEMORY;
+  }
+  plan->d_tw_fwd = plan->d_block;
+  plan->d_tw_inv = static_cast<uint64_t*>(plan->d_block) + nf;
+  plan->d_err = reinterpret_cast<uint32_t*>(static_cast<uint64_t*>(plan->d_block) + nf + ni);
+  return map_cuda(cudaMemcpy(plan->d_block, img.data(), img.size() * 8, cudaMemcpyHostToDevice));
 }
 
 LC_API int lc_ntt_plan_create_u32(uint32_t log_n, const uint32_t* q, const uint32_t* two_adicity,
@@ -437,9 +438,7 @@ LC_API int lc_ntt_plan_create_goldilocks(uint32_t log_n, lc_ntt_plan** out) {
 
 LC_API void lc_ntt_plan_destroy(lc_ntt_plan* plan) {
   if (!plan) return;
-  if (plan->d_tw_fwd) cudaFree(plan->d_tw_fwd);
-  if (plan->d_tw_inv) cudaFree(plan->d_tw_inv);
-  if (plan->d_err) cudaFree(plan->d_err);
+  if (plan->d_block) cudaFree(plan->d_block);  // both tables and the error word
   if (plan->d_pow) cudaFree(plan->d_pow);
   plan->staging.release();
   delete plan;
