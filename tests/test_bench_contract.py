@@ -74,3 +74,27 @@ def test_short_summaries_fit_the_kept_tail():
     assert c["plain"]["v"] == 1235000.0 and c["int8_roofline"]["frac"] == 1230000.0
     assert c["cpu"]["1t"] and c["cpu"]["all"] and tail["fold"]["cpu"]["1t"] and tail["uneven_batch"]["cpu"]["1t"]
     assert bench.compact_commit(None) is None and bench.compact_fold({}) is None
+
+
+def test_compact_summaries_close_the_line():
+    """The short summaries of configs 1, 3, 4 and 5 that end the GPU arm's
+    line keep their keys with a leg missing or partly filled, and round the
+    figures to a few significant digits."""
+    sys.path.insert(0, ROOT)
+    import bench
+    for fn in (bench.compact_commit, bench.compact_fold, bench.compact_uneven, bench.compact_single):
+        assert fn(None) is None
+    c = bench.compact_commit({"bit_exact": True, "plain": {"ms_per_batch": 7.531234, "value": 1.114e9,
+                                                            "e2e": {"value": 4.838e8, "h2d_bytes_per_step": 1,
+                                                                    "d2h_bytes_per_step": 2}},
+                              "speedup_ntt_tensor_products_vs_plain": 4.2543})
+    assert c["plain"] == {"ms": 7.531, "v": 1.114e9, "e2e": 4.838e8}
+    assert c["ntt_tensor"] == {"ms": None, "v": None, "e2e": None}
+    assert c["ntt_tensor_vs_plain"] == 4.25 and c["e2e_bytes"] == {"h2d": 1, "d2h": 2} and c["cpu"] is None
+    f = bench.compact_fold({"m": 1 << 20, "graph": {"ms_per_step": 3.66412}, "forms_agree": True})
+    assert f["ms"] == 3.664 and f["eager_ms"] is None and f["forms_agree"] is True
+    u = bench.compact_uneven({"jobs": 512, "batch": {"ms": 48.5512, "bit_exact_vs_one_by_one": True}})
+    assert u["batch_ms"] == 48.55 and u["bit_exact"] is True and u["one_by_one_ms"] is None
+    s = bench.compact_single({"device_us_per_commit": 13.61, "e2e_us_per_commit": 30.64})
+    assert s == {"device_us": 13.6, "e2e_us": 30.6, "cpu_1t_us": None}
+    assert len(json.dumps({"commit": c, "fold": f, "uneven_batch": u, "single_commit": s})) < 1500
