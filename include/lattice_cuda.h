@@ -167,8 +167,9 @@ LC_API int lc_ajtai_commit_i8(lc_ajtai_key *key, const int8_t *s, size_t batch, 
 LC_API int lc_ajtai_commit_u8(lc_ajtai_key *key, const uint8_t *s, size_t batch, void *out,
                               lc_stream stream);
 /* Host-buffer variants (synchronous).  Small commitments (those the
- * single-launch kernel takes: at most 4 witnesses, 2048 ring elements) run
- * that kernel directly on page-locked host memory -- the caller's buffers
+ * single-launch kernel takes: at most 4 witnesses, 2048 ring elements, with
+ * a witness of at most 256 KiB) run that kernel directly on page-locked host
+ * memory -- the caller's buffers
  * when they are pinned (output 16-byte aligned), else the key's pinned
  * staging buffers -- with no copies queued; larger ones upload, commit on
  * the device and download. */

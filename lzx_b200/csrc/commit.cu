@@ -1693,12 +1693,15 @@ static int commit_host(lc_ajtai_key* key, const void* s, size_t in_elem, size_t 
     // a commitment small enough for the single-launch kernel, with input and
     // output in page-locked host memory (the staging buffers or the caller's):
     // the kernel reads the witness and writes the rows over the host link
-    // itself, so neither copy is queued
+    // itself, so neither copy is queued.  Only for witnesses of up to 256 KiB,
+    // where the copies' fixed cost outweighs the kernel's slower loads over
+    // the link; larger ones are copied at the copy engine's rate
     const void* hin = stage_in ? key->h_stage_in : s;
     void* hout = stage_out ? key->h_stage_out : out;
     void* din = nullptr;
     void* dout = nullptr;
-    if (key->engine == LC_ENGINE_NTT && mapped_host(hin, &din) && mapped_host(hout, &dout) &&
+    if (key->engine == LC_ENGINE_NTT && in_bytes <= ((size_t)256 << 10) && mapped_host(hin, &din) &&
+        mapped_host(hout, &dout) &&
         reinterpret_cast<uintptr_t>(din) % in_elem == 0 && (reinterpret_cast<uintptr_t>(dout) & 15) == 0) {
       int frc = LC_ERR_UNSUPPORTED;
       if (in_elem == 1)
