@@ -44,3 +44,23 @@ def test_fold_is_congruent_and_in_range():
         want = sum(x << (8 * l) for l, x in enumerate(d)) % P
         assert 0 <= got <= M64
         assert got % P == want, d
+
+
+def test_crt_residue_step_needs_one_correction():
+    """The CRT residues of z (lzx_b200/csrc/pipeline.cu ``crt_residues_kernel``
+    and ``crt_ntt_kernel``): t = x - floor(x mu / 2^64) q with
+    mu = floor((2^64 - 1) / q) stays below 2q for every 64-bit x (the
+    quotient estimate is short by at most one, since
+    x/q - x mu/2^64 = x (1 + (2^64 - 1) mod q) / (q 2^64) < 1), so one
+    conditional subtraction gives x mod q; checked on random values, on
+    multiples of q and their neighbours up to 2^64 - 1."""
+    rng = np.random.default_rng(11)
+    for q in (1073738753, 1073732609, 1073731073, 1073726977, 3 * (1 << 30) + 1, 2013265921, 12289):
+        mu = M64 // q
+        xs = [int(x) for x in rng.integers(0, 1 << 63, size=2000, dtype=np.int64)] + [M64, P - 1, 0, 1]
+        top = M64 // q
+        xs += [k * q + d for k in range(top - 500, top + 1) for d in (0, 1, q - 1) if k * q + d <= M64]
+        for x in xs:
+            t = x - ((x * mu) >> 64) * q
+            assert 0 <= t < 2 * q
+            assert (t - q if t >= q else t) == x % q
