@@ -1,4 +1,4 @@
-"""CPU model of the witness-transform limb fold.
+"""CPU models of the limb folds and residue steps of the tensor-core and CRT kernels.
 
 The tensor-core witness transforms (lzx_b200/csrc/tc_commit.cu ``tn_fold``,
 lzx_b200/csrc/batch.cu ``tw_fold_gl``) turn eight signed limb sums D_l into
@@ -64,3 +64,32 @@ def test_crt_residue_step_needs_one_correction():
             t = x - ((x * mu) >> 64) * q
             assert 0 <= t < 2 * q
             assert (t - q if t >= q else t) == x % q
+
+
+def test_crt_lane_fold_matches_modulo():
+    """The uneven batch's tensor-core fold for 30-bit lanes
+    (lzx_b200/csrc/batch.cu ``tw_fold``, admitted by ``tw_fold_exact``):
+    v = sum_l 2^(8l) D_l plus the offset q 2^19, two folds by 2^30 == c
+    (q = 2^30 - c) in the 64- and 32-bit widths the kernel uses, and one
+    min(y, y - q), equal v mod q for the CRT primes at d = 128 and 256 on
+    random and extreme limb sums (|D_l| <= d 128 255)."""
+    rng = np.random.default_rng(13)
+    mask30, m32 = (1 << 30) - 1, (1 << 32) - 1
+    for q in (1073738753, 1073732609, 1073731073, 1073726977):
+        c, off = (1 << 30) - q, q << 19
+        for d in (128, 256):
+            lim = d * 128 * 255
+            vmax = d * 128 * 255 * 16843009
+            assert off > vmax and c <= (1 << 20)  # what tw_fold_exact requires
+            cases = [[lim] * 4, [-lim] * 4, [0] * 4, [lim, -lim, lim, -lim], [-lim, 0, 0, lim]]
+            cases += rng.integers(-lim, lim + 1, size=(3000, 4)).tolist()
+            for x in cases:
+                v = off + x[0] + 256 * x[1] + 65536 * x[2] + 16777216 * x[3]
+                assert 0 < v < (1 << 63)
+                u = v
+                w = (u >> 30) * c + (u & mask30)
+                assert (u >> 30) < (1 << 32) and w < (1 << 64)
+                y = ((w >> 30) * c + (w & mask30))
+                assert y <= m32 and y < 2 * q  # the 32-bit sum does not wrap
+                got = min(y, (y - q) & m32)
+                assert got == (x[0] + 256 * x[1] + 65536 * x[2] + 16777216 * x[3]) % q
